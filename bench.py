@@ -1,0 +1,376 @@
+"""Benchmark: integral-direct 2J-K Fock build on (H2O)8 / 6-31G** (N = 200).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pqb|reference]
+                    [--precision mixed|fp64] [--no-cpu-baseline]
+
+One step = one full 2J-K Fock build G(D) = 2J(D) - K(D) for a fixed SCF
+density D of the seeded (H2O)8 cluster (Schwarz 1e-12; mixed precision puts
+quartets with Q_ab Q_cd < 1e-5 in FP32).  value = nominal unique quartets
+Q = P(P+1)/2 (P = N(N+1)/2, 202,015,050) per second of Fock build, i.e. the
+same count the reference's get2ints evaluates (PyQuante/Ints.py:146-167).
+Under torchrun the quartet lists are sharded over ranks and J/K summed
+with one NCCL all-reduce per build (strong scaling).
+
+The reference arm (--impl reference) times the reference's own C Rys engine
+(oracle/_ref/ref_fock, compiled from the reference's Src/lib/utils/crys.c)
+over a bounded sample of the same quartets on all host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "(H2O)8 cluster, 6-31G** cartesian, N=200, seed 0, 9 A cube"
+SCHWARZ = 1e-12
+FP32_THRESH = 1e-5
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="pqb", choices=["pqb", "reference"])
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+def molecule():
+    from pyquante_b200 import geometries
+    return geometries.water_cluster(8, seed=0)
+
+
+def nominal_quartets(n):
+    P = n * (n + 1) // 2
+    return P * (P + 1) // 2
+
+
+# ------------------------------------------------------------ CPU reference --
+def _oracle_table(bs):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyq_oracle as O
+    return O, O.Table([O.BF(bf.origin, bf.powers, list(zip(bf.pexps, bf.pcoefs))) for bf in bs.bfs])
+
+
+def reference_rate(bs, seconds, seed=0, nproc=None):
+    """Quartets/s of the reference's compiled Rys engine (ref_fock, forked
+    workers over bra rows) on a bounded random sample of bra rows."""
+    O, tab = _oracle_table(bs)
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_fock")
+    if not os.path.exists(exe):
+        raise RuntimeError("oracle/_ref/ref_fock not built (make -C oracle ref)")
+    nproc = nproc or os.cpu_count() or 1
+    n = tab.nbf
+    P = n * (n + 1) // 2
+    rng = np.random.default_rng(seed)
+    with tempfile.TemporaryDirectory() as td:
+        bpath = os.path.join(td, "basis.bin")
+        tab.write(bpath)
+
+        def run(nrows):
+            rows = np.sort(rng.choice(P, size=nrows, replace=False)).astype(np.int64)
+            rpath = os.path.join(td, "rows.bin")
+            rows.tofile(rpath)
+            out = subprocess.run([exe, bpath, rpath, str(nproc)], capture_output=True, text=True, check=True)
+            return json.loads(out.stdout)
+
+        probe = run(max(nproc, 4))
+        rate = probe["quartets"] / max(probe["seconds"], 1e-6)
+        avg_row = nominal_quartets(n) / P
+        nrows = int(min(P, max(nproc, rate * seconds / avg_row)))
+        r = run(nrows)
+    return dict(value=r["quartets"] / r["seconds"], quartets=r["quartets"], seconds=r["seconds"], rows=nrows,
+                cores=nproc)
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from pyquante_b200.Basis.basis import BasisSet
+    bs = BasisSet(molecule(), "6-31g**")
+    cores = os.cpu_count() or 1
+    per_step = max(2.0, min(20.0, 120.0 / max(a.steps + a.warmup, 1)))
+    for i in range(a.warmup):
+        reference_rate(bs, per_step / 2, seed=100 + i, nproc=cores)
+    rates, secs, counts = [], [], []
+    for i in range(a.steps):
+        r = reference_rate(bs, per_step, seed=i, nproc=cores)
+        rates.append(r["value"])
+        secs.append(r["seconds"])
+        counts.append(r["quartets"])
+    value = sum(counts) / sum(secs)
+    Q = nominal_quartets(len(bs))
+    line = {
+        "impl": "reference", "metric": "ERI quartets/s (2J-K Fock build, nominal unique (ij|kl))",
+        "value": value, "unit": "quartets/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * Q / value, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": "fp64", "nominal_quartets": Q,
+                   "sample": "random bra rows of Ints.get2ints, all kl >= ij per row, ~%.0f s per step" % per_step},
+        "cpu_baseline": {"value": value, "unit": "quartets/s", "cores": cores, "kind": "reference",
+                         "sample": "%d quartets over %d steps" % (sum(counts), a.steps)},
+        "e2e": {"value": value, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------- clocks --
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def __enter__(self):
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([c.strip() for c in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._th = threading.Thread(target=loop, daemon=True)
+        self._th.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._th.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# --------------------------------------------------------------- GPU arm --
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import torch
+    import torch.distributed as dist
+
+    from pyquante_b200 import Ints, _lib
+    from pyquante_b200.Basis.basis import BasisSet
+    from pyquante_b200.LA2 import geigh, mkdens
+    from pyquante_b200.engine import BasisEngine
+    from pyquante_b200.flops import class_flops, quartet_class_ls
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    mol = molecule()
+    bs = BasisSet(mol, "6-31g**")
+    n = len(bs)
+    Q = nominal_quartets(n)
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        # before any CUDA work in this process: the baseline forks workers
+        cpu = reference_rate(bs, a.cpu_seconds)
+    eng = BasisEngine(bs.bfs, device=local)
+    counts = eng.plan(SCHWARZ, FP32_THRESH)
+    if world > 1:
+        eng.ctx.check(eng.ctx.lib.pqb_plan_shard(eng.ctx.h, rank, world))
+    # a realistic density: a few SCF iterations from the core guess
+    S, h = Ints.get1ints(bs, mol)
+    St = torch.as_tensor(S, device="cuda")
+    ht = torch.as_tensor(h, device="cuda")
+    nocc = mol.get_nel() // 2
+    _, C = geigh(ht, St)
+    for _ in range(3):
+        D = mkdens(C, 0, nocc).contiguous()
+        J, K = eng.jk(D, "fp64", SCHWARZ, FP32_THRESH)
+        if world > 1:
+            dist.all_reduce(J)
+            dist.all_reduce(K)
+        _, C = geigh(ht + 2 * J - K, St)
+    D = mkdens(C, 0, nocc).contiguous()
+    J = torch.empty_like(D)
+    K = torch.empty_like(D)
+    G = torch.empty_like(D)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def build(mode):
+        eng.jk(D, mode, SCHWARZ, FP32_THRESH, J=J, K=K)
+        if world > 1:
+            dist.all_reduce(J)
+            dist.all_reduce(K)
+        torch.sub(J.mul(2.0), K, out=G)
+
+    def timed(mode, steps):
+        tot = 0.0
+        for _ in range(steps):
+            flush.zero_()          # L2 flush between timed builds, outside the timed window
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            build(mode)
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / steps
+
+    for _ in range(a.warmup):
+        build(a.precision)
+        build("fp64")
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms = timed(a.precision, a.steps)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+    ms_fp64 = timed("fp64", a.steps)
+    if world > 1:
+        t = torch.tensor([ms, ms_fp64], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_fp64 = t.tolist()
+
+    # end to end through the public API: pinned host D in, host G out
+    Dh = D.cpu().pin_memory()
+    direct = Ints.DirectInts(eng, a.precision, SCHWARZ, FP32_THRESH)
+    Gh = torch.empty_like(Dh).pin_memory()
+
+    def e2e_step():
+        Dd = Dh.to("cuda", non_blocking=True)
+        Jd, Kd = direct.jk(Dd)
+        if world > 1:
+            dist.all_reduce(Jd)
+            dist.all_reduce(Kd)
+        Gh.copy_(2.0 * Jd - Kd, non_blocking=True)
+
+    for _ in range(a.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = 0.0
+    for _ in range(a.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    e2e_ms /= a.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t[0])
+
+    # roofline: per-class FP64 timing of the direct J/K kernels
+    qs = (torch.zeros(42, dtype=torch.int64)).numpy()
+    ps = qs.copy()
+    import ctypes
+    qa = (ctypes.c_int64 * 42)()
+    pa = (ctypes.c_int64 * 42)()
+    eng.ctx.check(eng.ctx.lib.pqb_plan_stats(eng.ctx.h, qa, pa))
+    qs = np.array(qa[:]).reshape(2, 21)
+    ps = np.array(pa[:]).reshape(2, 21)
+    per_class = []
+    launches = 2   # two symmetrise kernels per build
+    for part in (0, 1):
+        for qc in range(21):
+            if qs[part, qc] == 0:
+                continue
+            launches += 1
+            tms = []
+            for _ in range(3):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                eng.ctx.check(eng.ctx.lib.pqb_jk_direct_class(eng.ctx.h, _lib.ptr(D), _lib.ptr(J), _lib.ptr(K), part,
+                                                              qc, _lib.PQB_FP64, _lib.stream_ptr()))
+                e1.record(stream)
+                e1.synchronize()
+                tms.append(e0.elapsed_time(e1))
+            t_ms = sorted(tms)[1]
+            fl = class_flops(qc, int(ps[part, qc]), int(qs[part, qc]))
+            per_class.append(dict(part=part, cls=quartet_class_ls(qc), ms=t_ms, flops=fl,
+                                  tflops=fl / (t_ms * 1e-3) / 1e12))
+    peak = ctypes.c_double()
+    eng.ctx.check(eng.ctx.lib.pqb_fp64_peak(eng.ctx.h, 200000, ctypes.byref(peak)))
+    peak_tf = peak.value / 1e12
+    dom = max(per_class, key=lambda r: r["ms"])
+    tot_fl = sum(r["flops"] for r in per_class)
+    tot_ms = sum(r["ms"] for r in per_class)
+    if rank == 0:
+        line = {
+            "metric": "ERI quartets/s (2J-K Fock build, nominal unique (ij|kl))",
+            "value": Q / (ms * 1e-3), "unit": "quartets/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64+f32" if a.precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": a.precision, "schwarz": SCHWARZ,
+                       "fp32_threshold": FP32_THRESH, "nominal_quartets": Q,
+                       "shell_quartets": counts["shell_quartets"], "kept_fp64": counts["fp64"],
+                       "kept_fp32": counts["fp32"], "l2": "256 MiB buffer zeroed between timed builds",
+                       "fp64_ms_per_step": ms_fp64, "mixed_speedup_vs_fp64": ms_fp64 / ms,
+                       "parallelism": "quartet shards x%d + NCCL all-reduce of J,K" % world if world > 1 else "1 GPU"},
+            "e2e": {"value": Q / (e2e_ms * 1e-3), "unit": "quartets/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": int(D.numel() * 8), "d2h_bytes_per_step": int(D.numel() * 8),
+                    "api": "pyquante_b200.Ints.DirectInts.jk (the get2JmK path) from pinned host D"},
+            "roofline": {"bound": "fp64", "achieved": dom["tflops"], "peak": peak_tf, "unit": "TFLOP/s",
+                         "frac": dom["tflops"] / peak_tf, "traffic": None,
+                         "kernel": "eri_*_kernel class (%d%d|%d%d) FP64 J/K" % tuple(dom["cls"]),
+                         "peak_source": "measured DFMA probe (pqb_fp64_peak) on this GPU",
+                         "all_classes_frac": tot_fl / (tot_ms * 1e-3) / 1e12 / peak_tf},
+            "gpu_launches": launches * a.steps,
+            "clocks": clk.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = {"value": cpu["value"], "unit": "quartets/s", "cores": cpu["cores"],
+                                    "kind": "reference",
+                                    "sample": "%d quartets (%d random bra rows, all kl >= ij) in %.1f s" % (
+                                        cpu["quartets"], cpu["rows"], cpu["seconds"])}
+        line["per_class_fp64"] = [dict(cls="%d%d|%d%d" % r["cls"], part=r["part"], ms=round(r["ms"], 4),
+                                       tflops=round(r["tflops"], 3)) for r in sorted(per_class, key=lambda r: -r["ms"])]
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

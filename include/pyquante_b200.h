@@ -1,0 +1,144 @@
+/* pyquante_b200 — C ABI of the B200 two-electron-integral and Fock-build
+ * engine.  Plain C: opaque context, raw device pointers, sizes, int status.
+ * No torch or CUDA types appear in the signatures; `stream` is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Every function returns PQB_OK (0) or a PQB_E_* code; the message of the
+ * last failure is available from pqb_last_error().  Device buffers are owned
+ * by the caller; the context owns only its shell/pair/quartet tables.
+ *
+ * Reference interfaces replaced (PyQuante, paths inside the project):
+ *   - PyQuante/Ints.py:146-167  get2ints      -> pqb_eri_packed
+ *   - PyQuante/Ints.py:195-238  getJ/getK/get2JmK on stored integrals
+ *                                             -> pqb_jk_packed
+ *   - the same three, integral-direct        -> pqb_jk_direct
+ *   - PyQuante/Ints.py:73-87    get1ints (S, T+V) -> pqb_oneint
+ *   - Src/crys.c:1556-1674 contr_coulomb, :1676-1711 coulomb_repulsion,
+ *     Src/cints.c:572-803 (same two), Src/chgp.c:701-890 (contr_coulomb,
+ *     hrr, vrr)                                -> pqb_eri_functions
+ *   - Src/cints.c:413-425 ijkl2intindex (32-bit; overflows at nbf >= 304)
+ *                                             -> pqb_ijkl2intindex (64-bit)
+ *   - Src/lib/utils/math.c:27-36 Fgamma (integer m) -> pqb_boys_eval
+ *   - Src/crys.c:99-1438 Roots                -> pqb_rys_eval
+ */
+#ifndef PYQUANTE_B200_H
+#define PYQUANTE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    PQB_OK = 0,
+    PQB_E_ARG = 1,      /* bad argument (NULL pointer, negative size, ...)   */
+    PQB_E_CLASS = 2,    /* angular momentum beyond what the kernels support  */
+    PQB_E_NPRIM = 3,    /* too many primitives in one contraction            */
+    PQB_E_SHAPE = 4,    /* buffer length does not match the basis            */
+    PQB_E_CUDA = 5,     /* a CUDA runtime call failed                        */
+    PQB_E_STATE = 6,    /* call order: e.g. no basis uploaded yet            */
+    PQB_E_TIMEOUT = 7,  /* a bounded device wait gave up                     */
+    PQB_E_NOMEM = 8     /* device allocation failed                          */
+};
+
+/* precision modes of pqb_jk_direct */
+enum { PQB_FP64 = 0, PQB_MIXED = 1 };
+/* engines of pqb_eri_functions */
+enum { PQB_ENGINE_RYS = 0, PQB_ENGINE_HGP = 1 };
+
+typedef struct pqb_ctx pqb_ctx;
+
+int pqb_version(void);
+int pqb_create(pqb_ctx **ctx, int device);
+void pqb_destroy(pqb_ctx *ctx);
+/* copies the last error message (NUL-terminated, truncated to len) */
+int pqb_last_error(const pqb_ctx *ctx, char *buf, size_t len);
+
+/* Shell basis for the class engine.  Shell s has angular momentum
+ * shell_l[s] <= 2 (cartesian, PyQuante component order), shell_nprim[s]
+ * primitives starting at prim_off[s] in prim_exp/prim_coef, centre
+ * shell_xyz[3s..3s+2] (bohr) and functions [shell_f0[s], shell_f0[s]+ncart).
+ * The contracted function f = fscale[f] * sum_p prim_coef[p] * g(alpha_p),
+ * g the UNNORMALISED cartesian primitive: prim_coef carries contraction
+ * coefficient, primitive norm and contracted norm of the shell's first
+ * component; fscale carries each component's ratio to it.  Builds shell
+ * pairs and the unscreened quartet lists. */
+int pqb_shells_upload(pqb_ctx *ctx, int nshell, const int *shell_l, const int *shell_nprim, const int *prim_off,
+                      const int *shell_f0, const double *shell_xyz, const double *prim_exp, const double *prim_coef,
+                      int nbf, const double *fscale);
+
+/* Schwarz factors Q_ab = sqrt(max |(ab|ab)|) for every shell pair, computed
+ * on the device; copied to Q_host (length npairs) when it is not NULL. */
+int pqb_schwarz(pqb_ctx *ctx, double *Q_host, void *stream);
+int pqb_num_pairs(const pqb_ctx *ctx);
+
+/* Screened quartet plan for pqb_jk_direct: quartets with Q_ab Q_cd <
+ * schwarz_thresh are dropped; below fp32_thresh they go to the FP32 list
+ * (used in PQB_MIXED mode).  counts (may be NULL) receives
+ * {shell quartets, kept FP64, kept FP32, dropped}. */
+int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *counts);
+
+/* Per-class statistics of the current plan, arrays of 2*21 int64 indexed
+ * [part*21 + class] (part 0 = FP64 list, 1 = FP32-eligible list; class =
+ * bra*(bra+1)/2 + ket over pair classes ss ps pp ds dp dd): shell quartets and
+ * primitive quartets. */
+int pqb_plan_stats(const pqb_ctx *ctx, int64_t *quartets, int64_t *prim_quartets);
+
+/* Keep only every nranks-th quartet of each class list of the current plan,
+ * starting at rank (multi-GPU sharding of one Fock build). */
+int pqb_plan_shard(pqb_ctx *ctx, int rank, int nranks);
+
+/* FP64 FMA throughput probe: `iters` dependent-chain FMA rounds on every SM;
+ * returns achieved FP64 FLOP/s in *flops (a roofline denominator). */
+int pqb_fp64_peak(pqb_ctx *ctx, int iters, double *flops);
+
+/* All unique (ij|kl), i>=j, k>=l, ij>=kl, at ijkl2intindex (64-bit) into
+ * out (device, len = P(P+1)/2, P = nbf(nbf+1)/2).  Unscreened, FP64. */
+int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream);
+
+/* Integral-direct J_ij = sum_kl (ij|kl) D_kl and K_ij = sum_kl (ik|jl) D_kl
+ * for a symmetric density D (device, nbf x nbf, row-major); J and K are
+ * overwritten.  mode = PQB_FP64 or PQB_MIXED. */
+int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode, void *stream);
+
+/* One class list of the plan only (part 0 FP64 list / 1 FP32-eligible list,
+ * class 0..20), accumulating unsymmetrised contributions into Jacc/Kacc
+ * (not cleared).  For per-class timing and tuning. */
+int pqb_jk_direct_class(pqb_ctx *ctx, const double *D, double *Jacc, double *Kacc, int part, int qclass, int mode,
+                        void *stream);
+
+/* The same J and K from stored packed integrals (device). */
+int pqb_jk_packed(pqb_ctx *ctx, const double *ints, int64_t len, const double *D, double *J, double *K, int nbf,
+                  void *stream);
+
+/* Stateless per-function kernels over a device function table:
+ * origin[3n], powers[3n], prim_off[n+1], exps/cn[prim_off[n]] where
+ * cn = contraction coefficient * primitive norm, norms[n] (contracted norm).
+ * pqb_eri_functions: out[q] = norms_a..d * sum cn_a..cn_d (prim ERI) for the
+ * function quartets quartets[4q..4q+3] (total angular momentum <= 9), by Rys
+ * quadrature (PQB_ENGINE_RYS) or Head-Gordon--Pople (PQB_ENGINE_HGP;
+ * |a|+|b| <= 4 and |c|+|d| <= 4).  aux_m > 0 (HGP only) returns the
+ * auxiliary (ab|cd)^(m) of chgp.vrr (Src/chgp.c:244-419) instead.
+ * pqb_oneint: S, T, V (each n x n, any may be NULL) with V = sum_atoms Z_a
+ * <i|-1/|r-R_a||j>. */
+int pqb_eri_functions(pqb_ctx *ctx, int engine, int aux_m, int nq, const int *quartets, int n, const double *origin,
+                      const int *powers, const int *prim_off, const double *exps, const double *cn,
+                      const double *norms, double *out, void *stream);
+int pqb_oneint(pqb_ctx *ctx, int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
+               const double *cn, const double *norms, int natoms, const double *atom_xyz, const double *atom_z,
+               double *S, double *T, double *V, void *stream);
+
+/* Canonical packed index, 64-bit. */
+int64_t pqb_ijkl2intindex(int64_t i, int64_t j, int64_t k, int64_t l);
+
+/* Kernel-level checks: F_0..F_m(T_i) into F[i*(m+1)+k] (m <= 16), and the
+ * n-root Rys rule (n <= 5) at T_i into u[i*n+r], w[i*n+r].  Device arrays. */
+int pqb_boys_eval(pqb_ctx *ctx, int m, int count, const double *T, double *F, void *stream);
+int pqb_rys_eval(pqb_ctx *ctx, int nroots, int count, const double *T, double *u, double *w, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

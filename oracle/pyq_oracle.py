@@ -1,0 +1,362 @@
+"""CPU oracle for the ERI / Fock-build path — TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
+import this module; the product (pyquante_b200) never does.
+
+Two independent CPU sources of truth, both driven through ctypes:
+  * the REFERENCE's own C engines, compiled from its sources by
+    ``make -C oracle ref`` into oracle/_ref/ (Src/lib/utils/crys.c — the Rys
+    engine PyQuante/CGBF.py:24 binds for get2ints — plus Src/chgp.c and
+    Src/cints.c through include-shims, and ref_fock.c, a C driver with the
+    loop of PyQuante/Ints.py:146-167);
+  * this project's plain-C restatement (oracle/eri_oracle.c, built by
+    ``make -C oracle``): Head-Gordon--Pople ERIs with a long-double Boys
+    function, THO one-electron integrals, get2ints/getJ/getK.
+
+The Python layer restates what the reference's Python 2 code does
+(it cannot run here): the integral loop order and packing
+(PyQuante/Ints.py:146-193), get2JmK (Ints.py:225-238), and the RHF loop
+(PyQuante/hartree_fock.py:66-149 with LA2.geigh's Cholesky orthogonalisation,
+PyQuante/LA2.py:47-75,113-131, and Convergence.DIIS, :73-136).
+
+Parity pin: the restatement is checked against the compiled reference
+(tests/test_oracle.py) and against the reference's own known answers
+(Boys values of Src/lib/utils/tests/TestMath.c:18-20; RHF energies of
+Tests/h2o.py:16 and Tests/h2.py:16; see tests/golden/).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+BUILD_DIR = os.path.join(HERE, "_build")
+
+_d = ctypes.c_double
+_i = ctypes.c_int
+_i64 = ctypes.c_int64
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+_libs = {}
+
+
+def _load(name, path):
+    if name not in _libs:
+        if not os.path.exists(path):
+            return None
+        _libs[name] = ctypes.CDLL(path)
+    return _libs[name]
+
+
+def oracle_lib():
+    lib = _load("oracle", os.path.join(BUILD_DIR, "liboracle.so"))
+    if lib is None:
+        raise RuntimeError("oracle not built: make -C oracle")
+    lib.orc_boys.restype = _d
+    lib.orc_boys.argtypes = [_i, _d]
+    lib.orc_ijkl2intindex.restype = _i64
+    lib.orc_ijkl2intindex.argtypes = [_i64] * 4
+    lib.orc_get2ints.argtypes = [_i64, _dp, _i64p, _i64p, _dp, _dp, _dp, _dp, _dp]
+    lib.orc_get1ints.argtypes = [_i64, _dp, _i64p, _i64p, _dp, _dp, _dp, _dp, _i64, _dp, _dp, _dp, _dp]
+    lib.orc_getJK.argtypes = [_i64, _dp, _dp, _dp, _dp]
+    lib.orc_contr_eri.restype = _d
+    return lib
+
+
+def ref_available():
+    return all(os.path.exists(os.path.join(REF_DIR, f)) for f in
+               ("libref_crys.so", "libref_chgp.so", "libref_cints.so", "libref_fock.so", "ref_fock"))
+
+
+def ref_lib(which):
+    """which in {'crys', 'chgp', 'cints', 'fock'}; None when not built."""
+    lib = _load("ref_" + which, os.path.join(REF_DIR, "libref_%s.so" % which))
+    if lib is None:
+        return None
+    if which == "crys":
+        lib.coulomb_repulsion.restype = _d
+        lib.coulomb_repulsion.argtypes = [_d, _d, _d, _d, _i, _i, _i, _d] * 4
+        lib.contr_coulomb.restype = _d
+        lib.contr_coulomb.argtypes = [_i, _dp, _dp, _dp, _d, _d, _d, _i, _i, _i] * 4
+        lib.Fgamma.restype = _d
+        lib.Fgamma.argtypes = [_d, _d]
+        lib.Fm.restype = _d
+        lib.Fm.argtypes = [_i, _d]
+    elif which == "chgp":
+        lib.ref_chgp_hrr.restype = _d
+        lib.ref_chgp_hrr.argtypes = [_d, _d, _d, _d, _i, _i, _i, _d] * 4
+        lib.ref_chgp_vrr.restype = _d
+        lib.ref_chgp_vrr.argtypes = ([_d, _d, _d, _d, _i, _i, _i, _d] + [_d, _d, _d, _d, _d] +
+                                     [_d, _d, _d, _d, _i, _i, _i, _d] + [_d, _d, _d, _d, _d] + [_i])
+        lib.ref_chgp_contr.restype = _d
+        lib.ref_chgp_contr.argtypes = [_i, _dp, _dp, _dp, _dp, _ip] * 4
+        lib.ref_chgp_Fgamma.restype = _d
+        lib.ref_chgp_Fgamma.argtypes = [_d, _d]
+    elif which == "cints":
+        lib.ref_cints_coulomb_repulsion.restype = _d
+        lib.ref_cints_coulomb_repulsion.argtypes = [_d, _d, _d, _d, _i, _i, _i, _d] * 4
+        for f in ("ref_cints_overlap", "ref_cints_kinetic"):
+            getattr(lib, f).restype = _d
+            getattr(lib, f).argtypes = [_d, _i, _i, _i, _d, _d, _d] * 2
+        lib.ref_cints_nuclear.restype = _d
+        lib.ref_cints_nuclear.argtypes = [_d, _d, _d, _d, _i, _i, _i, _d] * 2 + [_d, _d, _d]
+        lib.ref_cints_ijkl2intindex.restype = _i
+        lib.ref_cints_ijkl2intindex.argtypes = [_i] * 4
+        lib.ref_cints_Fgamma.restype = _d
+        lib.ref_cints_Fgamma.argtypes = [_d, _d]
+    elif which == "fock":
+        lib.ref_get2ints.restype = _i
+        lib.ref_get2ints.argtypes = [_i64, _dp, _i64p, _i64p, _dp, _dp, _dp, _dp, _dp, _i]
+        lib.ref_get2JmK.argtypes = [_i64, _dp, _dp, _dp]
+        lib.ref_ijkl2intindex64.restype = _i64
+        lib.ref_ijkl2intindex64.argtypes = [_i64] * 4
+        lib.ref_time_rows.restype = _d
+        lib.ref_time_rows.argtypes = [_i64, _dp, _i64p, _i64p, _dp, _dp, _dp, _dp, _i64p, _i64, _i, _i64p, _dp]
+    return lib
+
+
+# ------------------------------------------------------------------ basis --
+def _fact2(n):
+    r = 1
+    while n > 1:
+        r *= n
+        n -= 2
+    return r
+
+
+def prim_norm(alpha, powers):
+    """Src/lib/primitive-gto.c:76-83."""
+    l, m, n = powers
+    L = l + m + n
+    return np.sqrt(2.0 ** (2 * L + 1.5) * alpha ** (L + 1.5) /
+                   (_fact2(2 * l - 1) * _fact2(2 * m - 1) * _fact2(2 * n - 1) * np.pi ** 1.5))
+
+
+SYM2POWERS = {
+    "S": [(0, 0, 0)],
+    "P": [(1, 0, 0), (0, 1, 0), (0, 0, 1)],
+    "D": [(2, 0, 0), (1, 1, 0), (1, 0, 1), (0, 2, 0), (0, 1, 1), (0, 0, 2)],
+}
+
+
+class BF:
+    """One contracted function as PyQuante's BasisSet builds it
+    (PyQuante/Basis/basis.py:27-46, CGBF.py:27-75): norm 1, per-primitive
+    per-component norms."""
+
+    def __init__(self, origin, powers, prims):
+        self.origin = tuple(float(c) for c in origin)
+        self.powers = tuple(powers)
+        self.pexps = [float(a) for a, _ in prims]
+        self.pcoefs = [float(c) for _, c in prims]
+        self.pnorms = [prim_norm(a, powers) for a in self.pexps]
+        self.norm = 1.0
+
+
+def build_basis(atoms, basis_data):
+    """atoms: [(Z, (x, y, z) bohr)], basis_data: {Z: [(sym, [(exp, coef)])]}."""
+    bfs = []
+    for z, xyz in atoms:
+        for sym, prims in basis_data[z]:
+            for p in SYM2POWERS[sym]:
+                bfs.append(BF(xyz, p, prims))
+    return bfs
+
+
+class Table:
+    """Flat per-function arrays (the layout ref_fock.c / eri_oracle.c read)."""
+
+    def __init__(self, bfs):
+        self.nbf = len(bfs)
+        self.origin = np.ascontiguousarray([bf.origin for bf in bfs], dtype=np.float64).reshape(-1)
+        self.powers = np.ascontiguousarray([bf.powers for bf in bfs], dtype=np.int64).reshape(-1)
+        off = [0]
+        for bf in bfs:
+            off.append(off[-1] + len(bf.pexps))
+        self.prim_off = np.array(off, dtype=np.int64)
+        self.exps = np.array([e for bf in bfs for e in bf.pexps], dtype=np.float64)
+        self.coefs = np.array([c for bf in bfs for c in bf.pcoefs], dtype=np.float64)
+        self.pnorms = np.array([c for bf in bfs for c in bf.pnorms], dtype=np.float64)
+        self.norms = np.array([bf.norm for bf in bfs], dtype=np.float64)
+
+    def args(self):
+        P = lambda a, t: a.ctypes.data_as(t)  # noqa: E731
+        return (self.nbf, P(self.origin, _dp), P(self.powers, _i64p), P(self.prim_off, _i64p),
+                P(self.exps, _dp), P(self.coefs, _dp), P(self.pnorms, _dp), P(self.norms, _dp))
+
+    def write(self, path):
+        with open(path, "wb") as f:
+            np.array([self.nbf, len(self.exps)], dtype=np.int64).tofile(f)
+            for a in (self.origin, self.powers, self.prim_off, self.exps, self.coefs, self.pnorms, self.norms):
+                a.tofile(f)
+
+
+def nquartets(nbf):
+    P = nbf * (nbf + 1) // 2
+    return P * (P + 1) // 2
+
+
+def ijkl2intindex(i, j, k, l):
+    if i < j:
+        i, j = j, i
+    if k < l:
+        k, l = l, k
+    ij, kl = i * (i + 1) // 2 + j, k * (k + 1) // 2 + l
+    if ij < kl:
+        ij, kl = kl, ij
+    return ij * (ij + 1) // 2 + kl
+
+
+# -------------------------------------------------------------- integrals --
+def ref_get2ints(bfs, nproc=1):
+    """Every unique (ij|kl) from the reference's compiled Rys engine."""
+    lib = ref_lib("fock")
+    if lib is None:
+        raise RuntimeError("reference not built: make -C oracle ref")
+    t = Table(bfs)
+    out = np.zeros(nquartets(t.nbf))
+    rc = lib.ref_get2ints(*t.args(), out.ctypes.data_as(_dp), nproc)
+    if rc != 0:
+        raise RuntimeError("ref_get2ints failed (%d)" % rc)
+    return out
+
+
+def _carr(x):
+    return (ctypes.c_double * len(x))(*x)
+
+
+def ref_contr(a, b, c, d):
+    """CGBF.coulomb (PyQuante/CGBF.py:191-199) on the reference's compiled
+    crys.contr_coulomb for one function quartet."""
+    crys = ref_lib("crys")
+    args = []
+    for f in (a, b, c, d):
+        args += [len(f.pexps), _carr(f.pexps), _carr(f.pcoefs), _carr(f.pnorms), *f.origin, *f.powers]
+    return crys.contr_coulomb(*args) * a.norm * b.norm * c.norm * d.norm
+
+
+def orc_contr(a, b, c, d):
+    """The same quartet from this project's C restatement (HGP)."""
+    t = Table([a, b, c, d])
+    out = np.zeros(nquartets(4))
+    oracle_lib().orc_get2ints(*t.args(), out.ctypes.data_as(_dp))
+    return out[ijkl2intindex(0, 1, 2, 3)]
+
+
+def orc_get2ints(bfs):
+    """Every unique (ij|kl) from this project's C restatement (HGP)."""
+    t = Table(bfs)
+    out = np.zeros(nquartets(t.nbf))
+    oracle_lib().orc_get2ints(*t.args(), out.ctypes.data_as(_dp))
+    return out
+
+
+def orc_get1ints(bfs, atoms):
+    t = Table(bfs)
+    n = t.nbf
+    S = np.zeros((n, n))
+    h = np.zeros((n, n))
+    xyz = np.ascontiguousarray([p for _, p in atoms], dtype=np.float64).reshape(-1)
+    z = np.array([float(zz) for zz, _ in atoms])
+    oracle_lib().orc_get1ints(*t.args(), len(atoms), xyz.ctypes.data_as(_dp), z.ctypes.data_as(_dp),
+                              S.ctypes.data_as(_dp), h.ctypes.data_as(_dp))
+    return S, h
+
+
+def ref_get1ints(bfs, atoms):
+    """PyQuante/Ints.py:73-87 over the reference's compiled cints
+    (CGBF.overlap/kinetic/nuclear -> PGBF -> cints, PyQuante/PGBF.py:72-99)."""
+    lib = ref_lib("cints")
+    if lib is None:
+        raise RuntimeError("reference not built: make -C oracle ref")
+    n = len(bfs)
+    S = np.zeros((n, n))
+    h = np.zeros((n, n))
+    for i, a in enumerate(bfs):
+        for j, b in enumerate(bfs):
+            s = t = v = 0.0
+            for ea, ca, na in zip(a.pexps, a.pcoefs, a.pnorms):
+                for eb, cb, nb in zip(b.pexps, b.pcoefs, b.pnorms):
+                    s += ca * cb * na * nb * lib.ref_cints_overlap(ea, *a.powers, *a.origin, eb, *b.powers, *b.origin)
+                    t += ca * cb * na * nb * lib.ref_cints_kinetic(ea, *a.powers, *a.origin, eb, *b.powers, *b.origin)
+                    for z, c in atoms:
+                        v += z * ca * cb * lib.ref_cints_nuclear(*a.origin, na, *a.powers, ea,
+                                                                 *b.origin, nb, *b.powers, eb, *c)
+            S[i, j] = a.norm * b.norm * s
+            h[i, j] = a.norm * b.norm * (t + v)
+    return S, h
+
+
+def unpack(ints, nbf):
+    """Full (n,n,n,n) tensor from the packed array (small n only)."""
+    idx = np.zeros((nbf, nbf, nbf, nbf), dtype=np.int64)
+    r = np.arange(nbf)
+    i, j, k, l = np.meshgrid(r, r, r, r, indexing="ij")
+    a, b = np.maximum(i, j), np.minimum(i, j)
+    c, d = np.maximum(k, l), np.minimum(k, l)
+    ij, kl = a * (a + 1) // 2 + b, c * (c + 1) // 2 + d
+    hi, lo = np.maximum(ij, kl), np.minimum(ij, kl)
+    idx[...] = hi * (hi + 1) // 2 + lo
+    return np.asarray(ints)[idx]
+
+
+def getJK(ints, D):
+    """J_ij = sum_kl (ij|kl) D_kl, K_ij = sum_kl (ik|jl) D_kl (PyQuante/Ints.py:195-223)."""
+    n = D.shape[0]
+    full = unpack(ints, n)
+    J = np.einsum("ijkl,kl->ij", full, D)
+    K = np.einsum("ikjl,kl->ij", full, D)
+    return J, K
+
+
+def get2JmK(ints, D):
+    J, K = getJK(ints, D)
+    return 2 * J - K
+
+
+# -------------------------------------------------------------------- SCF --
+def geigh(H, S):
+    X = np.linalg.inv(np.linalg.cholesky(S)).T
+    e, v = np.linalg.eigh(X.T @ H @ X)
+    return e, X @ v
+
+
+def enuke(atoms):
+    e = 0.0
+    for i, (zi, ri) in enumerate(atoms):
+        for zj, rj in atoms[:i]:
+            e += zi * zj / np.linalg.norm(np.subtract(ri, rj))
+    return e
+
+
+def rhf(atoms, S, h, ints, nclosed, conv=1e-10, maxiter=100, diis=False):
+    """PyQuante/hartree_fock.py:66-149 (DIIS per Convergence.py:73-136)."""
+    en = enuke(atoms)
+    orbe, orbs = geigh(h, S)
+    eold = 0.0
+    Fs, Es = [], []
+    energy = 0.0
+    for _ in range(maxiter):
+        D = orbs[:, :nclosed] @ orbs[:, :nclosed].T
+        F = h + get2JmK(ints, D)
+        if diis:
+            err = (F @ D @ S - S @ D @ F).ravel()
+            Fs.append(F)
+            Es.append(err)
+            m = len(Es)
+            a = np.zeros((m + 1, m + 1))
+            a[:m, :m] = np.array(Es) @ np.array(Es).T
+            a[m, :m] = a[:m, m] = -1.0
+            b = np.zeros(m + 1)
+            b[m] = -1.0
+            c = np.linalg.solve(a, b)
+            F = sum(c[i] * Fs[i] for i in range(m))
+        orbe, orbs = geigh(F, S)
+        energy = float((D * h).sum() + (D * F).sum() + en)
+        if abs(energy - eold) < conv:
+            break
+        eold = energy
+    return energy, orbe, orbs

@@ -1,0 +1,16 @@
+// Direct J/K instantiations of the ERI engine with FP32 recurrences and
+// contraction (roots, weights and prefactors in FP64; digestion into J/K in
+// FP64).  Used only for quartets whose Schwarz bound is below the mixed-
+// precision threshold.
+#include "eri_engine.cuh"
+#include "eri_launch.h"
+
+namespace pqb {
+cudaError_t launch_jk_f32(int qc, const int2 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+                          const double *D, double *Jacc, double *Kacc, const double *fscale, int n,
+                          cudaStream_t st, int nsm)
+{
+    EpiJK epi{D, Jacc, Kacc, fscale, n};
+    return launch_eri<float>(qc, list, nq, pairs, prims, epi, st, nsm);
+}
+}  // namespace pqb

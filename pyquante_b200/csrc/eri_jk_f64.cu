@@ -1,0 +1,13 @@
+// Direct J/K instantiations of the ERI engine (FP64 integrals).
+#include "eri_engine.cuh"
+#include "eri_launch.h"
+
+namespace pqb {
+cudaError_t launch_jk_f64(int qc, const int2 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+                          const double *D, double *Jacc, double *Kacc, const double *fscale, int n,
+                          cudaStream_t st, int nsm)
+{
+    EpiJK epi{D, Jacc, Kacc, fscale, n};
+    return launch_eri<double>(qc, list, nq, pairs, prims, epi, st, nsm);
+}
+}  // namespace pqb

@@ -1,0 +1,980 @@
+// C ABI of the engine (declared in include/pyquante_b200.h): context,
+// shell/pair tables, quartet planning, and the kernels that are not
+// class-templated (general-L scalar ERIs by Rys and by Head-Gordon--Pople,
+// one-electron integrals, stored-integral J/K, Boys/Rys probes).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#define PQB_TABQ static __device__ const
+#define PQB_CTABQ static __constant__ const
+#include "../../include/pyquante_b200.h"
+#include "eri_launch.h"
+#include "pqb_device.cuh"
+#include "pqb_types.h"
+
+using namespace pqb;
+
+struct pqb_ctx {
+    int device = 0;
+    int nsm = 148;
+    std::string err;
+    // basis
+    int nbf = 0, nshell = 0;
+    std::vector<int> sh_l, sh_np, sh_off, sh_f0;
+    std::vector<double> sh_xyz, pr_exp, pr_coef, fscale_h;
+    // device tables
+    PairInfo *d_pairs = nullptr;
+    PrimPair *d_prims = nullptr;
+    double *d_fscale = nullptr;
+    unsigned long long *d_q2 = nullptr;
+    std::vector<PairInfo> pairs;
+    std::vector<double> Q;           // Schwarz factors (host)
+    bool have_q = false;
+    // unscreened lists (packed integrals): per class offset/count into d_full
+    int2 *d_full = nullptr;
+    int64_t full_off[kNumQuartetClass] = {0}, full_cnt[kNumQuartetClass] = {0};
+    // Schwarz (diagonal) list
+    int2 *d_diag = nullptr;
+    int64_t diag_off[kNumQuartetClass] = {0}, diag_cnt[kNumQuartetClass] = {0};
+    // screened plan: [0] FP64 part, [1] FP32-eligible part
+    int2 *d_plan = nullptr;
+    size_t plan_cap = 0;
+    int64_t plan_off[2][kNumQuartetClass] = {{0}}, plan_cnt[2][kNumQuartetClass] = {{0}};
+    int64_t plan_prims[2][kNumQuartetClass] = {{0}};
+    std::vector<int2> plan_h;        // host copy of the plan (for sharding)
+    bool have_plan = false;
+    // small scratch
+    double *d_atoms = nullptr;
+    size_t atoms_cap = 0;
+};
+
+static int fail(pqb_ctx *ctx, int code, const char *fmt, ...)
+{
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        ctx->err = buf;
+    }
+    return code;
+}
+
+#define PQB_CK(ctx, call)                                                                              \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return fail(ctx, PQB_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+static void free_dev(void *p)
+{
+    if (p) cudaFree(p);
+}
+
+// ===================================================================== kernels
+
+// In-place M = M + M^T (the J/K accumulators hold one triangle's worth of
+// each unique contribution; see EpiJK).
+__global__ void symmetrize_kernel(double *M, int n)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t P = (int64_t)n * (n + 1) / 2;
+    if (t >= P) return;
+    int i = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((int64_t)i * (i + 1) / 2 > t) --i;
+    while ((int64_t)(i + 1) * (i + 2) / 2 <= t) ++i;
+    int j = (int)(t - (int64_t)i * (i + 1) / 2);
+    double s = M[(int64_t)i * n + j] + M[(int64_t)j * n + i];
+    M[(int64_t)i * n + j] = s;
+    M[(int64_t)j * n + i] = s;
+}
+
+__device__ __forceinline__ double binom_d(int n, int k)
+{
+    double r = 1.0;
+    for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+    return r;
+}
+
+// ---- general-L Rys: one thread per function quartet (crys.contr_coulomb
+// semantics, Src/crys.c:34-97; the 2-D recursion of ABD eqs 11-16 and the
+// binomial transfer of Src/crys.c:1518-1534, in t^2 form).
+__device__ double rys_axis_general(double u, double zeta, double eta, double PA, double QC, double PQ, double AB,
+                                   double CD, int la, int lb, int lc, int ld)
+{
+    const int NB = la + lb, MK = lc + ld;
+    double G[10][10];
+    const double zpe = zeta + eta;
+    const double b00 = 0.5 * u / zpe, b10 = (0.5 - 0.5 * eta / zpe * u) / zeta, b01 = (0.5 - 0.5 * zeta / zpe * u) / eta;
+    const double c00 = PA - eta / zpe * u * PQ, c01 = QC + zeta / zpe * u * PQ;
+    G[0][0] = 1.0;
+    if (NB > 0) G[1][0] = c00;
+    for (int n = 1; n < NB; ++n) G[n + 1][0] = n * b10 * G[n - 1][0] + c00 * G[n][0];
+    for (int n = 0; n <= NB; ++n) {
+        if (MK > 0) G[n][1] = c01 * G[n][0] + (n > 0 ? n * b00 * G[n - 1][0] : 0.0);
+        for (int m = 1; m < MK; ++m)
+            G[n][m + 1] = m * b01 * G[n][m - 1] + c01 * G[n][m] + (n > 0 ? n * b00 * G[n - 1][m] : 0.0);
+    }
+    double s = 0.0;
+    for (int p = 0; p <= lb; ++p) {
+        double sp = 0.0;
+        for (int q = 0; q <= ld; ++q) sp += binom_d(ld, q) * pow(CD, ld - q) * G[la + p][lc + q];
+        s += binom_d(lb, p) * pow(AB, lb - p) * sp;
+    }
+    return s;
+}
+
+struct FuncTable {
+    const double *origin;
+    const int *powers;
+    const int *prim_off;
+    const double *exps, *cn, *norms;
+};
+
+__global__ void eri_general_rys_kernel(int nq, const int *__restrict__ quartets, FuncTable ft, double *out)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    int f[4];
+    for (int x = 0; x < 4; ++x) f[x] = quartets[4 * q + x];
+    int L = 0;
+    for (int x = 0; x < 4; ++x) L += ft.powers[3 * f[x]] + ft.powers[3 * f[x] + 1] + ft.powers[3 * f[x] + 2];
+    if (L > 9) {   // beyond the 5-root tables (the host rejects these first)
+        out[q] = nan("");
+        return;
+    }
+    const int nr = L / 2 + 1;
+    const double *A = ft.origin + 3 * f[0], *B = ft.origin + 3 * f[1], *C = ft.origin + 3 * f[2], *D = ft.origin + 3 * f[3];
+    double sum = 0.0;
+    for (int p = ft.prim_off[f[0]]; p < ft.prim_off[f[0] + 1]; ++p)
+        for (int qq = ft.prim_off[f[1]]; qq < ft.prim_off[f[1] + 1]; ++qq) {
+            const double a = ft.exps[p], b = ft.exps[qq], zeta = a + b;
+            double P[3], rab2 = 0.0;
+            for (int x = 0; x < 3; ++x) {
+                P[x] = (a * A[x] + b * B[x]) / zeta;
+                rab2 += (A[x] - B[x]) * (A[x] - B[x]);
+            }
+            const double Kab = ft.cn[p] * ft.cn[qq] * kPairPre / zeta * exp(-a * b / zeta * rab2);
+            for (int r = ft.prim_off[f[2]]; r < ft.prim_off[f[2] + 1]; ++r)
+                for (int s = ft.prim_off[f[3]]; s < ft.prim_off[f[3] + 1]; ++s) {
+                    const double c = ft.exps[r], d = ft.exps[s], eta = c + d;
+                    double Qc[3], rcd2 = 0.0, rpq2 = 0.0;
+                    for (int x = 0; x < 3; ++x) {
+                        Qc[x] = (c * C[x] + d * D[x]) / eta;
+                        rcd2 += (C[x] - D[x]) * (C[x] - D[x]);
+                        rpq2 += (P[x] - Qc[x]) * (P[x] - Qc[x]);
+                    }
+                    const double Kcd = ft.cn[r] * ft.cn[s] * kPairPre / eta * exp(-c * d / eta * rcd2);
+                    const double T = zeta * eta / (zeta + eta) * rpq2;
+                    const double pre = Kab * Kcd / sqrt(zeta + eta);
+                    for (int k = 0; k < nr; ++k) {
+                        double u, w;
+                        rys_root(nr, k, T, u, w);
+                        double prod = w * pre;
+                        for (int x = 0; x < 3; ++x)
+                            prod *= rys_axis_general(u, zeta, eta, P[x] - A[x], Qc[x] - C[x], P[x] - Qc[x], A[x] - B[x],
+                                                     C[x] - D[x], ft.powers[3 * f[0] + x], ft.powers[3 * f[1] + x],
+                                                     ft.powers[3 * f[2] + x], ft.powers[3 * f[3] + x]);
+                        sum += prod;
+                    }
+                }
+        }
+    out[q] = ft.norms[f[0]] * ft.norms[f[1]] * ft.norms[f[2]] * ft.norms[f[3]] * sum;
+}
+
+// ---- general-L Head-Gordon--Pople (the scheme of Src/chgp.c:78-419): an
+// Obara--Saika VRR for (e0|f0)^(m), computed bottom-up over the box
+// e' <= a+b, f' <= c+d (componentwise), then the HRR
+// (a,b+1_i|..) = (a+1_i,b|..) + AB_i (a,b|..) applied in closed (binomial)
+// form.  Boys values by table + downward recursion.  Per-side momentum
+// |a|+|b| <= 4 and |c|+|d| <= 4 bound the box to 12 x 12 entries.
+#define PQB_HGP_BOX 12
+__global__ void eri_general_hgp_kernel(int nq, int aux_m, const int *__restrict__ quartets, FuncTable ft, double *out)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    int f[4];
+    for (int x = 0; x < 4; ++x) f[x] = quartets[4 * q + x];
+    int la[3], lb[3], lc[3], ld[3], E[3], F[3];
+    for (int x = 0; x < 3; ++x) {
+        la[x] = ft.powers[3 * f[0] + x];
+        lb[x] = ft.powers[3 * f[1] + x];
+        lc[x] = ft.powers[3 * f[2] + x];
+        ld[x] = ft.powers[3 * f[3] + x];
+        E[x] = la[x] + lb[x];
+        F[x] = lc[x] + ld[x];
+    }
+    const int Es[3] = {1, E[0] + 1, (E[0] + 1) * (E[1] + 1)};
+    const int Fs[3] = {1, F[0] + 1, (F[0] + 1) * (F[1] + 1)};
+    const int nE = (E[0] + 1) * (E[1] + 1) * (E[2] + 1), nF = (F[0] + 1) * (F[1] + 1) * (F[2] + 1);
+    const int M = E[0] + E[1] + E[2] + F[0] + F[1] + F[2] + aux_m;
+    if (nE > PQB_HGP_BOX || nF > PQB_HGP_BOX || M > 8 || aux_m < 0) {   // outside the box (the host rejects these first)
+        out[q] = nan("");
+        return;
+    }
+    double V[PQB_HGP_BOX * PQB_HGP_BOX * 9];   // [e][f][m], m <= 8
+    const double *A = ft.origin + 3 * f[0], *B = ft.origin + 3 * f[1], *C = ft.origin + 3 * f[2], *D = ft.origin + 3 * f[3];
+    double sum = 0.0;
+    for (int p = ft.prim_off[f[0]]; p < ft.prim_off[f[0] + 1]; ++p)
+        for (int p2 = ft.prim_off[f[1]]; p2 < ft.prim_off[f[1] + 1]; ++p2)
+            for (int r = ft.prim_off[f[2]]; r < ft.prim_off[f[2] + 1]; ++r)
+                for (int s = ft.prim_off[f[3]]; s < ft.prim_off[f[3] + 1]; ++s) {
+                    const double a = ft.exps[p], b = ft.exps[p2], c = ft.exps[r], d = ft.exps[s];
+                    const double zeta = a + b, eta = c + d, ze = zeta + eta;
+                    double PA[3], QC[3], WP[3], WQ[3], rab2 = 0, rcd2 = 0, rpq2 = 0;
+                    for (int x = 0; x < 3; ++x) {
+                        const double P = (a * A[x] + b * B[x]) / zeta, Qx = (c * C[x] + d * D[x]) / eta;
+                        const double W = (zeta * P + eta * Qx) / ze;
+                        PA[x] = P - A[x];
+                        QC[x] = Qx - C[x];
+                        WP[x] = W - P;
+                        WQ[x] = W - Qx;
+                        rab2 += (A[x] - B[x]) * (A[x] - B[x]);
+                        rcd2 += (C[x] - D[x]) * (C[x] - D[x]);
+                        rpq2 += (P - Qx) * (P - Qx);
+                    }
+                    const double pre = ft.cn[p] * ft.cn[p2] * ft.cn[r] * ft.cn[s] * 2.0 * pow(kPi, 2.5) /
+                                       (zeta * eta * sqrt(ze)) * exp(-a * b / zeta * rab2 - c * d / eta * rcd2);
+                    double Fm[17];
+                    boys_rt(M, zeta * eta / ze * rpq2, Fm);
+                    const double o2z = 0.5 / zeta, o2e = 0.5 / eta, o2ze = 0.5 / ze, rz = eta / ze, re = zeta / ze;
+                    for (int ex = 0; ex <= E[0]; ++ex)
+                        for (int ey = 0; ey <= E[1]; ++ey)
+                            for (int ez = 0; ez <= E[2]; ++ez)
+                                for (int fx = 0; fx <= F[0]; ++fx)
+                                    for (int fy = 0; fy <= F[1]; ++fy)
+                                        for (int fz = 0; fz <= F[2]; ++fz) {
+                                            const int e3[3] = {ex, ey, ez}, f3[3] = {fx, fy, fz};
+                                            const int ie = ex * Es[0] + ey * Es[1] + ez * Es[2];
+                                            const int jf = fx * Fs[0] + fy * Fs[1] + fz * Fs[2];
+                                            const int tot = ex + ey + ez + fx + fy + fz;
+                                            for (int m = 0; m <= M - tot; ++m) {
+                                                double v;
+                                                if (ex + ey + ez > 0) {
+                                                    const int i = ex ? 0 : (ey ? 1 : 2);
+                                                    const int e1 = ie - Es[i];
+                                                    v = PA[i] * V[(e1 * nF + jf) * 9 + m] + WP[i] * V[(e1 * nF + jf) * 9 + m + 1];
+                                                    if (e3[i] > 1) {
+                                                        const int e2 = e1 - Es[i];
+                                                        v += (e3[i] - 1) * o2z *
+                                                             (V[(e2 * nF + jf) * 9 + m] - rz * V[(e2 * nF + jf) * 9 + m + 1]);
+                                                    }
+                                                    if (f3[i] > 0) v += f3[i] * o2ze * V[(e1 * nF + jf - Fs[i]) * 9 + m + 1];
+                                                } else if (fx + fy + fz > 0) {
+                                                    const int i = fx ? 0 : (fy ? 1 : 2);
+                                                    const int f1 = jf - Fs[i];
+                                                    v = QC[i] * V[(ie * nF + f1) * 9 + m] + WQ[i] * V[(ie * nF + f1) * 9 + m + 1];
+                                                    if (f3[i] > 1) {
+                                                        const int f2 = f1 - Fs[i];
+                                                        v += (f3[i] - 1) * o2e *
+                                                             (V[(ie * nF + f2) * 9 + m] - re * V[(ie * nF + f2) * 9 + m + 1]);
+                                                    }
+                                                } else {
+                                                    v = pre * Fm[m];
+                                                }
+                                                V[(ie * nF + jf) * 9 + m] = v;
+                                            }
+                                        }
+                    (void)nE;
+                    // HRR in binomial form: b onto a, d onto c
+                    double s2 = 0.0;
+                    for (int bx = 0; bx <= lb[0]; ++bx)
+                        for (int by = 0; by <= lb[1]; ++by)
+                            for (int bz = 0; bz <= lb[2]; ++bz) {
+                                const double cb = binom_d(lb[0], bx) * binom_d(lb[1], by) * binom_d(lb[2], bz) *
+                                                  pow(A[0] - B[0], lb[0] - bx) * pow(A[1] - B[1], lb[1] - by) *
+                                                  pow(A[2] - B[2], lb[2] - bz);
+                                const int ie = (la[0] + bx) * Es[0] + (la[1] + by) * Es[1] + (la[2] + bz) * Es[2];
+                                for (int dx = 0; dx <= ld[0]; ++dx)
+                                    for (int dy = 0; dy <= ld[1]; ++dy)
+                                        for (int dz = 0; dz <= ld[2]; ++dz) {
+                                            const double cdf = binom_d(ld[0], dx) * binom_d(ld[1], dy) *
+                                                               binom_d(ld[2], dz) * pow(C[0] - D[0], ld[0] - dx) *
+                                                               pow(C[1] - D[1], ld[1] - dy) * pow(C[2] - D[2], ld[2] - dz);
+                                            const int jf =
+                                                (lc[0] + dx) * Fs[0] + (lc[1] + dy) * Fs[1] + (lc[2] + dz) * Fs[2];
+                                            s2 += cb * cdf * V[(ie * nF + jf) * 9 + aux_m];
+                                        }
+                            }
+                    sum += s2;
+                }
+    out[q] = ft.norms[f[0]] * ft.norms[f[1]] * ft.norms[f[2]] * ft.norms[f[3]] * sum;
+}
+
+// ---- one-electron integrals, one thread per (i, j): overlap and kinetic by
+// the Obara--Saika 1-D overlap recursion (the kinetic combination of
+// Src/cints.c:190-213), nuclear attraction by 1-electron Rys quadrature
+// (T = zeta |P-C|^2, n = (li+lj)/2+1 roots).
+__global__ void oneint_kernel(int n, FuncTable ft, int natoms, const double *__restrict__ atoms, double *S, double *Tk,
+                              double *V)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)n * n) return;
+    const int i = (int)(t / n), j = (int)(t % n);
+    const double *A = ft.origin + 3 * i, *B = ft.origin + 3 * j;
+    int li[3], lj[3];
+    for (int x = 0; x < 3; ++x) {
+        li[x] = ft.powers[3 * i + x];
+        lj[x] = ft.powers[3 * j + x];
+    }
+    const int Ltot = li[0] + li[1] + li[2] + lj[0] + lj[1] + lj[2];
+    if (li[0] + li[1] + li[2] > 3 || lj[0] + lj[1] + lj[2] > 3) {   // f at most (the host rejects these first)
+        if (S) S[t] = nan("");
+        if (Tk) Tk[t] = nan("");
+        if (V) V[t] = nan("");
+        return;
+    }
+    double s_sum = 0, t_sum = 0, v_sum = 0;
+    for (int p = ft.prim_off[i]; p < ft.prim_off[i + 1]; ++p)
+        for (int q = ft.prim_off[j]; q < ft.prim_off[j + 1]; ++q) {
+            const double a = ft.exps[p], b = ft.exps[q], g = a + b;
+            double P[3], rab2 = 0;
+            for (int x = 0; x < 3; ++x) {
+                P[x] = (a * A[x] + b * B[x]) / g;
+                rab2 += (A[x] - B[x]) * (A[x] - B[x]);
+            }
+            const double E = exp(-a * b / g * rab2);
+            const double w = ft.cn[p] * ft.cn[q];
+            // 1-D overlaps S_x[u][v], u <= li_x, v <= lj_x + 2
+            double Sx[3][7][9];
+            for (int x = 0; x < 3; ++x) {
+                const double pa = P[x] - A[x], pb = P[x] - B[x], o2g = 0.5 / g;
+                const int U = li[x], W = lj[x] + 2;
+                Sx[x][0][0] = 1.0;
+                for (int v = 0; v < W; ++v)
+                    Sx[x][0][v + 1] = pb * Sx[x][0][v] + (v > 0 ? v * o2g * Sx[x][0][v - 1] : 0.0);
+                for (int u = 0; u < U; ++u)
+                    for (int v = 0; v <= W; ++v)
+                        Sx[x][u + 1][v] = pa * Sx[x][u][v] + (u > 0 ? u * o2g * Sx[x][u - 1][v] : 0.0) +
+                                          (v > 0 ? v * o2g * Sx[x][u][v - 1] : 0.0);
+            }
+            const double pre = pow(kPi / g, 1.5) * E;
+            auto ov = [&](int dx, int dy, int dz) {
+                return Sx[0][li[0]][lj[0] + dx] * Sx[1][li[1]][lj[1] + dy] * Sx[2][li[2]][lj[2] + dz];
+            };
+            const double s0 = ov(0, 0, 0);
+            const int Lj = lj[0] + lj[1] + lj[2];
+            double tk = b * (2 * Lj + 3) * s0 - 2.0 * b * b * (ov(2, 0, 0) + ov(0, 2, 0) + ov(0, 0, 2));
+            if (lj[0] >= 2) tk -= 0.5 * lj[0] * (lj[0] - 1) * ov(-2, 0, 0);
+            if (lj[1] >= 2) tk -= 0.5 * lj[1] * (lj[1] - 1) * ov(0, -2, 0);
+            if (lj[2] >= 2) tk -= 0.5 * lj[2] * (lj[2] - 1) * ov(0, 0, -2);
+            s_sum += w * pre * s0;
+            t_sum += w * pre * tk;
+            if (V) {
+                const int nr = Ltot / 2 + 1;
+                double vv = 0.0;
+                for (int c = 0; c < natoms; ++c) {
+                    const double *Cn = atoms + 4 * c;
+                    double pc2 = 0;
+                    for (int x = 0; x < 3; ++x) pc2 += (P[x] - Cn[x]) * (P[x] - Cn[x]);
+                    const double T = g * pc2;
+                    double acc = 0.0;
+                    for (int r = 0; r < nr; ++r) {
+                        double u, wr;
+                        rys_root(nr, r, T, u, wr);
+                        double prod = wr;
+                        for (int x = 0; x < 3; ++x) {
+                            const double c00 = (P[x] - A[x]) - u * (P[x] - Cn[x]), b10 = 0.5 * (1.0 - u) / g;
+                            const int NB = li[x] + lj[x];
+                            double G[8];
+                            G[0] = 1.0;
+                            if (NB > 0) G[1] = c00;
+                            for (int k = 1; k < NB; ++k) G[k + 1] = k * b10 * G[k - 1] + c00 * G[k];
+                            double sx = 0.0;
+                            for (int pp = 0; pp <= lj[x]; ++pp)
+                                sx += binom_d(lj[x], pp) * pow(A[x] - B[x], lj[x] - pp) * G[li[x] + pp];
+                            prod *= sx;
+                        }
+                        acc += prod;
+                    }
+                    vv -= Cn[3] * acc;
+                }
+                v_sum += w * 2.0 * kPi / g * E * vv;
+            }
+        }
+    const double nn = ft.norms[i] * ft.norms[j];
+    if (S) S[t] = nn * s_sum;
+    if (Tk) Tk[t] = nn * t_sum;
+    if (V) V[t] = nn * v_sum;
+}
+
+// ---- stored-integral J/K: one block per packed bra row IJ (i >= j); the row
+// holds (ij|kl) for every kl <= ij, contiguous.  Same unique-quartet
+// digestion as EpiJK.
+__global__ void jk_packed_kernel(const double *__restrict__ ints, const double *__restrict__ D, double *Jacc,
+                                 double *Kacc, int n)
+{
+    const int64_t IJ = blockIdx.x;
+    int i = (int)((sqrt(8.0 * (double)IJ + 1.0) - 1.0) * 0.5);
+    while ((int64_t)i * (i + 1) / 2 > IJ) --i;
+    while ((int64_t)(i + 1) * (i + 2) / 2 <= IJ) ++i;
+    const int j = (int)(IJ - (int64_t)i * (i + 1) / 2);
+    const double *row = ints + IJ * (IJ + 1) / 2;
+    const double Dij = D[(int64_t)i * n + j];
+    double jij = 0.0;
+    for (int64_t KL = threadIdx.x; KL <= IJ; KL += blockDim.x) {
+        int k = (int)((sqrt(8.0 * (double)KL + 1.0) - 1.0) * 0.5);
+        while ((int64_t)k * (k + 1) / 2 > KL) --k;
+        while ((int64_t)(k + 1) * (k + 2) / 2 <= KL) ++k;
+        const int l = (int)(KL - (int64_t)k * (k + 1) / 2);
+        const double v = row[KL] * (i == j ? 0.5 : 1.0) * (k == l ? 0.5 : 1.0) * (IJ == KL ? 0.5 : 1.0);
+        jij += v * D[(int64_t)k * n + l];
+        atomicAdd(Jacc + (int64_t)k * n + l, 2.0 * v * Dij);
+        atomicAdd(Kacc + (int64_t)i * n + k, v * D[(int64_t)j * n + l]);
+        atomicAdd(Kacc + (int64_t)i * n + l, v * D[(int64_t)j * n + k]);
+        atomicAdd(Kacc + (int64_t)j * n + k, v * D[(int64_t)i * n + l]);
+        atomicAdd(Kacc + (int64_t)j * n + l, v * D[(int64_t)i * n + k]);
+    }
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) jij += __shfl_down_sync(0xffffffffu, jij, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = jij;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        atomicAdd(Jacc + (int64_t)i * n + j, 2.0 * s);
+    }
+}
+
+__global__ void boys_eval_kernel(int m, int count, const double *T, double *F)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    double f[17];
+    boys_rt(m, T[t], f);
+    for (int k = 0; k <= m; ++k) F[(int64_t)t * (m + 1) + k] = f[k];
+}
+
+__global__ void rys_eval_kernel(int nr, int count, const double *T, double *u, double *w)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    for (int r = 0; r < nr; ++r) rys_root(nr, r, T[t], u[(int64_t)t * nr + r], w[(int64_t)t * nr + r]);
+}
+
+// FP64 FMA probe: 8 independent chains per thread keep the DFMA pipe full.
+__global__ void dfma_probe_kernel(int iters, double *sink)
+{
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = threadIdx.x * 1e-3 + k;
+    const double b = 0.999999, c = 1e-9;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fma(a[k], b, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k];
+    if (s == 12345.678) sink[0] = s;   // never true; keeps the chains live
+}
+
+__global__ void finalize_q_kernel(const unsigned long long *q2, double *Q, int np)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < np) Q[t] = sqrt(__longlong_as_double((long long)q2[t]));
+}
+
+// ====================================================================== host
+
+static inline int64_t pair_idx64(int64_t i, int64_t j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
+
+extern "C" {
+
+int pqb_version(void) { return 1; }
+
+int64_t pqb_ijkl2intindex(int64_t i, int64_t j, int64_t k, int64_t l)
+{
+    int64_t ij = pair_idx64(i, j), kl = pair_idx64(k, l);
+    return ij >= kl ? ij * (ij + 1) / 2 + kl : kl * (kl + 1) / 2 + ij;
+}
+
+int pqb_create(pqb_ctx **out, int device)
+{
+    if (!out) return PQB_E_ARG;
+    *out = nullptr;
+    pqb_ctx *ctx = new pqb_ctx();
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return PQB_E_CUDA;
+    }
+    cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device);
+    *out = ctx;
+    return PQB_OK;
+}
+
+static void release_basis(pqb_ctx *ctx)
+{
+    free_dev(ctx->d_pairs);
+    free_dev(ctx->d_prims);
+    free_dev(ctx->d_fscale);
+    free_dev(ctx->d_q2);
+    free_dev(ctx->d_full);
+    free_dev(ctx->d_diag);
+    free_dev(ctx->d_plan);
+    ctx->d_pairs = nullptr;
+    ctx->d_prims = nullptr;
+    ctx->d_fscale = nullptr;
+    ctx->d_q2 = nullptr;
+    ctx->d_full = ctx->d_diag = ctx->d_plan = nullptr;
+    ctx->plan_cap = 0;
+    ctx->have_q = ctx->have_plan = false;
+}
+
+void pqb_destroy(pqb_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    release_basis(ctx);
+    free_dev(ctx->d_atoms);
+    delete ctx;
+}
+
+int pqb_last_error(const pqb_ctx *ctx, char *buf, size_t len)
+{
+    if (!ctx || !buf || len == 0) return PQB_E_ARG;
+    snprintf(buf, len, "%s", ctx->err.c_str());
+    return PQB_OK;
+}
+
+int pqb_num_pairs(const pqb_ctx *ctx) { return ctx ? (int)ctx->pairs.size() : 0; }
+
+// Bucket quartet (bra, ket) lists by class, each class sorted by descending
+// primitive-quartet count (block-mode kernels advance their quartets in
+// lockstep over primitive quartets).
+static void bucket_sorted(const std::vector<PairInfo> &pairs, std::vector<std::vector<int2>> &cls,
+                          std::vector<int2> &flat, int64_t *off, int64_t *cnt)
+{
+    flat.clear();
+    for (int c = 0; c < kNumQuartetClass; ++c) {
+        auto &v = cls[c];
+        int maxp = 1;
+        for (auto &e : v) maxp = std::max(maxp, pairs[e.x].nprim * pairs[e.y].nprim);
+        std::vector<int64_t> hist(maxp + 2, 0);
+        for (auto &e : v) hist[maxp - pairs[e.x].nprim * pairs[e.y].nprim]++;
+        int64_t s = 0;
+        for (auto &h : hist) {
+            int64_t t = h;
+            h = s;
+            s += t;
+        }
+        std::vector<int2> sorted(v.size());
+        for (auto &e : v) sorted[hist[maxp - pairs[e.x].nprim * pairs[e.y].nprim]++] = e;
+        off[c] = (int64_t)flat.size();
+        cnt[c] = (int64_t)sorted.size();
+        flat.insert(flat.end(), sorted.begin(), sorted.end());
+    }
+}
+
+static inline int2 oriented_quartet(const std::vector<PairInfo> &pairs, int p, int q, int &qc)
+{
+    int cp = pairs[p].cls, cq = pairs[q].cls;
+    if (cp < cq) {
+        std::swap(p, q);
+        std::swap(cp, cq);
+    }
+    qc = quartet_class(cp, cq);
+    return make_int2(p, q);
+}
+
+int pqb_shells_upload(pqb_ctx *ctx, int nshell, const int *shell_l, const int *shell_nprim, const int *prim_off,
+                      const int *shell_f0, const double *shell_xyz, const double *prim_exp, const double *prim_coef,
+                      int nbf, const double *fscale)
+{
+    if (!ctx || nshell <= 0 || !shell_l || !shell_nprim || !prim_off || !shell_f0 || !shell_xyz || !prim_exp ||
+        !prim_coef || !fscale || nbf <= 0)
+        return fail(ctx, PQB_E_ARG, "pqb_shells_upload: bad arguments");
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    release_basis(ctx);
+    int nf = 0;
+    for (int s = 0; s < nshell; ++s) {
+        if (shell_l[s] < 0 || shell_l[s] > kMaxL)
+            return fail(ctx, PQB_E_CLASS, "shell %d: angular momentum %d > %d (s, p, d supported)", s, shell_l[s],
+                        kMaxL);
+        if (shell_nprim[s] <= 0 || shell_nprim[s] > 64)
+            return fail(ctx, PQB_E_NPRIM, "shell %d: %d primitives (1..64 supported)", s, shell_nprim[s]);
+        if (shell_f0[s] != nf) return fail(ctx, PQB_E_SHAPE, "shell %d: functions not consecutive", s);
+        nf += ncart(shell_l[s]);
+    }
+    if (nf != nbf) return fail(ctx, PQB_E_SHAPE, "shells cover %d functions, nbf = %d", nf, nbf);
+    ctx->nbf = nbf;
+    ctx->nshell = nshell;
+    // pairs
+    std::vector<PairInfo> pairs;
+    std::vector<PrimPair> prims;
+    pairs.reserve((size_t)nshell * (nshell + 1) / 2);
+    for (int a = 0; a < nshell; ++a)
+        for (int b = 0; b <= a; ++b) {
+            int s1 = a, s2 = b;
+            if (shell_l[s2] > shell_l[s1]) std::swap(s1, s2);
+            PairInfo pi{};
+            const double *A = shell_xyz + 3 * s1, *B = shell_xyz + 3 * s2;
+            double r2 = 0;
+            for (int x = 0; x < 3; ++x) {
+                pi.A[x] = A[x];
+                pi.AB[x] = A[x] - B[x];
+                r2 += pi.AB[x] * pi.AB[x];
+            }
+            pi.prim_off = (int)prims.size();
+            for (int p = prim_off[s1]; p < prim_off[s1] + shell_nprim[s1]; ++p)
+                for (int q = prim_off[s2]; q < prim_off[s2] + shell_nprim[s2]; ++q) {
+                    const double al = prim_exp[p], be = prim_exp[q], z = al + be;
+                    const double e = exp(-al * be / z * r2);
+                    // keep unless the pair's overlap weight is below 1e-20
+                    if (fabs(prim_coef[p] * prim_coef[q]) * e * pow(kPi / z, 1.5) < 1e-20) continue;
+                    PrimPair pp{};
+                    pp.zeta = z;
+                    for (int x = 0; x < 3; ++x) pp.P[x] = (al * A[x] + be * B[x]) / z;
+                    pp.K = prim_coef[p] * prim_coef[q] * kPairPre / z * e;
+                    prims.push_back(pp);
+                }
+            pi.nprim = (int)prims.size() - pi.prim_off;
+            pi.fa = shell_f0[s1];
+            pi.fb = shell_f0[s2];
+            pi.sa = s1;
+            pi.sb = s2;
+            pi.la = shell_l[s1];
+            pi.lb = shell_l[s2];
+            pi.cls = pair_class(pi.la, pi.lb);
+            pairs.push_back(pi);
+        }
+    if (prims.empty()) prims.push_back(PrimPair{});
+    ctx->pairs = pairs;
+    const int np = (int)pairs.size();
+    PQB_CK(ctx, cudaMalloc(&ctx->d_pairs, sizeof(PairInfo) * np));
+    PQB_CK(ctx, cudaMalloc(&ctx->d_prims, sizeof(PrimPair) * prims.size()));
+    PQB_CK(ctx, cudaMalloc(&ctx->d_fscale, sizeof(double) * nbf));
+    PQB_CK(ctx, cudaMalloc(&ctx->d_q2, sizeof(unsigned long long) * np));
+    PQB_CK(ctx, cudaMemcpy(ctx->d_pairs, pairs.data(), sizeof(PairInfo) * np, cudaMemcpyHostToDevice));
+    PQB_CK(ctx, cudaMemcpy(ctx->d_prims, prims.data(), sizeof(PrimPair) * prims.size(), cudaMemcpyHostToDevice));
+    PQB_CK(ctx, cudaMemcpy(ctx->d_fscale, fscale, sizeof(double) * nbf, cudaMemcpyHostToDevice));
+    // unscreened quartet list (packed integrals) and diagonal list (Schwarz)
+    std::vector<std::vector<int2>> cls(kNumQuartetClass), dcls(kNumQuartetClass);
+    for (int p = 0; p < np; ++p) {
+        int qc;
+        dcls[quartet_class(pairs[p].cls, pairs[p].cls)].push_back(make_int2(p, p));
+        for (int q = 0; q <= p; ++q) {
+            int2 e = oriented_quartet(pairs, p, q, qc);
+            cls[qc].push_back(e);
+        }
+    }
+    std::vector<int2> flat;
+    bucket_sorted(pairs, cls, flat, ctx->full_off, ctx->full_cnt);
+    PQB_CK(ctx, cudaMalloc(&ctx->d_full, sizeof(int2) * std::max<size_t>(flat.size(), 1)));
+    PQB_CK(ctx, cudaMemcpy(ctx->d_full, flat.data(), sizeof(int2) * flat.size(), cudaMemcpyHostToDevice));
+    bucket_sorted(pairs, dcls, flat, ctx->diag_off, ctx->diag_cnt);
+    PQB_CK(ctx, cudaMalloc(&ctx->d_diag, sizeof(int2) * std::max<size_t>(flat.size(), 1)));
+    PQB_CK(ctx, cudaMemcpy(ctx->d_diag, flat.data(), sizeof(int2) * flat.size(), cudaMemcpyHostToDevice));
+    return PQB_OK;
+}
+
+int pqb_schwarz(pqb_ctx *ctx, double *Q_host, void *stream)
+{
+    if (!ctx) return PQB_E_ARG;
+    if (!ctx->d_pairs) return fail(ctx, PQB_E_STATE, "pqb_schwarz: no basis uploaded");
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const int np = (int)ctx->pairs.size();
+    PQB_CK(ctx, cudaMemsetAsync(ctx->d_q2, 0, sizeof(unsigned long long) * np, st));
+    for (int c = 0; c < kNumQuartetClass; ++c)
+        PQB_CK(ctx, launch_schwarz_f64(c, ctx->d_diag + ctx->diag_off[c], (int)ctx->diag_cnt[c], ctx->d_pairs,
+                                       ctx->d_prims, ctx->d_q2, ctx->d_fscale, st, ctx->nsm));
+    double *dQ = nullptr;
+    PQB_CK(ctx, cudaMalloc(&dQ, sizeof(double) * np));
+    finalize_q_kernel<<<(np + 255) / 256, 256, 0, st>>>(ctx->d_q2, dQ, np);
+    ctx->Q.assign(np, 0.0);
+    cudaError_t e = cudaMemcpyAsync(ctx->Q.data(), dQ, sizeof(double) * np, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(dQ);
+    if (e != cudaSuccess) return fail(ctx, PQB_E_CUDA, "pqb_schwarz: %s", cudaGetErrorString(e));
+    ctx->have_q = true;
+    if (Q_host) memcpy(Q_host, ctx->Q.data(), sizeof(double) * np);
+    return PQB_OK;
+}
+
+int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *counts)
+{
+    if (!ctx) return PQB_E_ARG;
+    if (!ctx->have_q) return fail(ctx, PQB_E_STATE, "pqb_plan: call pqb_schwarz first");
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    const auto &pairs = ctx->pairs;
+    const auto &Q = ctx->Q;
+    const int np = (int)pairs.size();
+    std::vector<std::vector<int2>> c64(kNumQuartetClass), c32(kNumQuartetClass);
+    int64_t total = 0, dropped = 0;
+    for (int p = 0; p < np; ++p) {
+        total += p + 1;
+        for (int q = 0; q <= p; ++q) {
+            const double b = Q[p] * Q[q];
+            if (b < schwarz_thresh) {
+                ++dropped;
+                continue;
+            }
+            int qc;
+            int2 e = oriented_quartet(pairs, p, q, qc);
+            (b < fp32_thresh ? c32 : c64)[qc].push_back(e);
+        }
+    }
+    std::vector<int2> f64, f32;
+    bucket_sorted(pairs, c64, f64, ctx->plan_off[0], ctx->plan_cnt[0]);
+    bucket_sorted(pairs, c32, f32, ctx->plan_off[1], ctx->plan_cnt[1]);
+    for (int c = 0; c < kNumQuartetClass; ++c) ctx->plan_off[1][c] += (int64_t)f64.size();
+    const size_t need = f64.size() + f32.size();
+    if (need > ctx->plan_cap) {
+        free_dev(ctx->d_plan);
+        ctx->d_plan = nullptr;
+        PQB_CK(ctx, cudaMalloc(&ctx->d_plan, sizeof(int2) * std::max<size_t>(need, 1)));
+        ctx->plan_cap = need;
+    }
+    if (!f64.empty())
+        PQB_CK(ctx, cudaMemcpy(ctx->d_plan, f64.data(), sizeof(int2) * f64.size(), cudaMemcpyHostToDevice));
+    if (!f32.empty())
+        PQB_CK(ctx, cudaMemcpy(ctx->d_plan + f64.size(), f32.data(), sizeof(int2) * f32.size(), cudaMemcpyHostToDevice));
+    ctx->plan_h = f64;
+    ctx->plan_h.insert(ctx->plan_h.end(), f32.begin(), f32.end());
+    for (int part = 0; part < 2; ++part)
+        for (int c = 0; c < kNumQuartetClass; ++c) {
+            int64_t s = 0;
+            for (int64_t q = 0; q < ctx->plan_cnt[part][c]; ++q) {
+                const int2 e = ctx->plan_h[ctx->plan_off[part][c] + q];
+                s += (int64_t)pairs[e.x].nprim * pairs[e.y].nprim;
+            }
+            ctx->plan_prims[part][c] = s;
+        }
+    ctx->have_plan = true;
+    if (counts) {
+        counts[0] = total;
+        counts[1] = (int64_t)f64.size();
+        counts[2] = (int64_t)f32.size();
+        counts[3] = dropped;
+    }
+    return PQB_OK;
+}
+
+int pqb_plan_stats(const pqb_ctx *ctx, int64_t *quartets, int64_t *prim_quartets)
+{
+    if (!ctx || !quartets || !prim_quartets) return PQB_E_ARG;
+    if (!ctx->have_plan) return PQB_E_STATE;
+    for (int part = 0; part < 2; ++part)
+        for (int c = 0; c < kNumQuartetClass; ++c) {
+            quartets[part * kNumQuartetClass + c] = ctx->plan_cnt[part][c];
+            prim_quartets[part * kNumQuartetClass + c] = ctx->plan_prims[part][c];
+        }
+    return PQB_OK;
+}
+
+int pqb_plan_shard(pqb_ctx *ctx, int rank, int nranks)
+{
+    if (!ctx || nranks < 1 || rank < 0 || rank >= nranks) return fail(ctx, PQB_E_ARG, "pqb_plan_shard: bad rank");
+    if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_plan_shard: call pqb_plan first");
+    if (nranks == 1) return PQB_OK;
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    const size_t total = ctx->plan_h.size();
+    std::vector<int2> out;
+    out.reserve(total / nranks + 64);
+    int64_t off[2][kNumQuartetClass], cnt[2][kNumQuartetClass], prims[2][kNumQuartetClass];
+    for (int part = 0; part < 2; ++part)
+        for (int c = 0; c < kNumQuartetClass; ++c) {
+            off[part][c] = (int64_t)out.size();
+            prims[part][c] = 0;
+            for (int64_t q = rank; q < ctx->plan_cnt[part][c]; q += nranks) {
+                const int2 e = ctx->plan_h[ctx->plan_off[part][c] + q];
+                out.push_back(e);
+                prims[part][c] += (int64_t)ctx->pairs[e.x].nprim * ctx->pairs[e.y].nprim;
+            }
+            cnt[part][c] = (int64_t)out.size() - off[part][c];
+        }
+    if (!out.empty())
+        PQB_CK(ctx, cudaMemcpy(ctx->d_plan, out.data(), sizeof(int2) * out.size(), cudaMemcpyHostToDevice));
+    memcpy(ctx->plan_off, off, sizeof off);
+    memcpy(ctx->plan_cnt, cnt, sizeof cnt);
+    memcpy(ctx->plan_prims, prims, sizeof prims);
+    ctx->plan_h.swap(out);
+    return PQB_OK;
+}
+
+int pqb_fp64_peak(pqb_ctx *ctx, int iters, double *flops)
+{
+    if (!ctx || iters <= 0 || !flops) return fail(ctx, PQB_E_ARG, "pqb_fp64_peak: bad arguments");
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    double *sink = nullptr;
+    cudaEvent_t e0, e1;
+    PQB_CK(ctx, cudaMalloc(&sink, sizeof(double)));
+    PQB_CK(ctx, cudaEventCreate(&e0));
+    PQB_CK(ctx, cudaEventCreate(&e1));
+    const int blocks = ctx->nsm * 8, threads = 256;
+    dfma_probe_kernel<<<blocks, threads>>>(iters / 10 + 1, sink);   // warm-up
+    PQB_CK(ctx, cudaEventRecord(e0));
+    dfma_probe_kernel<<<blocks, threads>>>(iters, sink);
+    PQB_CK(ctx, cudaEventRecord(e1));
+    PQB_CK(ctx, cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PQB_CK(ctx, cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    *flops = 2.0 * 8.0 * (double)iters * blocks * threads / (ms * 1e-3);
+    return PQB_OK;
+}
+
+int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
+{
+    if (!ctx || !out) return fail(ctx, PQB_E_ARG, "pqb_eri_packed: bad arguments");
+    if (!ctx->d_pairs) return fail(ctx, PQB_E_STATE, "pqb_eri_packed: no basis uploaded");
+    const int64_t P = (int64_t)ctx->nbf * (ctx->nbf + 1) / 2;
+    if (len != P * (P + 1) / 2) return fail(ctx, PQB_E_SHAPE, "pqb_eri_packed: len %lld != %lld", (long long)len, (long long)(P * (P + 1) / 2));
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int c = 0; c < kNumQuartetClass; ++c)
+        PQB_CK(ctx, launch_packed_f64(c, ctx->d_full + ctx->full_off[c], (int)ctx->full_cnt[c], ctx->d_pairs,
+                                      ctx->d_prims, out, ctx->d_fscale, st, ctx->nsm));
+    return PQB_OK;
+}
+
+int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode, void *stream)
+{
+    if (!ctx || !D || !J || !K) return fail(ctx, PQB_E_ARG, "pqb_jk_direct: bad arguments");
+    if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_jk_direct: call pqb_plan first");
+    if (mode != PQB_FP64 && mode != PQB_MIXED) return fail(ctx, PQB_E_ARG, "pqb_jk_direct: mode %d", mode);
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const int n = ctx->nbf;
+    PQB_CK(ctx, cudaMemsetAsync(J, 0, sizeof(double) * n * n, st));
+    PQB_CK(ctx, cudaMemsetAsync(K, 0, sizeof(double) * n * n, st));
+    for (int c = kNumQuartetClass - 1; c >= 0; --c) {
+        PQB_CK(ctx, launch_jk_f64(c, ctx->d_plan + ctx->plan_off[0][c], (int)ctx->plan_cnt[0][c], ctx->d_pairs,
+                                  ctx->d_prims, D, J, K, ctx->d_fscale, n, st, ctx->nsm));
+        if (mode == PQB_MIXED)
+            PQB_CK(ctx, launch_jk_f32(c, ctx->d_plan + ctx->plan_off[1][c], (int)ctx->plan_cnt[1][c], ctx->d_pairs,
+                                      ctx->d_prims, D, J, K, ctx->d_fscale, n, st, ctx->nsm));
+        else
+            PQB_CK(ctx, launch_jk_f64(c, ctx->d_plan + ctx->plan_off[1][c], (int)ctx->plan_cnt[1][c], ctx->d_pairs,
+                                      ctx->d_prims, D, J, K, ctx->d_fscale, n, st, ctx->nsm));
+    }
+    const int64_t P = (int64_t)n * (n + 1) / 2;
+    symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, n);
+    symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K, n);
+    PQB_CK(ctx, cudaGetLastError());
+    return PQB_OK;
+}
+
+int pqb_jk_direct_class(pqb_ctx *ctx, const double *D, double *Jacc, double *Kacc, int part, int qclass, int mode,
+                        void *stream)
+{
+    if (!ctx || !D || !Jacc || !Kacc || part < 0 || part > 1 || qclass < 0 || qclass >= kNumQuartetClass)
+        return fail(ctx, PQB_E_ARG, "pqb_jk_direct_class: bad arguments");
+    if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_jk_direct_class: call pqb_plan first");
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const int2 *list = ctx->d_plan + ctx->plan_off[part][qclass];
+    const int nq = (int)ctx->plan_cnt[part][qclass];
+    if (mode == PQB_MIXED && part == 1)
+        PQB_CK(ctx, launch_jk_f32(qclass, list, nq, ctx->d_pairs, ctx->d_prims, D, Jacc, Kacc, ctx->d_fscale, ctx->nbf,
+                                  st, ctx->nsm));
+    else
+        PQB_CK(ctx, launch_jk_f64(qclass, list, nq, ctx->d_pairs, ctx->d_prims, D, Jacc, Kacc, ctx->d_fscale, ctx->nbf,
+                                  st, ctx->nsm));
+    return PQB_OK;
+}
+
+int pqb_jk_packed(pqb_ctx *ctx, const double *ints, int64_t len, const double *D, double *J, double *K, int nbf,
+                  void *stream)
+{
+    if (!ctx || !ints || !D || !J || !K || nbf <= 0) return fail(ctx, PQB_E_ARG, "pqb_jk_packed: bad arguments");
+    const int64_t P = (int64_t)nbf * (nbf + 1) / 2;
+    if (len != P * (P + 1) / 2) return fail(ctx, PQB_E_SHAPE, "pqb_jk_packed: len %lld != %lld", (long long)len, (long long)(P * (P + 1) / 2));
+    if (P > 0x7fffffffLL) return fail(ctx, PQB_E_SHAPE, "pqb_jk_packed: nbf too large");
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    PQB_CK(ctx, cudaMemsetAsync(J, 0, sizeof(double) * nbf * nbf, st));
+    PQB_CK(ctx, cudaMemsetAsync(K, 0, sizeof(double) * nbf * nbf, st));
+    jk_packed_kernel<<<(unsigned)P, 256, 0, st>>>(ints, D, J, K, nbf);
+    symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, nbf);
+    symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K, nbf);
+    PQB_CK(ctx, cudaGetLastError());
+    return PQB_OK;
+}
+
+int pqb_eri_functions(pqb_ctx *ctx, int engine, int aux_m, int nq, const int *quartets, int n, const double *origin,
+                      const int *powers, const int *prim_off, const double *exps, const double *cn,
+                      const double *norms, double *out, void *stream)
+{
+    if (!ctx || nq < 0 || !quartets || n <= 0 || !origin || !powers || !prim_off || !exps || !cn || !norms || !out)
+        return fail(ctx, PQB_E_ARG, "pqb_eri_functions: bad arguments");
+    if (engine != PQB_ENGINE_RYS && engine != PQB_ENGINE_HGP)
+        return fail(ctx, PQB_E_ARG, "pqb_eri_functions: engine %d", engine);
+    if (aux_m < 0 || (aux_m > 0 && engine != PQB_ENGINE_HGP))
+        return fail(ctx, PQB_E_ARG, "pqb_eri_functions: aux_m %d needs the HGP engine", aux_m);
+    if (nq == 0) return PQB_OK;
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    FuncTable ft{origin, powers, prim_off, exps, cn, norms};
+    if (engine == PQB_ENGINE_RYS)
+        eri_general_rys_kernel<<<(nq + 63) / 64, 64, 0, st>>>(nq, quartets, ft, out);
+    else
+        eri_general_hgp_kernel<<<(nq + 31) / 32, 32, 0, st>>>(nq, aux_m, quartets, ft, out);
+    PQB_CK(ctx, cudaGetLastError());
+    return PQB_OK;
+}
+
+int pqb_oneint(pqb_ctx *ctx, int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
+               const double *cn, const double *norms, int natoms, const double *atom_xyz, const double *atom_z,
+               double *S, double *T, double *V, void *stream)
+{
+    if (!ctx || n <= 0 || !origin || !powers || !prim_off || !exps || !cn || !norms || natoms < 0 ||
+        (V && natoms > 0 && (!atom_xyz || !atom_z)))
+        return fail(ctx, PQB_E_ARG, "pqb_oneint: bad arguments");
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    // atoms (host arrays) -> packed device scratch {x, y, z, Z}
+    std::vector<double> at(4 * (size_t)std::max(natoms, 1), 0.0);
+    for (int a = 0; a < natoms; ++a) {
+        for (int x = 0; x < 3; ++x) at[4 * a + x] = atom_xyz[3 * a + x];
+        at[4 * a + 3] = atom_z[a];
+    }
+    if (at.size() > ctx->atoms_cap) {
+        free_dev(ctx->d_atoms);
+        ctx->d_atoms = nullptr;
+        PQB_CK(ctx, cudaMalloc(&ctx->d_atoms, sizeof(double) * at.size()));
+        ctx->atoms_cap = at.size();
+    }
+    PQB_CK(ctx, cudaMemcpyAsync(ctx->d_atoms, at.data(), sizeof(double) * at.size(), cudaMemcpyHostToDevice, st));
+    FuncTable ft{origin, powers, prim_off, exps, cn, norms};
+    const int64_t nn = (int64_t)n * n;
+    oneint_kernel<<<(unsigned)((nn + 127) / 128), 128, 0, st>>>(n, ft, natoms, ctx->d_atoms, S, T, V);
+    PQB_CK(ctx, cudaGetLastError());
+    // the host staging buffer must outlive the async copy
+    PQB_CK(ctx, cudaStreamSynchronize(st));
+    return PQB_OK;
+}
+
+int pqb_boys_eval(pqb_ctx *ctx, int m, int count, const double *T, double *F, void *stream)
+{
+    if (!ctx || m < 0 || m > 16 || count < 0 || !T || !F) return fail(ctx, PQB_E_ARG, "pqb_boys_eval: bad arguments");
+    if (count == 0) return PQB_OK;
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    boys_eval_kernel<<<(count + 127) / 128, 128, 0, (cudaStream_t)stream>>>(m, count, T, F);
+    PQB_CK(ctx, cudaGetLastError());
+    return PQB_OK;
+}
+
+int pqb_rys_eval(pqb_ctx *ctx, int nroots, int count, const double *T, double *u, double *w, void *stream)
+{
+    if (!ctx || nroots < 1 || nroots > PQB_RYS_NMAX || count < 0 || !T || !u || !w)
+        return fail(ctx, PQB_E_ARG, "pqb_rys_eval: bad arguments");
+    if (count == 0) return PQB_OK;
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    rys_eval_kernel<<<(count + 127) / 128, 128, 0, (cudaStream_t)stream>>>(nroots, count, T, u, w);
+    PQB_CK(ctx, cudaGetLastError());
+    return PQB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,197 @@
+// Device building blocks shared by every kernel of the engine:
+//   - the Boys function F_m(T) (table + 8-term Taylor + downward recursion),
+//   - Rys roots/weights (piecewise Chebyshev tables, large-T limit),
+//   - cartesian-component helpers in PyQuante's order (PyQuante/Ints.py:23-29),
+//   - the 2-D Rys recurrence and the horizontal transfer that together replace
+//     Recur/Shift of the reference (Src/crys.c:1481-1534).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#ifndef PQB_TABQ
+#define PQB_TABQ static __device__ const
+#endif
+#ifndef PQB_CTABQ
+#define PQB_CTABQ static __constant__ const
+#endif
+#include "rys_tables.inc"
+
+namespace pqb {
+
+constexpr double kPi = 3.14159265358979323846;
+// sqrt(2) * pi^(5/4): K_ab = sqrt(2) pi^(5/4)/zeta exp(-mu R^2) so that
+// K_ab K_cd / sqrt(zeta+eta) = 2 pi^(5/2)/(zeta eta sqrt(zeta+eta)) exp(...)
+constexpr double kPairPre = 5.9149671727956128778;
+
+__host__ __device__ constexpr int ncart(int L) { return (L + 1) * (L + 2) / 2; }
+// x / y / z exponent of cartesian component i of a shell of angular momentum L,
+// PyQuante order: x from L down to 0, then y from L-x down to 0.
+__host__ __device__ constexpr int cart_lx(int L, int i)
+{
+    int x = L;
+    while (i >= L - x + 1) { i -= L - x + 1; --x; }
+    return x;
+}
+__host__ __device__ constexpr int cart_ly(int L, int i)
+{
+    int x = L;
+    while (i >= L - x + 1) { i -= L - x + 1; --x; }
+    return L - x - i;
+}
+__host__ __device__ constexpr int cart_lz(int L, int i) { return L - cart_lx(L, i) - cart_ly(L, i); }
+__host__ __device__ constexpr int cart_l(int L, int i, int axis)
+{
+    return axis == 0 ? cart_lx(L, i) : (axis == 1 ? cart_ly(L, i) : cart_lz(L, i));
+}
+
+// ------------------------------------------------------------------ Boys --
+// F_m(T) for m = 0..M into F[].  T < TMAX: F_M by Taylor about the nearest
+// grid point T_k = k/16 (|dT| <= 1/32, 8 terms, remainder < 3e-17 F), then
+// F_m = (2T F_{m+1} + e^{-T})/(2m+1).  T >= TMAX: F_0 = sqrt(pi/T)/2 and
+// F_{m+1} = ((2m+1) F_m - e^{-T})/(2T) (stable for T > m).
+template <int M>
+__device__ __forceinline__ void boys(double T, double *F)
+{
+    static_assert(M + 8 <= PQB_BOYS_NORD, "Boys table too short");
+    if (T < PQB_BOYS_TMAX) {
+        int k = __double2int_rn(T * PQB_BOYS_STEP_INV);
+        double d = -(T - k * (1.0 / PQB_BOYS_STEP_INV));
+        const double *row = pqb_boys_tab + k * PQB_BOYS_NORD + M;
+        double f = __ldg(row + 7);
+#pragma unroll
+        for (int j = 6; j >= 0; --j) f = fma(f, d * (1.0 / (j + 1)), __ldg(row + j));
+        F[M] = f;
+        if (M > 0) {
+            double e = exp(-T), t2 = 2.0 * T;
+#pragma unroll
+            for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * (1.0 / (2 * m + 1));
+        }
+    } else {
+        double it = 1.0 / T;
+        F[0] = 0.5 * sqrt(kPi * it);
+        if (M > 0) {
+            double e = exp(-T), h = 0.5 * it;
+#pragma unroll
+            for (int m = 0; m < M; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+        }
+    }
+}
+
+// Runtime-order variant (m <= 16) for the general-L kernels.
+__device__ __forceinline__ void boys_rt(int M, double T, double *F)
+{
+    if (T < PQB_BOYS_TMAX) {
+        int k = __double2int_rn(T * PQB_BOYS_STEP_INV);
+        double d = -(T - k * (1.0 / PQB_BOYS_STEP_INV));
+        const double *row = pqb_boys_tab + k * PQB_BOYS_NORD + M;
+        double f = __ldg(row + 7);
+#pragma unroll
+        for (int j = 6; j >= 0; --j) f = fma(f, d * (1.0 / (j + 1)), __ldg(row + j));
+        F[M] = f;
+        double e = exp(-T), t2 = 2.0 * T;
+        for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) / (2 * m + 1);
+    } else {
+        double it = 1.0 / T, e = exp(-T), h = 0.5 * it;
+        F[0] = 0.5 * sqrt(kPi * it);
+        for (int m = 0; m < M; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+    }
+}
+
+// ------------------------------------------------------------------- Rys --
+__device__ __forceinline__ double clenshaw14(const double *c, double x)
+{
+    double b1 = 0.0, b2 = 0.0, x2 = 2.0 * x;
+#pragma unroll
+    for (int k = PQB_RYS_NCOEF - 1; k >= 1; --k) {
+        double t = fma(x2, b1, __ldg(c + k) - b2);
+        b2 = b1;
+        b1 = t;
+    }
+    return fma(x, b1, __ldg(c) - b2);
+}
+
+// Root r (0-based, ascending) of the n-point Rys rule at T, as u = t^2 in
+// (0,1), and its weight (sum_r w_r = F_0(T)).
+__device__ __forceinline__ void rys_root(int n, int r, double T, double &u, double &w)
+{
+    if (T < pqb_rys_tasym[n]) {
+        int iv = (int)T;
+        double x = 2.0 * (T - iv) - 1.0;
+        const double *c = pqb_rys_coef + pqb_rys_offset[n] + (iv * 2 * n + 2 * r) * PQB_RYS_NCOEF;
+        u = clenshaw14(c, x);
+        w = clenshaw14(c + PQB_RYS_NCOEF, x);
+    } else {
+        double it = 1.0 / T;
+        u = pqb_rys_asym_root[n][r] * it;
+        w = pqb_rys_asym_weight[n][r] * sqrt(it);
+    }
+}
+
+// ------------------------------------------------ 2-D Rys integrals (one axis)
+// For one root u and one cartesian axis: G(n,m) = I_x(n,0|m,0) by the Rys
+// recurrence (bra exponent sum zeta, ket eta), then the horizontal transfer
+// I(a,b+1|c,d) = I(a+1,b|c,d) + AB I(a,b|c,d) and likewise on the ket, giving
+// out[((a*(LB+1)+b)*(LC+1)+c)*(LD+1)+d] for a<=LA, b<=LB, c<=LC, d<=LD.
+// `scale` multiplies every output (the root weight times the quartet
+// prefactor goes on one axis).  All sizes are compile-time: fully unrolled,
+// register resident.
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void rys2d(double u, double zeta, double eta, double PA, double QC, double PQ,
+                                      double AB, double CD, double scale, R *out)
+{
+    constexpr int NB = LA + LB, MK = LC + LD;
+    const double zpe = zeta + eta;
+    const double b00 = 0.5 * u / zpe;
+    const double b10 = (0.5 - 0.5 * eta / zpe * u) / zeta;
+    const double b01 = (0.5 - 0.5 * zeta / zpe * u) / eta;
+    const double c00 = PA - eta / zpe * u * PQ;
+    const double c01 = QC + zeta / zpe * u * PQ;
+    R g[NB + 1][MK + 1];
+    g[0][0] = (R)scale;
+    if (NB > 0) g[1][0] = (R)(c00 * scale);
+#pragma unroll
+    for (int n = 1; n < NB; ++n) g[n + 1][0] = (R)(n * b10) * g[n - 1][0] + (R)c00 * g[n][0];
+#pragma unroll
+    for (int n = 0; n <= NB; ++n) {
+        if (MK > 0) g[n][1] = (R)c01 * g[n][0] + (n > 0 ? (R)(n * b00) * g[n - 1][0] : (R)0);
+#pragma unroll
+        for (int m = 1; m < MK; ++m)
+            g[n][m + 1] = (R)(m * b01) * g[n][m - 1] + (R)c01 * g[n][m] +
+                          (n > 0 ? (R)(n * b00) * g[n - 1][m] : (R)0);
+    }
+    // ket transfer: h[n][c][d] for n <= NB, c <= LC, d <= LD
+    R h[NB + 1][LC + 1][LD + 1];
+#pragma unroll
+    for (int n = 0; n <= NB; ++n) {
+        R t[MK + 1][LD + 1];
+#pragma unroll
+        for (int m = 0; m <= MK; ++m) t[m][0] = g[n][m];
+#pragma unroll
+        for (int d = 1; d <= LD; ++d)
+#pragma unroll
+            for (int m = 0; m + d <= MK; ++m) t[m][d] = t[m + 1][d - 1] + (R)CD * t[m][d - 1];
+#pragma unroll
+        for (int c = 0; c <= LC; ++c)
+#pragma unroll
+            for (int d = 0; d <= LD; ++d) h[n][c][d] = t[c][d];
+    }
+    // bra transfer
+#pragma unroll
+    for (int c = 0; c <= LC; ++c)
+#pragma unroll
+        for (int d = 0; d <= LD; ++d) {
+            R t[NB + 1][LB + 1];
+#pragma unroll
+            for (int n = 0; n <= NB; ++n) t[n][0] = h[n][c][d];
+#pragma unroll
+            for (int b = 1; b <= LB; ++b)
+#pragma unroll
+                for (int n = 0; n + b <= NB; ++n) t[n][b] = t[n + 1][b - 1] + (R)AB * t[n][b - 1];
+#pragma unroll
+            for (int a = 0; a <= LA; ++a)
+#pragma unroll
+                for (int b = 0; b <= LB; ++b) out[((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d] = t[a][b];
+        }
+}
+
+}  // namespace pqb

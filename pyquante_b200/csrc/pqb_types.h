@@ -1,0 +1,43 @@
+// Device-resident data layout of a basis (built by the host in pqb_capi.cu).
+//
+// Shell pairs are stored once per unordered pair of shells, oriented so the
+// first shell has the higher angular momentum (ties: higher shell index);
+// the Rys horizontal transfer moves momentum from the first to the second.
+// Each pair owns a run of primitive pairs with the Gaussian-product data.
+#pragma once
+#include <stdint.h>
+
+namespace pqb {
+
+constexpr int kMaxL = 2;                         // shells up to d (cartesian)
+constexpr int kNumPairClass = 6;                 // ss ps pp ds dp dd
+constexpr int kNumQuartetClass = 21;             // bra class >= ket class
+
+struct PairInfo {
+    double A[3];       // centre of the first shell
+    double AB[3];      // A - B
+    int prim_off;      // first PrimPair
+    int nprim;         // number of (screened) primitive pairs
+    int fa, fb;        // first basis-function index of each shell
+    int sa, sb;        // shell indices
+    int cls;           // pair class: index of (La, Lb) in ss ps pp ds dp dd
+    int la, lb;
+    int pad;
+};
+
+struct PrimPair {
+    double zeta;       // alpha_a + alpha_b
+    double P[3];       // Gaussian product centre
+    double K;          // c_a c_b sqrt(2) pi^(5/4)/zeta exp(-alpha_a alpha_b/zeta |AB|^2)
+    double pad;
+};
+
+__host__ __device__ inline int pair_class(int la, int lb)   // la >= lb
+{
+    return la * (la + 1) / 2 + lb;
+}
+
+// quartet class index for bra class cb >= ket class ck
+__host__ __device__ inline int quartet_class(int cb, int ck) { return cb * (cb + 1) / 2 + ck; }
+
+}  // namespace pqb

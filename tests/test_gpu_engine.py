@@ -1,0 +1,262 @@
+"""GPU parity: the CUDA engine through the C ABI against the oracle, the
+reference's compiled C (oracle/_ref, when present) and the golden fixtures.
+
+Tolerances (FP64 path): 1e-10 absolute per integral, 1e-8 Eh total energy,
+1e-10 on J/K elements; mixed precision: stated per test."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import pyq_oracle as O
+from conftest import GOLDEN
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from pyquante_b200 import Ints, _lib, chgp, cints, crys, geometries  # noqa: E402
+from pyquante_b200.Basis.basis import BasisSet  # noqa: E402
+from pyquante_b200.engine import BasisEngine  # noqa: E402
+from pyquante_b200.hartree_fock import rhf  # noqa: E402
+
+ERI_TOL = 1e-10
+E_TOL = 1e-8
+
+
+def atoms_of(mol):
+    return [(a.atno, tuple(float(c) for c in a.r)) for a in mol.atoms]
+
+
+def oracle_bfs(bs):
+    return [O.BF(bf.origin, bf.powers, list(zip(bf.pexps, bf.pcoefs))) for bf in bs.bfs]
+
+
+# ------------------------------------------------------------ Boys / Rys --
+def test_boys_device_matches_40_digit_values():
+    ctx = _lib.context()
+    g = json.load(open(os.path.join(GOLDEN, "boys.json")))
+    for m in sorted({int(r[0]) for r in g["mpmath"]}):
+        rows = [r for r in g["mpmath"] if r[0] == m]
+        T = torch.tensor([r[1] for r in rows], dtype=torch.float64, device="cuda")
+        F = torch.empty(len(rows) * (m + 1), dtype=torch.float64, device="cuda")
+        ctx.check(ctx.lib.pqb_boys_eval(ctx.h, m, len(rows), _lib.ptr(T), _lib.ptr(F), _lib.stream_ptr()))
+        got = F.view(len(rows), m + 1)[:, m].cpu().numpy()
+        ref = np.array([r[2] for r in rows])
+        assert np.all(np.abs(got - ref) <= 2e-14 * np.abs(ref)), (m, got, ref)
+    # TestMath.c:18-19 through the cints drop-in
+    assert abs(cints.Fgamma(0, 1.0) - 0.7468241328124271) < 1e-8
+    assert abs(cints.Fgamma(0.5, 6.8) - 0.073447516533246701) < 1e-8
+
+
+def test_rys_roots_weights_match_40_digit_values():
+    ctx = _lib.context()
+    g = np.load(os.path.join(GOLDEN, "rys.npz"))
+    T = torch.tensor(g["T"], dtype=torch.float64, device="cuda")
+    for n in range(1, 6):
+        u = torch.empty(len(g["T"]) * n, dtype=torch.float64, device="cuda")
+        w = torch.empty_like(u)
+        ctx.check(ctx.lib.pqb_rys_eval(ctx.h, n, len(g["T"]), _lib.ptr(T), _lib.ptr(u), _lib.ptr(w),
+                                       _lib.stream_ptr()))
+        uu = u.view(-1, n).cpu().numpy()
+        ww = w.view(-1, n).cpu().numpy()
+        assert np.all(np.abs(uu - g["u%d" % n]) <= 1e-14 * np.abs(g["u%d" % n]) + 1e-300), n
+        assert np.all(np.abs(ww - g["w%d" % n]) <= 1e-14 * np.abs(g["w%d" % n]) + 1e-300), n
+
+
+# ------------------------------------------------------- packed integrals --
+def test_packed_sto3g_water_vs_reference_golden():
+    mol = geometries.water()
+    bs = BasisSet(mol, "sto-3g")
+    ints = Ints.get2ints(bs)
+    gold = np.load(os.path.join(GOLDEN, "eri_sto3g_water.npy"))
+    assert len(ints) == 406
+    assert np.abs(ints.numpy() - gold).max() < ERI_TOL
+
+
+def test_packed_631ss_water_vs_reference_and_oracle():
+    mol = geometries.water()
+    bs = BasisSet(mol, "6-31g**")
+    assert len(bs) == 25
+    ints = Ints.get2ints(bs).numpy()
+    s = np.load(os.path.join(GOLDEN, "eri_631ss_water_sample.npz"))
+    assert np.abs(ints[s["index"]] - s["value"]).max() < ERI_TOL
+    orc = O.orc_get2ints(oracle_bfs(bs))
+    assert np.abs(ints - orc).max() < ERI_TOL
+
+
+def test_packed_two_waters_every_class_vs_oracle():
+    mol = geometries.water_cluster(2, seed=4)
+    bs = BasisSet(mol, "6-31g**")
+    ints = Ints.get2ints(bs).numpy()
+    orc = O.orc_get2ints(oracle_bfs(bs))
+    assert np.abs(ints - orc).max() < ERI_TOL
+
+
+def test_packed_h2o8_sample_vs_reference_engine():
+    """(H2O)8 / 6-31G**, N = 200, Q = 202,015,050 integrals (1.6 GB)."""
+    mol = geometries.water_cluster(8, seed=0)
+    bs = BasisSet(mol, "6-31g**")
+    assert len(bs) == 200
+    eng = BasisEngine(bs.bfs)
+    t = eng.eri_packed()
+    assert t.numel() == 202015050
+    s = np.load(os.path.join(GOLDEN, "eri_631ss_h2o8_sample.npz"))
+    idx = np.array([O.ijkl2intindex(*q) for q in s["quartets"]])
+    got = t[torch.from_numpy(idx).cuda()].cpu().numpy()
+    assert np.abs(got - s["value"]).max() < ERI_TOL
+    # size-independent property: every slot written once, finite
+    assert bool(torch.isfinite(t).all())
+    del t
+
+
+# --------------------------------------------------------- one-electron --
+def test_one_electron_vs_oracle():
+    for mol, basis in [(geometries.water(), "sto-3g"), (geometries.water_cluster(2, seed=1), "6-31g**")]:
+        bs = BasisSet(mol, basis)
+        S, h = Ints.get1ints(bs, mol)
+        So, ho = O.orc_get1ints(oracle_bfs(bs), atoms_of(mol))
+        assert np.abs(S - So).max() < 1e-12
+        assert np.abs(h - ho).max() < 1e-10
+
+
+# ----------------------------------------------------------- scalar API --
+def test_scalar_entry_points_vs_reference():
+    rng = np.random.default_rng(2)
+    mol = geometries.water_cluster(2, seed=7)
+    bs = BasisSet(mol, "6-31g**")
+    bfs = bs.bfs
+    have_ref = O.ref_available()
+    for _ in range(12):
+        i, j, k, l = (int(x) for x in rng.integers(0, len(bfs), 4))
+        a, b, c, d = bfs[i], bfs[j], bfs[k], bfs[l]
+        args = []
+        for f in (a, b, c, d):
+            args += [f.pexps, f.pcoefs, f.pnorms, f.origin, f.powers]
+        ob = [O.BF(f.origin, f.powers, list(zip(f.pexps, f.pcoefs))) for f in (a, b, c, d)]
+        want = O.orc_contr(*ob)
+        if have_ref:
+            assert abs(O.ref_contr(*ob) - want) < 1e-12
+        assert abs(crys.contr_coulomb(*args) - want) < ERI_TOL
+        assert abs(cints.contr_coulomb(*args) - want) < ERI_TOL
+        assert abs(chgp.contr_coulomb(*args) - want) < ERI_TOL
+        pa = (a.origin, a.pnorms[0], a.powers, a.pexps[0])
+        pb = (b.origin, b.pnorms[0], b.powers, b.pexps[0])
+        pc = (c.origin, c.pnorms[0], c.powers, c.pexps[0])
+        pd = (d.origin, d.pnorms[0], d.powers, d.pexps[0])
+        v1 = crys.coulomb_repulsion(*pa, *pb, *pc, *pd)
+        v2 = chgp.coulomb_repulsion(*pa, *pb, *pc, *pd)
+        assert abs(v1 - v2) <= 1e-12 * max(1.0, abs(v1))
+        if have_ref:
+            rc = O.ref_lib("crys")
+            r = rc.coulomb_repulsion(*pa[0], pa[1], *pa[2], pa[3], *pb[0], pb[1], *pb[2], pb[3],
+                                     *pc[0], pc[1], *pc[2], pc[3], *pd[0], pd[1], *pd[2], pd[3])
+            assert abs(v1 - r) <= 1e-12 * max(1.0, abs(r))
+            # chgp.vrr with m > 0 against the reference (its Boys is 3e-7 accurate)
+            rh = O.ref_lib("chgp")
+            for m in (0, 1, 2):
+                want_v = rh.ref_chgp_vrr(*pa[0], pa[1], *pa[2], pa[3], *pb[0], pb[1], pb[3],
+                                         *pc[0], pc[1], *pc[2], pc[3], *pd[0], pd[1], pd[3], m)
+                got_v = chgp.vrr(pa[0], pa[1], pa[2], pa[3], pb[0], pb[1], pb[3], pc[0], pc[1], pc[2], pc[3],
+                                 pd[0], pd[1], pd[3], m)
+                assert abs(got_v - want_v) <= 1e-6 * abs(want_v) + 1e-12
+
+
+def test_scalar_errors_are_raised_not_garbage():
+    f = [[1.0], [1.0], [1.0], (0.0, 0.0, 0.0)]
+    with pytest.raises(_lib.EngineError):   # total L = 12 > 9: the reference silently uses stale roots
+        crys.contr_coulomb(*(f + [(3, 0, 0)]) * 4)
+    with pytest.raises(ValueError):
+        crys.contr_coulomb([1.0, 2.0], [1.0], [1.0], (0, 0, 0), (0, 0, 0), *(f + [(0, 0, 0)]) * 3)
+
+
+def test_general_per_function_path_vs_oracle():
+    """Functions that do not form shells (reordered list): per-function kernel."""
+    mol = geometries.water()
+    bs = BasisSet(mol, "6-31g**")
+    rng = np.random.default_rng(0)
+    order = rng.permutation(len(bs))
+    bfs = [bs.bfs[i] for i in order]
+    ints = Ints.get2ints(bfs)
+    assert not ints.engine.has_shells
+    orc = O.orc_get2ints([O.BF(f.origin, f.powers, list(zip(f.pexps, f.pcoefs))) for f in bfs])
+    assert np.abs(ints.numpy() - orc).max() < ERI_TOL
+
+
+# ------------------------------------------------------------------ J / K --
+def _rand_density(n, seed=0):
+    rng = np.random.default_rng(seed)
+    C = rng.standard_normal((n, max(1, n // 3))) * 0.3
+    return C @ C.T
+
+
+def test_jk_stored_and_direct_vs_oracle():
+    mol = geometries.water_cluster(2, seed=4)
+    bs = BasisSet(mol, "6-31g**")
+    D = _rand_density(len(bs))
+    orc = O.orc_get2ints(oracle_bfs(bs))
+    Jo, Ko = O.getJK(orc, D)
+    ints = Ints.get2ints(bs)
+    J, K = Ints.getJ(ints, D), Ints.getK(ints, D)
+    assert np.abs(J - Jo).max() < ERI_TOL and np.abs(K - Ko).max() < ERI_TOL
+    G = Ints.get2JmK(ints, D)
+    assert np.abs(G - (2 * Jo - Ko)).max() < 2 * ERI_TOL
+    d = Ints.get2ints(bs, direct=True, schwarz=0.0)
+    Jd, Kd = Ints.getJ(d, D), Ints.getK(d, D)
+    assert np.abs(Jd - Jo).max() < ERI_TOL and np.abs(Kd - Ko).max() < ERI_TOL
+    # torch in -> torch out, same values
+    Dt = torch.as_tensor(D, device="cuda")
+    Gt = Ints.get2JmK(d, Dt)
+    assert isinstance(Gt, torch.Tensor) and Gt.is_cuda
+    assert np.abs(Gt.cpu().numpy() - (2 * Jo - Ko)).max() < 2 * ERI_TOL
+
+
+def test_jk_mixed_precision_error_is_small():
+    mol = geometries.water_cluster(3, seed=2)
+    bs = BasisSet(mol, "6-31g**")
+    D = _rand_density(len(bs), 1)
+    e64 = Ints.get2ints(bs, direct=True, precision="fp64", schwarz=1e-12)
+    emx = Ints.get2ints(bs, direct=True, precision="mixed", schwarz=1e-12, fp32_threshold=1e-5)
+    G64 = Ints.get2JmK(e64, D)
+    Gmx = Ints.get2JmK(emx, D)
+    counts = emx.engine.plan_counts
+    assert counts["fp32"] > 0
+    # FP32 only where Q_ab Q_cd < 1e-5: element errors stay ~1e-5 * 1e-7 * |D| sums
+    assert np.abs(G64 - Gmx).max() < 1e-8
+
+
+# -------------------------------------------------------------- energies --
+def test_rhf_water_sto3g_energy():
+    e = json.load(open(os.path.join(GOLDEN, "energies.json")))
+    mol = geometries.water()
+    E, orbe, orbs = rhf(mol, basis_data="sto-3g", ConvCriteria=1e-12, MaxIter=100)
+    assert abs(E - e["water_sto3g"]) < E_TOL
+    E2, _, _ = rhf(mol, basis_data="sto-3g", ConvCriteria=1e-12, MaxIter=100, direct=True, schwarz=0.0)
+    assert abs(E2 - e["water_sto3g"]) < E_TOL
+
+
+def test_rhf_reference_test_geometries():
+    """Tests/h2o.py and Tests/h2.py known answers, and the oracle to 1e-8 Eh."""
+    from pyquante_b200.Molecule import Molecule
+    e = json.load(open(os.path.join(GOLDEN, "energies.json")))
+    h2o = Molecule("h2o", [(8, (0.0, 0.0, 0.0)), (1, (1.0, 0.0, 0.0)), (1, (0.0, 1.0, 0.0))], units="Angstrom")
+    E, _, _ = rhf(h2o, ConvCriteria=1e-12, MaxIter=100, DoAveraging=True)
+    assert abs(E - e["h2o_test_literal"]) < e["h2o_test_tol"]
+    assert abs(E - e["h2o_test_geometry_631ss"]) < E_TOL
+    h2 = Molecule("h2", [(1, (0.0, 0.0, 0.0)), (1, (1.0, 0.0, 0.0))], units="bohr")
+    E, _, _ = rhf(h2, ConvCriteria=1e-12, MaxIter=100)
+    assert abs(E - e["h2_test_literal"]) < e["h2_test_tol"]
+    assert abs(E - e["h2_631ss"]) < E_TOL
+
+
+def test_engine_rejects_bad_shapes():
+    mol = geometries.water()
+    eng = BasisEngine(BasisSet(mol, "sto-3g").bfs)
+    bad = torch.empty(10, dtype=torch.float64, device="cuda")
+    with pytest.raises(_lib.EngineError) as ei:
+        eng.ctx.check(eng.ctx.lib.pqb_eri_packed(eng.ctx.h, _lib.ptr(bad), 10, _lib.stream_ptr()))
+    assert ei.value.code == _lib.PQB_E_SHAPE
+    with pytest.raises(_lib.EngineError) as ei:
+        eng.ctx.check(eng.ctx.lib.pqb_jk_direct(eng.ctx.h, _lib.ptr(bad), _lib.ptr(bad), _lib.ptr(bad), 0,
+                                                _lib.stream_ptr()))
+    assert ei.value.code == _lib.PQB_E_STATE
