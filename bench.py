@@ -330,7 +330,8 @@ def main():
             t_ms = sorted(tms)[1]
             fl = class_flops(qc, int(ps[part, qc]), int(qs[part, qc]))
             per_class.append(dict(part=part, cls=quartet_class_ls(qc), ms=t_ms, flops=fl,
-                                  tflops=fl / (t_ms * 1e-3) / 1e12))
+                                  tflops=fl / (t_ms * 1e-3) / 1e12, items=int(qs[part, qc]),
+                                  prims=int(ps[part, qc])))
     peak = ctypes.c_double()
     eng.ctx.check(eng.ctx.lib.pqb_fp64_peak(eng.ctx.h, 200000, ctypes.byref(peak)))
     peak_tf = peak.value / 1e12
@@ -366,7 +367,8 @@ def main():
                                     "sample": "%d quartets (%d random bra rows, all kl >= ij) in %.1f s" % (
                                         cpu["quartets"], cpu["rows"], cpu["seconds"])}
         line["per_class_fp64"] = [dict(cls="%d%d|%d%d" % r["cls"], part=r["part"], ms=round(r["ms"], 4),
-                                       tflops=round(r["tflops"], 3)) for r in sorted(per_class, key=lambda r: -r["ms"])]
+                                       tflops=round(r["tflops"], 3), items=r["items"], prims=r["prims"])
+                                  for r in sorted(per_class, key=lambda r: -r["ms"])]
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

@@ -19,7 +19,7 @@ class DIIS:
     def getF(self, F, D):
         t = isinstance(F, torch.Tensor)
         err = (F @ D @ self.S - self.S @ D @ F).reshape(-1)
-        self.maxerr = float(err.abs().max())
+        self.maxerr = float(abs(err).max())
         self.Fs.append(F)
         self.Errs.append(err)
         nit = len(self.Errs)

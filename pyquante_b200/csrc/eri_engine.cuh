@@ -156,7 +156,7 @@ struct EpiSchwarz {
 
 // ---------------------------------------------------------- thread mode --
 template <int LA, int LB, int LC, int LD, typename R, class Epi>
-__global__ void __launch_bounds__(128) eri_thread_kernel(const int2 *__restrict__ list, int nq,
+__global__ void __launch_bounds__(128) eri_thread_kernel(const int4 *__restrict__ list, int nq,
                                                          const PairInfo *__restrict__ pairs,
                                                          const PrimPair *__restrict__ prims, Epi epi)
 {
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(128) eri_thread_kernel(const int2 *__restrict_
     constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
     constexpr int G2D = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
     for (int qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += gridDim.x * blockDim.x) {
-        const int2 e = list[qi];
+        const int4 e = list[qi];   // bra pair, ket pair, first primitive quartet, count
         const PairInfo &pb = pairs[e.x];
         const PairInfo &pk = pairs[e.y];
         const double Ax = pb.A[0], Ay = pb.A[1], Az = pb.A[2];
@@ -175,11 +175,16 @@ __global__ void __launch_bounds__(128) eri_thread_kernel(const int2 *__restrict_
         R acc[NAB * NCD];
 #pragma unroll
         for (int c = 0; c < NAB * NCD; ++c) acc[c] = (R)0;
-        const int npb = pb.nprim, npk = pk.nprim;
-        for (int ib = 0; ib < npb; ++ib) {
+        const int npk = pk.nprim;
+        int ib = e.z / npk, ik = e.z - (e.z / npk) * npk;
+        for (int t = 0; t < e.w; ++t) {
             const PrimPair P = prims[pb.prim_off + ib];
-            for (int ik = 0; ik < npk; ++ik) {
+            {
                 const PrimPair Q = prims[pk.prim_off + ik];
+                if (++ik == npk) {
+                    ik = 0;
+                    ++ib;
+                }
                 const double zpe = P.zeta + Q.zeta;
                 const double PQx = P.P[0] - Q.P[0], PQy = P.P[1] - Q.P[1], PQz = P.P[2] - Q.P[2];
                 const double T = P.zeta * Q.zeta / zpe * (PQx * PQx + PQy * PQy + PQz * PQz);
@@ -240,7 +245,7 @@ struct BlockLayout {
 
 struct SlotData {
     QCtx q;
-    int npb, npk, pb_off, pk_off;
+    int npk, pp0, npp, pb_off, pk_off;
     double A[3], AB[3], C[3], CD[3];
 };
 struct SlotPrim {
@@ -248,7 +253,7 @@ struct SlotPrim {
 };
 
 template <int LA, int LB, int LC, int LD, typename R, class Epi>
-__global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int2 *__restrict__ list, int nq,
+__global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__restrict__ list, int nq,
                                                                   const PairInfo *__restrict__ pairs,
                                                                   const PrimPair *__restrict__ prims, Epi epi)
 {
@@ -279,12 +284,13 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int2 *__
             SlotData &s = sd[tid];
             const int qi = base + tid;
             if (qi < nq) {
-                const int2 e = list[qi];
+                const int4 e = list[qi];
                 const PairInfo &pb = pairs[e.x];
                 const PairInfo &pk = pairs[e.y];
                 s.q = QCtx{pb.fa, pb.fb, pk.fa, pk.fb, pb.sa, pb.sb, pk.sa, pk.sb, e.x, e.y};
-                s.npb = pb.nprim;
                 s.npk = pk.nprim;
+                s.pp0 = e.z;
+                s.npp = e.w;
                 s.pb_off = pb.prim_off;
                 s.pk_off = pk.prim_off;
                 for (int x = 0; x < 3; ++x) {
@@ -293,10 +299,11 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int2 *__
                     s.C[x] = pk.A[x];
                     s.CD[x] = pk.AB[x];
                 }
-                atomicMax(&s_maxpp, s.npb * s.npk);
+                atomicMax(&s_maxpp, s.npp);
             } else {
                 s.q.bra = -1;
-                s.npb = s.npk = 0;
+                s.npk = 1;
+                s.pp0 = s.npp = 0;
                 s.pb_off = s.pk_off = 0;
                 for (int x = 0; x < 3; ++x) s.A[x] = s.AB[x] = s.C[x] = s.CD[x] = 0.0;
             }
@@ -315,9 +322,9 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int2 *__
             for (int t = tid; t < NSQ * NR; t += kBlockThreads) {
                 const int s = t / NR, r = t - s * NR;
                 const SlotData &S = sd[s];
-                const int np = S.npb * S.npk;
-                if (pp < np) {
-                    const int jb = pp / S.npk, jk = pp - jb * S.npk;
+                if (pp < S.npp) {
+                    const int g = S.pp0 + pp;
+                    const int jb = g / S.npk, jk = g - jb * S.npk;
                     const PrimPair P = prims[S.pb_off + jb];
                     const PrimPair Q = prims[S.pk_off + jk];
                     const double zpe = P.zeta + Q.zeta;
@@ -409,7 +416,7 @@ __host__ __device__ constexpr int pc_la(int c) { return c == 0 ? 0 : (c <= 2 ? 1
 __host__ __device__ constexpr int pc_lb(int c) { return c == 0 ? 0 : (c == 1 ? 0 : (c == 2 ? 1 : c - 3)); }
 
 template <int LA, int LB, int LC, int LD, typename R, class Epi>
-inline cudaError_t launch_eri_class(const int2 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+inline cudaError_t launch_eri_class(const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                                     const Epi &epi, cudaStream_t st, int nsm)
 {
     if (nq <= 0) return cudaSuccess;
@@ -436,7 +443,7 @@ inline cudaError_t launch_eri_class(const int2 *list, int nq, const PairInfo *pa
 
 // Run class `qc` (0..20): bra pair class cb >= ket pair class ck.
 template <typename R, class Epi>
-inline cudaError_t launch_eri(int qc, const int2 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+inline cudaError_t launch_eri(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                               const Epi &epi, cudaStream_t st, int nsm)
 {
 #define PQB_CASE(CB, CK)                                                                                       \

@@ -3,7 +3,7 @@
 #include "eri_launch.h"
 
 namespace pqb {
-cudaError_t launch_packed_f64(int qc, const int2 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+cudaError_t launch_packed_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                               double *out, const double *fscale, cudaStream_t st, int nsm)
 {
     EpiPacked epi{out, fscale};

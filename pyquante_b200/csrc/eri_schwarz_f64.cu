@@ -3,7 +3,7 @@
 #include "eri_launch.h"
 
 namespace pqb {
-cudaError_t launch_schwarz_f64(int qc, const int2 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+cudaError_t launch_schwarz_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                                unsigned long long *Q2bits, const double *fscale, cudaStream_t st, int nsm)
 {
     EpiSchwarz epi{Q2bits, fscale};

@@ -36,17 +36,21 @@ struct pqb_ctx {
     std::vector<double> Q;           // Schwarz factors (host)
     bool have_q = false;
     // unscreened lists (packed integrals): per class offset/count into d_full
-    int2 *d_full = nullptr;
+    int4 *d_full = nullptr;
     int64_t full_off[kNumQuartetClass] = {0}, full_cnt[kNumQuartetClass] = {0};
     // Schwarz (diagonal) list
-    int2 *d_diag = nullptr;
+    int4 *d_diag = nullptr;
     int64_t diag_off[kNumQuartetClass] = {0}, diag_cnt[kNumQuartetClass] = {0};
     // screened plan: [0] FP64 part, [1] FP32-eligible part
-    int2 *d_plan = nullptr;
+    int4 *d_plan = nullptr;
     size_t plan_cap = 0;
     int64_t plan_off[2][kNumQuartetClass] = {{0}}, plan_cnt[2][kNumQuartetClass] = {{0}};
     int64_t plan_prims[2][kNumQuartetClass] = {{0}};
-    std::vector<int2> plan_h;        // host copy of the plan (for sharding)
+    std::vector<int4> plan_h;        // host copy of the plan (for sharding)
+    // fork/join streams for concurrent class launches
+    static constexpr int kStreams = 8;
+    cudaStream_t streams[kStreams] = {nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[kStreams] = {nullptr};
     bool have_plan = false;
     // small scratch
     double *d_atoms = nullptr;
@@ -511,6 +515,18 @@ int pqb_create(pqb_ctx **out, int device)
     return PQB_OK;
 }
 
+static cudaError_t ensure_streams(pqb_ctx *ctx)
+{
+    if (ctx->ev_fork) return cudaSuccess;
+    for (int k = 0; k < pqb_ctx::kStreams; ++k) {
+        cudaError_t e = cudaStreamCreateWithFlags(&ctx->streams[k], cudaStreamNonBlocking);
+        if (e != cudaSuccess) return e;
+        e = cudaEventCreateWithFlags(&ctx->ev_join[k], cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+}
+
 static void release_basis(pqb_ctx *ctx)
 {
     free_dev(ctx->d_pairs);
@@ -535,6 +551,11 @@ void pqb_destroy(pqb_ctx *ctx)
     cudaSetDevice(ctx->device);
     release_basis(ctx);
     free_dev(ctx->d_atoms);
+    for (int k = 0; k < pqb_ctx::kStreams; ++k) {
+        if (ctx->streams[k]) cudaStreamDestroy(ctx->streams[k]);
+        if (ctx->ev_join[k]) cudaEventDestroy(ctx->ev_join[k]);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     delete ctx;
 }
 
@@ -547,34 +568,38 @@ int pqb_last_error(const pqb_ctx *ctx, char *buf, size_t len)
 
 int pqb_num_pairs(const pqb_ctx *ctx) { return ctx ? (int)ctx->pairs.size() : 0; }
 
-// Bucket quartet (bra, ket) lists by class, each class sorted by descending
-// primitive-quartet count (block-mode kernels advance their quartets in
-// lockstep over primitive quartets).
-static void bucket_sorted(const std::vector<PairInfo> &pairs, std::vector<std::vector<int2>> &cls,
-                          std::vector<int2> &flat, int64_t *off, int64_t *cnt)
+// Bucket work items by class, each class sorted by descending primitive-
+// quartet count (block-mode kernels advance their items in lockstep over
+// primitive quartets; thread-mode warps then get similar trip counts).
+static void bucket_sorted(std::vector<std::vector<int4>> &cls, std::vector<int4> &flat, int64_t *off, int64_t *cnt)
 {
     flat.clear();
     for (int c = 0; c < kNumQuartetClass; ++c) {
         auto &v = cls[c];
         int maxp = 1;
-        for (auto &e : v) maxp = std::max(maxp, pairs[e.x].nprim * pairs[e.y].nprim);
+        for (auto &e : v) maxp = std::max(maxp, e.w);
         std::vector<int64_t> hist(maxp + 2, 0);
-        for (auto &e : v) hist[maxp - pairs[e.x].nprim * pairs[e.y].nprim]++;
+        for (auto &e : v) hist[maxp - e.w]++;
         int64_t s = 0;
         for (auto &h : hist) {
             int64_t t = h;
             h = s;
             s += t;
         }
-        std::vector<int2> sorted(v.size());
-        for (auto &e : v) sorted[hist[maxp - pairs[e.x].nprim * pairs[e.y].nprim]++] = e;
+        std::vector<int4> sorted(v.size());
+        for (auto &e : v) sorted[hist[maxp - e.w]++] = e;
         off[c] = (int64_t)flat.size();
         cnt[c] = (int64_t)sorted.size();
         flat.insert(flat.end(), sorted.begin(), sorted.end());
     }
 }
 
-static inline int2 oriented_quartet(const std::vector<PairInfo> &pairs, int p, int q, int &qc)
+// Primitive-quartet chunk for the J/K work items: long contractions
+// (up to 1296 primitive quartets for a 6-primitive s shell to the fourth)
+// are cut so no thread or block slot runs a long serial chain.
+static const int kChunk = 16;
+
+static inline int4 oriented_quartet(const std::vector<PairInfo> &pairs, int p, int q, int &qc)
 {
     int cp = pairs[p].cls, cq = pairs[q].cls;
     if (cp < cq) {
@@ -582,7 +607,7 @@ static inline int2 oriented_quartet(const std::vector<PairInfo> &pairs, int p, i
         std::swap(cp, cq);
     }
     qc = quartet_class(cp, cq);
-    return make_int2(p, q);
+    return make_int4(p, q, 0, pairs[p].nprim * pairs[q].nprim);
 }
 
 int pqb_shells_upload(pqb_ctx *ctx, int nshell, const int *shell_l, const int *shell_nprim, const int *prim_off,
@@ -657,22 +682,23 @@ int pqb_shells_upload(pqb_ctx *ctx, int nshell, const int *shell_l, const int *s
     PQB_CK(ctx, cudaMemcpy(ctx->d_prims, prims.data(), sizeof(PrimPair) * prims.size(), cudaMemcpyHostToDevice));
     PQB_CK(ctx, cudaMemcpy(ctx->d_fscale, fscale, sizeof(double) * nbf, cudaMemcpyHostToDevice));
     // unscreened quartet list (packed integrals) and diagonal list (Schwarz)
-    std::vector<std::vector<int2>> cls(kNumQuartetClass), dcls(kNumQuartetClass);
+    std::vector<std::vector<int4>> cls(kNumQuartetClass), dcls(kNumQuartetClass);
     for (int p = 0; p < np; ++p) {
         int qc;
-        dcls[quartet_class(pairs[p].cls, pairs[p].cls)].push_back(make_int2(p, p));
+        dcls[quartet_class(pairs[p].cls, pairs[p].cls)].push_back(
+            make_int4(p, p, 0, pairs[p].nprim * pairs[p].nprim));
         for (int q = 0; q <= p; ++q) {
-            int2 e = oriented_quartet(pairs, p, q, qc);
+            int4 e = oriented_quartet(pairs, p, q, qc);
             cls[qc].push_back(e);
         }
     }
-    std::vector<int2> flat;
-    bucket_sorted(pairs, cls, flat, ctx->full_off, ctx->full_cnt);
-    PQB_CK(ctx, cudaMalloc(&ctx->d_full, sizeof(int2) * std::max<size_t>(flat.size(), 1)));
-    PQB_CK(ctx, cudaMemcpy(ctx->d_full, flat.data(), sizeof(int2) * flat.size(), cudaMemcpyHostToDevice));
-    bucket_sorted(pairs, dcls, flat, ctx->diag_off, ctx->diag_cnt);
-    PQB_CK(ctx, cudaMalloc(&ctx->d_diag, sizeof(int2) * std::max<size_t>(flat.size(), 1)));
-    PQB_CK(ctx, cudaMemcpy(ctx->d_diag, flat.data(), sizeof(int2) * flat.size(), cudaMemcpyHostToDevice));
+    std::vector<int4> flat;
+    bucket_sorted(cls, flat, ctx->full_off, ctx->full_cnt);
+    PQB_CK(ctx, cudaMalloc(&ctx->d_full, sizeof(int4) * std::max<size_t>(flat.size(), 1)));
+    PQB_CK(ctx, cudaMemcpy(ctx->d_full, flat.data(), sizeof(int4) * flat.size(), cudaMemcpyHostToDevice));
+    bucket_sorted(dcls, flat, ctx->diag_off, ctx->diag_cnt);
+    PQB_CK(ctx, cudaMalloc(&ctx->d_diag, sizeof(int4) * std::max<size_t>(flat.size(), 1)));
+    PQB_CK(ctx, cudaMemcpy(ctx->d_diag, flat.data(), sizeof(int4) * flat.size(), cudaMemcpyHostToDevice));
     return PQB_OK;
 }
 
@@ -708,7 +734,7 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
     const auto &pairs = ctx->pairs;
     const auto &Q = ctx->Q;
     const int np = (int)pairs.size();
-    std::vector<std::vector<int2>> c64(kNumQuartetClass), c32(kNumQuartetClass);
+    std::vector<std::vector<int4>> c64(kNumQuartetClass), c32(kNumQuartetClass);
     int64_t total = 0, dropped = 0;
     for (int p = 0; p < np; ++p) {
         total += p + 1;
@@ -719,34 +745,32 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
                 continue;
             }
             int qc;
-            int2 e = oriented_quartet(pairs, p, q, qc);
-            (b < fp32_thresh ? c32 : c64)[qc].push_back(e);
+            int4 e = oriented_quartet(pairs, p, q, qc);
+            auto &dst = (b < fp32_thresh ? c32 : c64)[qc];
+            for (int s0 = 0; s0 < e.w; s0 += kChunk) dst.push_back(make_int4(e.x, e.y, s0, std::min(kChunk, e.w - s0)));
         }
     }
-    std::vector<int2> f64, f32;
-    bucket_sorted(pairs, c64, f64, ctx->plan_off[0], ctx->plan_cnt[0]);
-    bucket_sorted(pairs, c32, f32, ctx->plan_off[1], ctx->plan_cnt[1]);
+    std::vector<int4> f64, f32;
+    bucket_sorted(c64, f64, ctx->plan_off[0], ctx->plan_cnt[0]);
+    bucket_sorted(c32, f32, ctx->plan_off[1], ctx->plan_cnt[1]);
     for (int c = 0; c < kNumQuartetClass; ++c) ctx->plan_off[1][c] += (int64_t)f64.size();
     const size_t need = f64.size() + f32.size();
     if (need > ctx->plan_cap) {
         free_dev(ctx->d_plan);
         ctx->d_plan = nullptr;
-        PQB_CK(ctx, cudaMalloc(&ctx->d_plan, sizeof(int2) * std::max<size_t>(need, 1)));
+        PQB_CK(ctx, cudaMalloc(&ctx->d_plan, sizeof(int4) * std::max<size_t>(need, 1)));
         ctx->plan_cap = need;
     }
     if (!f64.empty())
-        PQB_CK(ctx, cudaMemcpy(ctx->d_plan, f64.data(), sizeof(int2) * f64.size(), cudaMemcpyHostToDevice));
+        PQB_CK(ctx, cudaMemcpy(ctx->d_plan, f64.data(), sizeof(int4) * f64.size(), cudaMemcpyHostToDevice));
     if (!f32.empty())
-        PQB_CK(ctx, cudaMemcpy(ctx->d_plan + f64.size(), f32.data(), sizeof(int2) * f32.size(), cudaMemcpyHostToDevice));
+        PQB_CK(ctx, cudaMemcpy(ctx->d_plan + f64.size(), f32.data(), sizeof(int4) * f32.size(), cudaMemcpyHostToDevice));
     ctx->plan_h = f64;
     ctx->plan_h.insert(ctx->plan_h.end(), f32.begin(), f32.end());
     for (int part = 0; part < 2; ++part)
         for (int c = 0; c < kNumQuartetClass; ++c) {
             int64_t s = 0;
-            for (int64_t q = 0; q < ctx->plan_cnt[part][c]; ++q) {
-                const int2 e = ctx->plan_h[ctx->plan_off[part][c] + q];
-                s += (int64_t)pairs[e.x].nprim * pairs[e.y].nprim;
-            }
+            for (int64_t q = 0; q < ctx->plan_cnt[part][c]; ++q) s += ctx->plan_h[ctx->plan_off[part][c] + q].w;
             ctx->plan_prims[part][c] = s;
         }
     ctx->have_plan = true;
@@ -778,7 +802,7 @@ int pqb_plan_shard(pqb_ctx *ctx, int rank, int nranks)
     if (nranks == 1) return PQB_OK;
     PQB_CK(ctx, cudaSetDevice(ctx->device));
     const size_t total = ctx->plan_h.size();
-    std::vector<int2> out;
+    std::vector<int4> out;
     out.reserve(total / nranks + 64);
     int64_t off[2][kNumQuartetClass], cnt[2][kNumQuartetClass], prims[2][kNumQuartetClass];
     for (int part = 0; part < 2; ++part)
@@ -786,14 +810,14 @@ int pqb_plan_shard(pqb_ctx *ctx, int rank, int nranks)
             off[part][c] = (int64_t)out.size();
             prims[part][c] = 0;
             for (int64_t q = rank; q < ctx->plan_cnt[part][c]; q += nranks) {
-                const int2 e = ctx->plan_h[ctx->plan_off[part][c] + q];
+                const int4 e = ctx->plan_h[ctx->plan_off[part][c] + q];
                 out.push_back(e);
-                prims[part][c] += (int64_t)ctx->pairs[e.x].nprim * ctx->pairs[e.y].nprim;
+                prims[part][c] += e.w;
             }
             cnt[part][c] = (int64_t)out.size() - off[part][c];
         }
     if (!out.empty())
-        PQB_CK(ctx, cudaMemcpy(ctx->d_plan, out.data(), sizeof(int2) * out.size(), cudaMemcpyHostToDevice));
+        PQB_CK(ctx, cudaMemcpy(ctx->d_plan, out.data(), sizeof(int4) * out.size(), cudaMemcpyHostToDevice));
     memcpy(ctx->plan_off, off, sizeof off);
     memcpy(ctx->plan_cnt, cnt, sizeof cnt);
     memcpy(ctx->plan_prims, prims, sizeof prims);
@@ -833,9 +857,19 @@ int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
     if (len != P * (P + 1) / 2) return fail(ctx, PQB_E_SHAPE, "pqb_eri_packed: len %lld != %lld", (long long)len, (long long)(P * (P + 1) / 2));
     PQB_CK(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;
-    for (int c = 0; c < kNumQuartetClass; ++c)
+    PQB_CK(ctx, ensure_streams(ctx));
+    PQB_CK(ctx, cudaEventRecord(ctx->ev_fork, st));
+    for (int k = 0; k < pqb_ctx::kStreams; ++k) PQB_CK(ctx, cudaStreamWaitEvent(ctx->streams[k], ctx->ev_fork, 0));
+    for (int c = kNumQuartetClass - 1, k = 0; c >= 0; --c) {
+        if (ctx->full_cnt[c] == 0) continue;
         PQB_CK(ctx, launch_packed_f64(c, ctx->d_full + ctx->full_off[c], (int)ctx->full_cnt[c], ctx->d_pairs,
-                                      ctx->d_prims, out, ctx->d_fscale, st, ctx->nsm));
+                                      ctx->d_prims, out, ctx->d_fscale, ctx->streams[k++ % pqb_ctx::kStreams],
+                                      ctx->nsm));
+    }
+    for (int k = 0; k < pqb_ctx::kStreams; ++k) {
+        PQB_CK(ctx, cudaEventRecord(ctx->ev_join[k], ctx->streams[k]));
+        PQB_CK(ctx, cudaStreamWaitEvent(st, ctx->ev_join[k], 0));
+    }
     return PQB_OK;
 }
 
@@ -849,15 +883,33 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
     const int n = ctx->nbf;
     PQB_CK(ctx, cudaMemsetAsync(J, 0, sizeof(double) * n * n, st));
     PQB_CK(ctx, cudaMemsetAsync(K, 0, sizeof(double) * n * n, st));
-    for (int c = kNumQuartetClass - 1; c >= 0; --c) {
-        PQB_CK(ctx, launch_jk_f64(c, ctx->d_plan + ctx->plan_off[0][c], (int)ctx->plan_cnt[0][c], ctx->d_pairs,
-                                  ctx->d_prims, D, J, K, ctx->d_fscale, n, st, ctx->nsm));
-        if (mode == PQB_MIXED)
-            PQB_CK(ctx, launch_jk_f32(c, ctx->d_plan + ctx->plan_off[1][c], (int)ctx->plan_cnt[1][c], ctx->d_pairs,
-                                      ctx->d_prims, D, J, K, ctx->d_fscale, n, st, ctx->nsm));
+    PQB_CK(ctx, ensure_streams(ctx));
+    // fork: class launches spread over the context's streams, heaviest first
+    PQB_CK(ctx, cudaEventRecord(ctx->ev_fork, st));
+    for (int k = 0; k < pqb_ctx::kStreams; ++k) PQB_CK(ctx, cudaStreamWaitEvent(ctx->streams[k], ctx->ev_fork, 0));
+    int order[2 * kNumQuartetClass];
+    double cost[2 * kNumQuartetClass];
+    for (int i = 0; i < 2 * kNumQuartetClass; ++i) {
+        order[i] = i;
+        const int part = i / kNumQuartetClass, c = i % kNumQuartetClass;
+        cost[i] = (double)ctx->plan_prims[part][c] * (1 + c) * (part == 1 && mode == PQB_MIXED ? 0.5 : 1.0);
+    }
+    std::sort(order, order + 2 * kNumQuartetClass, [&](int a, int b) { return cost[a] > cost[b]; });
+    for (int i = 0, k = 0; i < 2 * kNumQuartetClass; ++i) {
+        const int part = order[i] / kNumQuartetClass, c = order[i] % kNumQuartetClass;
+        const int nq = (int)ctx->plan_cnt[part][c];
+        if (nq == 0) continue;
+        cudaStream_t sk = ctx->streams[k++ % pqb_ctx::kStreams];
+        const int4 *list = ctx->d_plan + ctx->plan_off[part][c];
+        if (part == 1 && mode == PQB_MIXED)
+            PQB_CK(ctx, launch_jk_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, D, J, K, ctx->d_fscale, n, sk, ctx->nsm));
         else
-            PQB_CK(ctx, launch_jk_f64(c, ctx->d_plan + ctx->plan_off[1][c], (int)ctx->plan_cnt[1][c], ctx->d_pairs,
-                                      ctx->d_prims, D, J, K, ctx->d_fscale, n, st, ctx->nsm));
+            PQB_CK(ctx, launch_jk_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, D, J, K, ctx->d_fscale, n, sk, ctx->nsm));
+    }
+    // join
+    for (int k = 0; k < pqb_ctx::kStreams; ++k) {
+        PQB_CK(ctx, cudaEventRecord(ctx->ev_join[k], ctx->streams[k]));
+        PQB_CK(ctx, cudaStreamWaitEvent(st, ctx->ev_join[k], 0));
     }
     const int64_t P = (int64_t)n * (n + 1) / 2;
     symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, n);
@@ -874,7 +926,7 @@ int pqb_jk_direct_class(pqb_ctx *ctx, const double *D, double *Jacc, double *Kac
     if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_jk_direct_class: call pqb_plan first");
     PQB_CK(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;
-    const int2 *list = ctx->d_plan + ctx->plan_off[part][qclass];
+    const int4 *list = ctx->d_plan + ctx->plan_off[part][qclass];
     const int nq = (int)ctx->plan_cnt[part][qclass];
     if (mode == PQB_MIXED && part == 1)
         PQB_CK(ctx, launch_jk_f32(qclass, list, nq, ctx->d_pairs, ctx->d_prims, D, Jacc, Kacc, ctx->d_fscale, ctx->nbf,
