@@ -37,18 +37,28 @@ __device__ __forceinline__ int64_t fpair(int i, int j)
 }
 
 // ------------------------------------------------------------ epilogues --
+// Every epilogue offers
+//   thread_quartet<LA,LB,LC,LD>(q, acc[NAB*NCD])   whole quartet, thread mode
+//   block_ab<LA,LB,LC,LD>(q, ia, ib, acc[NCD], scr) one bra component pair,
+//                                                    block mode (scr: per-slot
+//                                                    shared scratch)
+//   block_flush<LA,LB,LC,LD>(q, scr, t, nt)          after a block barrier
+//   kScratch<LA,LB,LC,LD>                            doubles of scr per slot
+
+__device__ __forceinline__ bool skip_bra(const QCtx &q, int fi, int fj) { return q.sa == q.sb && fi < fj; }
 
 // Packed canonical integrals at ijkl2intindex (Src/cints.c:413-425), 64-bit.
 struct EpiPacked {
     double *out;
     const double *fscale;
-    static constexpr bool kNeedsSlotReduce = false;
+    template <int LA, int LB, int LC, int LD>
+    static constexpr int kScratch = 0;
     template <int LC, int LD, typename R>
-    __device__ __forceinline__ void ab_block(const QCtx &q, int ia, int ib, const R *acc, double *) const
+    __device__ __forceinline__ void ab(const QCtx &q, int ia, int ib, const R *acc) const
     {
         constexpr int NC = ncart(LC), ND = ncart(LD);
         const int fi = q.fa + ia, fj = q.fb + ib;
-        if (q.sa == q.sb && fi < fj) return;
+        if (skip_bra(q, fi, fj)) return;
         const int64_t IJ = fpair(fi, fj);
         const double sij = fscale[fi] * fscale[fj];
 #pragma unroll
@@ -63,8 +73,20 @@ struct EpiPacked {
                 out[hi * (hi + 1) / 2 + lo] = (double)acc[ic * ND + id] * sij * fscale[fk] * fscale[fl];
             }
     }
-    template <int LC, int LD>
-    __device__ __forceinline__ void finish_jkl(const QCtx &, const double *) const {}
+    template <int LA, int LB, int LC, int LD, typename R>
+    __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc) const
+    {
+        constexpr int NB = ncart(LB), NCD = ncart(LC) * ncart(LD);
+#pragma unroll
+        for (int ab = 0; ab < ncart(LA) * NB; ++ab) this->ab<LC, LD, R>(q, ab / NB, ab % NB, acc + ab * NCD);
+    }
+    template <int LA, int LB, int LC, int LD, typename R>
+    __device__ __forceinline__ void block_ab(const QCtx &q, int ia, int ib, const R *acc, double *) const
+    {
+        ab<LC, LD, R>(q, ia, ib, acc);
+    }
+    template <int LA, int LB, int LC, int LD>
+    __device__ __forceinline__ void block_flush(const QCtx &, double *, int, int) const {}
 };
 
 // Direct J/K digestion of unique quartets with 8-fold degeneracy weights:
@@ -73,28 +95,34 @@ struct EpiPacked {
 // v' = v * (1/2 if i==j) (1/2 if k==l) (1/2 if ij==kl); then J = Jacc + Jacc^T,
 // K = Kacc + Kacc^T reproduce J_ij = sum_kl (ij|kl) D_kl and
 // K_ij = sum_kl (ik|jl) D_kl of PyQuante/Ints.py:195-223 for symmetric D.
+// Contributions are first summed per quartet into its six J/K blocks
+// (ab, cd, ac, ad, bc, bd) and then added to global memory once per block
+// element, so a quartet costs NA NB + NC ND + (NA+NB)(NC+ND) atomics.
 struct EpiJK {
     const double *D;
     double *Jacc, *Kacc;
     const double *fscale;
     int n;
-    static constexpr bool kNeedsSlotReduce = true;
-    template <int LC, int LD, typename R>
-    __device__ __forceinline__ void ab_block(const QCtx &q, int ia, int ib, const R *acc, double *jkl) const
+    template <int LA, int LB, int LC, int LD>
+    static constexpr int kScratch = ncart(LA) * ncart(LB) + ncart(LC) * ncart(LD) +
+                                    (ncart(LA) + ncart(LB)) * (ncart(LC) + ncart(LD));
+
+    // digest one bra component pair: returns 2*sum_kl v' D_kl (the Jacc[i,j]
+    // term) and adds the other five block contributions through the sinks
+    template <int LC, int LD, typename R, class Sink>
+    __device__ __forceinline__ double ab(const QCtx &q, int ia, int ib, const R *acc, Sink &&sink) const
     {
         constexpr int NC = ncart(LC), ND = ncart(LD);
         const int fi = q.fa + ia, fj = q.fb + ib;
-        if (q.sa == q.sb && fi < fj) return;
+        if (skip_bra(q, fi, fj)) return 0.0;
         const int64_t IJ = fpair(fi, fj);
         const double sij = fscale[fi] * fscale[fj] * (fi == fj ? 0.5 : 1.0);
         const double Dij = __ldg(D + (int64_t)fi * n + fj);
-        double jij = 0.0, kik[NC], kjk[NC], kil[ND], kjl[ND];
+        const double *Di = D + (int64_t)fi * n, *Dj = D + (int64_t)fj * n;
+        double jij = 0.0;
 #pragma unroll
-        for (int c = 0; c < NC; ++c) kik[c] = kjk[c] = 0.0;
-#pragma unroll
-        for (int d = 0; d < ND; ++d) kil[d] = kjl[d] = 0.0;
-#pragma unroll
-        for (int ic = 0; ic < NC; ++ic)
+        for (int ic = 0; ic < NC; ++ic) {
+            double kik = 0.0, kjk = 0.0;
 #pragma unroll
             for (int id = 0; id < ND; ++id) {
                 const int fk = q.fc + ic, fl = q.fd + id;
@@ -104,31 +132,112 @@ struct EpiJK {
                 const double v = (double)acc[ic * ND + id] * sij * fscale[fk] * fscale[fl] *
                                  (fk == fl ? 0.5 : 1.0) * (IJ == KL ? 0.5 : 1.0);
                 jij += v * __ldg(D + (int64_t)fk * n + fl);
-                jkl[ic * ND + id] += v * Dij;
-                kik[ic] += v * __ldg(D + (int64_t)fj * n + fl);
-                kjk[ic] += v * __ldg(D + (int64_t)fi * n + fl);
-                kil[id] += v * __ldg(D + (int64_t)fj * n + fk);
-                kjl[id] += v * __ldg(D + (int64_t)fi * n + fk);
+                sink.jcd(ic * ND + id, 2.0 * v * Dij);
+                kik += v * __ldg(Dj + fl);
+                kjk += v * __ldg(Di + fl);
+                sink.kad(ia, id, v * __ldg(Dj + fk));
+                sink.kbd(ib, id, v * __ldg(Di + fk));
             }
-        atomicAdd(Jacc + (int64_t)fi * n + fj, 2.0 * jij);
-#pragma unroll
-        for (int ic = 0; ic < NC; ++ic) {
-            atomicAdd(Kacc + (int64_t)fi * n + q.fc + ic, kik[ic]);
-            atomicAdd(Kacc + (int64_t)fj * n + q.fc + ic, kjk[ic]);
+            sink.kac(ia, ic, kik);
+            sink.kbc(ib, ic, kjk);
         }
-#pragma unroll
-        for (int id = 0; id < ND; ++id) {
-            atomicAdd(Kacc + (int64_t)fi * n + q.fd + id, kil[id]);
-            atomicAdd(Kacc + (int64_t)fj * n + q.fd + id, kjl[id]);
-        }
+        return 2.0 * jij;
     }
-    // jkl[cd] summed over every bra component pair of the quartet
-    template <int LC, int LD>
-    __device__ __forceinline__ void finish_one(const QCtx &q, int cd, double v) const
+
+    // thread mode: block sums in registers, then one atomic per element
+    template <int LA, int LB, int LC, int LD, typename R>
+    __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc) const
     {
-        constexpr int ND = ncart(LD);
-        const int fk = q.fc + cd / ND, fl = q.fd + cd % ND;
-        if (v != 0.0) atomicAdd(Jacc + (int64_t)fk * n + fl, 2.0 * v);
+        constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NCD = NC * ND;
+        struct Regs {
+            double jcd_[NCD], kac_[NC], kad_[ND], kbc_[NB][NC], kbd_[NB][ND];
+            __device__ void jcd(int c, double v) { jcd_[c] += v; }
+            __device__ void kac(int, int c, double v) { kac_[c] += v; }
+            __device__ void kad(int, int d, double v) { kad_[d] += v; }
+            __device__ void kbc(int b, int c, double v) { kbc_[b][c] += v; }
+            __device__ void kbd(int b, int d, double v) { kbd_[b][d] += v; }
+        } r;
+#pragma unroll
+        for (int c = 0; c < NCD; ++c) r.jcd_[c] = 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) r.kbc_[b][c] = 0.0;
+#pragma unroll
+            for (int d = 0; d < ND; ++d) r.kbd_[b][d] = 0.0;
+        }
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) r.kac_[c] = 0.0;
+#pragma unroll
+            for (int d = 0; d < ND; ++d) r.kad_[d] = 0.0;
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib) {
+                const double jij = ab<LC, LD, R>(q, ia, ib, acc + (ia * NB + ib) * NCD, r);
+                if (jij != 0.0) atomicAdd(Jacc + (int64_t)(q.fa + ia) * n + q.fb + ib, jij);
+            }
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+                if (r.kac_[c] != 0.0) atomicAdd(Kacc + (int64_t)(q.fa + ia) * n + q.fc + c, r.kac_[c]);
+#pragma unroll
+            for (int d = 0; d < ND; ++d)
+                if (r.kad_[d] != 0.0) atomicAdd(Kacc + (int64_t)(q.fa + ia) * n + q.fd + d, r.kad_[d]);
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+                if (r.kbc_[b][c] != 0.0) atomicAdd(Kacc + (int64_t)(q.fb + b) * n + q.fc + c, r.kbc_[b][c]);
+#pragma unroll
+            for (int d = 0; d < ND; ++d)
+                if (r.kbd_[b][d] != 0.0) atomicAdd(Kacc + (int64_t)(q.fb + b) * n + q.fd + d, r.kbd_[b][d]);
+        }
+#pragma unroll
+        for (int c = 0; c < NCD; ++c)
+            if (r.jcd_[c] != 0.0) atomicAdd(Jacc + (int64_t)(q.fc + c / ND) * n + q.fd + c % ND, r.jcd_[c]);
+    }
+
+    // block mode: scratch layout [jab NAB | jcd NCD | kac NA*NC | kad NA*ND | kbc NB*NC | kbd NB*ND]
+    template <int LA, int LB, int LC, int LD, typename R>
+    __device__ __forceinline__ void block_ab(const QCtx &q, int ia, int ib, const R *acc, double *scr) const
+    {
+        constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+        struct Smem {
+            double *s;
+            __device__ void jcd(int c, double v) { atomicAdd(s + NA * NB + c, v); }
+            __device__ void kac(int a, int c, double v) { atomicAdd(s + NA * NB + NC * ND + a * NC + c, v); }
+            __device__ void kad(int a, int d, double v) { atomicAdd(s + NA * NB + NC * ND + NA * NC + a * ND + d, v); }
+            __device__ void kbc(int b, int c, double v)
+            {
+                atomicAdd(s + NA * NB + NC * ND + NA * NC + NA * ND + b * NC + c, v);
+            }
+            __device__ void kbd(int b, int d, double v)
+            {
+                atomicAdd(s + NA * NB + NC * ND + NA * NC + NA * ND + NB * NC + b * ND + d, v);
+            }
+        } sm{scr};
+        scr[ia * NB + ib] = ab<LC, LD, R>(q, ia, ib, acc, sm);
+    }
+    template <int LA, int LB, int LC, int LD>
+    __device__ __forceinline__ void block_flush(const QCtx &q, const double *scr, int t, int nt) const
+    {
+        constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+        constexpr int O1 = NA * NB, O2 = O1 + NC * ND, O3 = O2 + NA * NC, O4 = O3 + NA * ND, O5 = O4 + NB * NC,
+                      O6 = O5 + NB * ND;
+        for (int e = t; e < O6; e += nt) {
+            const double v = scr[e];
+            if (v == 0.0) continue;
+            int row, col;
+            double *M = Kacc;
+            if (e < O1) { row = q.fa + e / NB; col = q.fb + e % NB; M = Jacc; }
+            else if (e < O2) { row = q.fc + (e - O1) / ND; col = q.fd + (e - O1) % ND; M = Jacc; }
+            else if (e < O3) { row = q.fa + (e - O2) / NC; col = q.fc + (e - O2) % NC; }
+            else if (e < O4) { row = q.fa + (e - O3) / ND; col = q.fd + (e - O3) % ND; }
+            else if (e < O5) { row = q.fb + (e - O4) / NC; col = q.fc + (e - O4) % NC; }
+            else { row = q.fb + (e - O5) / ND; col = q.fd + (e - O5) % ND; }
+            atomicAdd(M + (int64_t)row * n + col, v);
+        }
     }
 };
 
@@ -136,9 +245,10 @@ struct EpiJK {
 struct EpiSchwarz {
     unsigned long long *Q2bits;   // bit patterns of non-negative doubles
     const double *fscale;
-    static constexpr bool kNeedsSlotReduce = false;
+    template <int LA, int LB, int LC, int LD>
+    static constexpr int kScratch = 0;
     template <int LC, int LD, typename R>
-    __device__ __forceinline__ void ab_block(const QCtx &q, int ia, int ib, const R *acc, double *) const
+    __device__ __forceinline__ void ab(const QCtx &q, int ia, int ib, const R *acc) const
     {
         constexpr int ND = ncart(LD), NCD = ncart(LC) * ncart(LD);
         const int cd = ia * ND + ib;   // (ic, id) == (ia, ib) on a diagonal quartet
@@ -150,8 +260,20 @@ struct EpiSchwarz {
         v = fabs(v) * s * s;
         atomicMax(Q2bits + q.bra, (unsigned long long)__double_as_longlong(v));
     }
-    template <int LC, int LD>
-    __device__ __forceinline__ void finish_one(const QCtx &, int, double) const {}
+    template <int LA, int LB, int LC, int LD, typename R>
+    __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc) const
+    {
+        constexpr int NB = ncart(LB), NCD = ncart(LC) * ncart(LD);
+#pragma unroll
+        for (int ab = 0; ab < ncart(LA) * NB; ++ab) this->ab<LC, LD, R>(q, ab / NB, ab % NB, acc + ab * NCD);
+    }
+    template <int LA, int LB, int LC, int LD, typename R>
+    __device__ __forceinline__ void block_ab(const QCtx &q, int ia, int ib, const R *acc, double *) const
+    {
+        ab<LC, LD, R>(q, ia, ib, acc);
+    }
+    template <int LA, int LB, int LC, int LD>
+    __device__ __forceinline__ void block_flush(const QCtx &, double *, int, int) const {}
 };
 
 // ---------------------------------------------------------- thread mode --
@@ -179,68 +301,57 @@ __global__ void __launch_bounds__(128) eri_thread_kernel(const int4 *__restrict_
         int ib = e.z / npk, ik = e.z - (e.z / npk) * npk;
         for (int t = 0; t < e.w; ++t) {
             const PrimPair P = prims[pb.prim_off + ib];
-            {
-                const PrimPair Q = prims[pk.prim_off + ik];
-                if (++ik == npk) {
-                    ik = 0;
-                    ++ib;
-                }
-                const double zpe = P.zeta + Q.zeta;
-                const double PQx = P.P[0] - Q.P[0], PQy = P.P[1] - Q.P[1], PQz = P.P[2] - Q.P[2];
-                const double T = P.zeta * Q.zeta / zpe * (PQx * PQx + PQy * PQy + PQz * PQz);
-                const double pre = P.K * Q.K * rsqrt(zpe);
+            const PrimPair Q = prims[pk.prim_off + ik];
+            if (++ik == npk) {
+                ik = 0;
+                ++ib;
+            }
+            const double zpe = P.zeta + Q.zeta;
+            const double PQx = P.P[0] - Q.P[0], PQy = P.P[1] - Q.P[1], PQz = P.P[2] - Q.P[2];
+            const double T = P.zeta * Q.zeta / zpe * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pre = P.K * Q.K * rsqrt(zpe);
 #pragma unroll
-                for (int r = 0; r < NR; ++r) {
-                    double u, w;
-                    rys_root(NR, r, T, u, w);
-                    R gx[G2D], gy[G2D], gz[G2D];
-                    rys2d<LA, LB, LC, LD, R>(u, P.zeta, Q.zeta, P.P[0] - Ax, Q.P[0] - Cx, PQx, ABx, CDx, w * pre, gx);
-                    rys2d<LA, LB, LC, LD, R>(u, P.zeta, Q.zeta, P.P[1] - Ay, Q.P[1] - Cy, PQy, ABy, CDy, 1.0, gy);
-                    rys2d<LA, LB, LC, LD, R>(u, P.zeta, Q.zeta, P.P[2] - Az, Q.P[2] - Cz, PQz, ABz, CDz, 1.0, gz);
+            for (int r = 0; r < NR; ++r) {
+                double u, w;
+                rys_root(NR, r, T, u, w);
+                R gx[G2D], gy[G2D], gz[G2D];
+                rys2d<LA, LB, LC, LD, R>(u, P.zeta, Q.zeta, P.P[0] - Ax, Q.P[0] - Cx, PQx, ABx, CDx, w * pre, gx);
+                rys2d<LA, LB, LC, LD, R>(u, P.zeta, Q.zeta, P.P[1] - Ay, Q.P[1] - Cy, PQy, ABy, CDy, 1.0, gy);
+                rys2d<LA, LB, LC, LD, R>(u, P.zeta, Q.zeta, P.P[2] - Az, Q.P[2] - Cz, PQz, ABz, CDz, 1.0, gz);
 #pragma unroll
-                    for (int ab = 0; ab < NAB; ++ab)
+                for (int ab = 0; ab < NAB; ++ab)
 #pragma unroll
-                        for (int cd = 0; cd < NCD; ++cd) {
-                            constexpr int dummy = 0;
-                            (void)dummy;
-                            const int ia = ab / NB, ib2 = ab % NB, ic = cd / ND, id = cd % ND;
-                            const int ox = ((cart_lx(LA, ia) * (LB + 1) + cart_lx(LB, ib2)) * (LC + 1) + cart_lx(LC, ic)) *
-                                               (LD + 1) + cart_lx(LD, id);
-                            const int oy = ((cart_ly(LA, ia) * (LB + 1) + cart_ly(LB, ib2)) * (LC + 1) + cart_ly(LC, ic)) *
-                                               (LD + 1) + cart_ly(LD, id);
-                            const int oz = ((cart_lz(LA, ia) * (LB + 1) + cart_lz(LB, ib2)) * (LC + 1) + cart_lz(LC, ic)) *
-                                               (LD + 1) + cart_lz(LD, id);
-                            acc[ab * NCD + cd] += gx[ox] * gy[oy] * gz[oz];
-                        }
-                }
+                    for (int cd = 0; cd < NCD; ++cd) {
+                        const int ia = ab / NB, ib2 = ab % NB, ic = cd / ND, id = cd % ND;
+                        const int ox = ((cart_lx(LA, ia) * (LB + 1) + cart_lx(LB, ib2)) * (LC + 1) + cart_lx(LC, ic)) *
+                                           (LD + 1) + cart_lx(LD, id);
+                        const int oy = ((cart_ly(LA, ia) * (LB + 1) + cart_ly(LB, ib2)) * (LC + 1) + cart_ly(LC, ic)) *
+                                           (LD + 1) + cart_ly(LD, id);
+                        const int oz = ((cart_lz(LA, ia) * (LB + 1) + cart_lz(LB, ib2)) * (LC + 1) + cart_lz(LC, ic)) *
+                                           (LD + 1) + cart_lz(LD, id);
+                        acc[ab * NCD + cd] += gx[ox] * gy[oy] * gz[oz];
+                    }
             }
         }
         const QCtx q{pb.fa, pb.fb, pk.fa, pk.fb, pb.sa, pb.sb, pk.sa, pk.sb, e.x, e.y};
-        double jkl[NCD];
-#pragma unroll
-        for (int c = 0; c < NCD; ++c) jkl[c] = 0.0;
-#pragma unroll
-        for (int ab = 0; ab < NAB; ++ab) epi.template ab_block<LC, LD, R>(q, ab / NB, ab % NB, acc + ab * NCD, jkl);
-        if constexpr (Epi::kNeedsSlotReduce) {
-#pragma unroll
-            for (int c = 0; c < NCD; ++c) epi.template finish_one<LC, LD>(q, c, jkl[c]);
-        }
+        epi.template thread_quartet<LA, LB, LC, LD, R>(q, acc);
     }
 }
 
 // ----------------------------------------------------------- block mode --
 constexpr int kBlockThreads = 256;
 
-template <int LA, int LB, int LC, int LD, typename R>
+template <int LA, int LB, int LC, int LD, typename R, class Epi>
 struct BlockLayout {
     static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     static constexpr int NAB = NA * NB, NCD = NC * ND;
     static constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
     static constexpr int G2D = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
     static constexpr int NSQ = kBlockThreads / NAB;
+    static constexpr int SCR = Epi::template kScratch<LA, LB, LC, LD>;
     static constexpr size_t g_bytes = ((size_t)NSQ * 3 * NR * G2D * sizeof(R) + 15) / 16 * 16;
-    static constexpr size_t jkl_bytes = (size_t)NSQ * NCD * sizeof(double);
-    static constexpr size_t bytes = g_bytes + jkl_bytes;
+    static constexpr size_t scr_bytes = (size_t)NSQ * SCR * sizeof(double);
+    static constexpr size_t bytes = g_bytes + scr_bytes;
 };
 
 struct SlotData {
@@ -257,12 +368,12 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
                                                                   const PairInfo *__restrict__ pairs,
                                                                   const PrimPair *__restrict__ prims, Epi epi)
 {
-    using Lay = BlockLayout<LA, LB, LC, LD, R>;
+    using Lay = BlockLayout<LA, LB, LC, LD, R, Epi>;
     constexpr int NB = Lay::NB, NC = Lay::NC, ND = Lay::ND, NAB = Lay::NAB, NCD = Lay::NCD;
-    constexpr int NR = Lay::NR, G2D = Lay::G2D, NSQ = Lay::NSQ;
+    constexpr int NR = Lay::NR, G2D = Lay::G2D, NSQ = Lay::NSQ, SCR = Lay::SCR;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *sg = reinterpret_cast<R *>(smem_raw);
-    double *sjkl = reinterpret_cast<double *>(smem_raw + Lay::g_bytes);
+    double *sscr = reinterpret_cast<double *>(smem_raw + Lay::g_bytes);
     __shared__ SlotData sd[NSQ];
     __shared__ SlotPrim sp[NSQ];
     __shared__ double su[NSQ][NR], sw[NSQ][NR];
@@ -308,8 +419,8 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
                 for (int x = 0; x < 3; ++x) s.A[x] = s.AB[x] = s.C[x] = s.CD[x] = 0.0;
             }
         }
-        if constexpr (Epi::kNeedsSlotReduce)
-            for (int t = tid; t < NSQ * NCD; t += kBlockThreads) sjkl[t] = 0.0;
+        if constexpr (SCR > 0)
+            for (int t = tid; t < NSQ * SCR; t += kBlockThreads) sscr[t] = 0.0;
         __syncthreads();
         const int maxpp = s_maxpp;
 
@@ -376,8 +487,6 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
                     for (int ic = 0; ic < NC; ++ic)
 #pragma unroll
                         for (int id = 0; id < ND; ++id) {
-                            constexpr int dummy = 0;
-                            (void)dummy;
                             const int cx = cart_lx(LC, ic) * (LD + 1) + cart_lx(LD, id);
                             const int cy = cart_ly(LC, ic) * (LD + 1) + cart_ly(LD, id);
                             const int cz = cart_lz(LC, ic) * (LD + 1) + cart_lz(LD, id);
@@ -386,23 +495,13 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
             }
         }
 
-        if (active && sd[slot].q.bra >= 0) {
-            double jkl[NCD];
-#pragma unroll
-            for (int c = 0; c < NCD; ++c) jkl[c] = 0.0;
-            epi.template ab_block<LC, LD, R>(sd[slot].q, ia, ib, acc, jkl);
-            if constexpr (Epi::kNeedsSlotReduce) {
-#pragma unroll
-                for (int c = 0; c < NCD; ++c)
-                    if (jkl[c] != 0.0) atomicAdd(sjkl + slot * NCD + c, jkl[c]);
-            }
-        }
-        if constexpr (Epi::kNeedsSlotReduce) {
+        if (active && sd[slot].q.bra >= 0)
+            epi.template block_ab<LA, LB, LC, LD, R>(sd[slot].q, ia, ib, acc, sscr + slot * SCR);
+        if constexpr (SCR > 0) {
             __syncthreads();
-            for (int t = tid; t < NSQ * NCD; t += kBlockThreads) {
-                const int s = t / NCD;
-                if (sd[s].q.bra >= 0) epi.template finish_one<LC, LD>(sd[s].q, t - s * NCD, sjkl[t]);
-            }
+            // flush: NAB threads per slot walk the slot's scratch
+            if (active && sd[slot].q.bra >= 0)
+                epi.template block_flush<LA, LB, LC, LD>(sd[slot].q, sscr + slot * SCR, ab, NAB);
         }
         __syncthreads();
     }
@@ -426,7 +525,7 @@ inline cudaError_t launch_eri_class(const int4 *list, int nq, const PairInfo *pa
         if (grid > nsm * 16) grid = nsm * 16;
         eri_thread_kernel<LA, LB, LC, LD, R, Epi><<<grid, 128, 0, st>>>(list, nq, pairs, prims, epi);
     } else {
-        using Lay = BlockLayout<LA, LB, LC, LD, R>;
+        using Lay = BlockLayout<LA, LB, LC, LD, R, Epi>;
         auto kern = eri_block_kernel<LA, LB, LC, LD, R, Epi>;
         static bool attr_set = false;   // per instantiation
         if (!attr_set) {

@@ -25,20 +25,14 @@ constexpr double kPairPre = 5.9149671727956128778;
 
 __host__ __device__ constexpr int ncart(int L) { return (L + 1) * (L + 2) / 2; }
 // x / y / z exponent of cartesian component i of a shell of angular momentum L,
-// PyQuante order: x from L down to 0, then y from L-x down to 0.
-__host__ __device__ constexpr int cart_lx(int L, int i)
-{
-    int x = L;
-    while (i >= L - x + 1) { i -= L - x + 1; --x; }
-    return x;
-}
-__host__ __device__ constexpr int cart_ly(int L, int i)
-{
-    int x = L;
-    while (i >= L - x + 1) { i -= L - x + 1; --x; }
-    return L - x - i;
-}
-__host__ __device__ constexpr int cart_lz(int L, int i) { return L - cart_lx(L, i) - cart_ly(L, i); }
+// PyQuante order (x from L down to 0, then y from L-x down to 0).  With
+// n = L - x = number of completed "x levels" before i (closed form for
+// L <= 4): x = L - n, z = i - n(n+1)/2, y = n - z.  Plain integer arithmetic
+// so unrolled loops fold every index to a constant.
+__host__ __device__ constexpr int cart_n(int i) { return (i >= 1) + (i >= 3) + (i >= 6) + (i >= 10); }
+__host__ __device__ constexpr int cart_lx(int L, int i) { return L - cart_n(i); }
+__host__ __device__ constexpr int cart_lz(int L, int i) { return i - cart_n(i) * (cart_n(i) + 1) / 2; }
+__host__ __device__ constexpr int cart_ly(int L, int i) { return cart_n(i) - cart_lz(L, i); }
 __host__ __device__ constexpr int cart_l(int L, int i, int axis)
 {
     return axis == 0 ? cart_lx(L, i) : (axis == 1 ? cart_ly(L, i) : cart_lz(L, i));
