@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--profile-builds", type=int, default=0,
+                   help="run this many untimed Fock builds after setup and exit (for ncu captures)")
     return p.parse_args()
 
 
@@ -224,6 +226,12 @@ def main():
             dist.all_reduce(K)
         _, C = geigh(ht + 2 * J - K, St)
     D = mkdens(C, 0, nocc).contiguous()
+    if a.profile_builds:
+        for _ in range(a.profile_builds):
+            eng.jk(D, a.precision, SCHWARZ, FP32_THRESH)
+        torch.cuda.synchronize()
+        print("profile builds done")
+        return
     J = torch.empty_like(D)
     K = torch.empty_like(D)
     G = torch.empty_like(D)
