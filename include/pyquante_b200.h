@@ -130,6 +130,24 @@ int pqb_oneint(pqb_ctx *ctx, int n, const double *origin, const int *powers, con
                const double *cn, const double *norms, int natoms, const double *atom_xyz, const double *atom_z,
                double *S, double *T, double *V, void *stream);
 
+/* Allocation-free variant of pqb_oneint, for callers that may not allocate
+ * device memory: code running where a framework's memory pool owns the GPU,
+ * inside a region that must not trigger allocation, or with a fixed memory
+ * budget.  No counterpart in the reference.  Differences from pqb_oneint:
+ * no context argument, atom_xyz[3*natoms] and atom_z[natoms] are DEVICE
+ * arrays, and the packed atom table the kernel reads lives in a file-scope
+ * device array of PQB_NOALLOC_MAX_ATOMS = 4096 atoms (128 KiB per GPU, held
+ * until exit); natoms above that returns PQB_E_SHAPE.  It calls no
+ * cudaMalloc/cudaFree.  The first call on each device looks the array's
+ * address up (cudaGetSymbolAddress, that device current); make that first
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU (e.g. on two streams) race; each call rewrites the
+ * entries it uses, so nothing needs clearing.  Status codes only (no
+ * context, so no pqb_last_error message). */
+int pqb_oneint_noalloc(int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
+                       const double *cn, const double *norms, int natoms, const double *atom_xyz,
+                       const double *atom_z, double *S, double *T, double *V, void *stream);
+
 /* Canonical packed index, 64-bit. */
 int64_t pqb_ijkl2intindex(int64_t i, int64_t j, int64_t k, int64_t l);
 

@@ -42,6 +42,8 @@ SIGNATURES = {
                                          _vp, _vp, _vp, _vp]),
     "pqb_oneint": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _c_dbl_p,
                                   _c_dbl_p, _vp, _vp, _vp, _vp]),
+    "pqb_oneint_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp,
+                                          _vp, _vp, _vp, _vp]),
     "pqb_ijkl2intindex": (ctypes.c_int64, [ctypes.c_int64] * 4),
     "pqb_boys_eval": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "pqb_rys_eval": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),

@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -406,6 +407,25 @@ __global__ void oneint_kernel(int n, FuncTable ft, int natoms, const double *__r
     if (S) S[t] = nn * s_sum;
     if (Tk) Tk[t] = nn * t_sum;
     if (V) V[t] = nn * v_sum;
+}
+
+// ---- allocation-free one-electron integrals (pqb_oneint_noalloc) --------
+// Scratch for the packed atom table {x, y, z, Z} that oneint_kernel reads:
+// a file-scope device array, so the entry point needs no cudaMalloc.  Every
+// GPU that loads this library holds it (128 KiB) until the process exits.
+#define PQB_NOALLOC_MAX_ATOMS 4096
+#define PQB_NOALLOC_MAX_DEVICES 64
+static __device__ __align__(256) double pqb_noalloc_atoms[4 * PQB_NOALLOC_MAX_ATOMS];
+
+__global__ void pack_atoms_kernel(int natoms, const double *__restrict__ xyz, const double *__restrict__ z,
+                                  double *out)
+{
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= natoms) return;
+    out[4 * a + 0] = xyz[3 * a + 0];
+    out[4 * a + 1] = xyz[3 * a + 1];
+    out[4 * a + 2] = xyz[3 * a + 2];
+    out[4 * a + 3] = z[a];
 }
 
 // ---- stored-integral J/K: one block per packed bra row IJ (i >= j); the row
@@ -1006,6 +1026,40 @@ int pqb_oneint(pqb_ctx *ctx, int n, const double *origin, const int *powers, con
     // the host staging buffer must outlive the async copy
     PQB_CK(ctx, cudaStreamSynchronize(st));
     return PQB_OK;
+}
+
+// Host code may not use pqb_noalloc_atoms' name as a device address: its
+// device address is looked up once per device with cudaGetSymbolAddress
+// (with that device current) and cached here.
+static double *g_noalloc_atoms[PQB_NOALLOC_MAX_DEVICES] = {nullptr};
+static std::mutex g_noalloc_mutex;
+
+int pqb_oneint_noalloc(int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
+                       const double *cn, const double *norms, int natoms, const double *atom_xyz,
+                       const double *atom_z, double *S, double *T, double *V, void *stream)
+{
+    if (n <= 0 || !origin || !powers || !prim_off || !exps || !cn || !norms || natoms < 0 ||
+        (natoms > 0 && (!atom_xyz || !atom_z)))
+        return PQB_E_ARG;
+    if (natoms > PQB_NOALLOC_MAX_ATOMS) return PQB_E_SHAPE;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= PQB_NOALLOC_MAX_DEVICES) return PQB_E_CUDA;
+    double *atoms = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_atoms[dev]) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, pqb_noalloc_atoms) != cudaSuccess || !p) return PQB_E_CUDA;
+            g_noalloc_atoms[dev] = static_cast<double *>(p);
+        }
+        atoms = g_noalloc_atoms[dev];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (natoms > 0) pack_atoms_kernel<<<(natoms + 127) / 128, 128, 0, st>>>(natoms, atom_xyz, atom_z, atoms);
+    FuncTable ft{origin, powers, prim_off, exps, cn, norms};
+    const int64_t nn = (int64_t)n * n;
+    oneint_kernel<<<(unsigned)((nn + 127) / 128), 128, 0, st>>>(n, ft, natoms, atoms, S, T, V);
+    return cudaGetLastError() == cudaSuccess ? PQB_OK : PQB_E_CUDA;
 }
 
 int pqb_boys_eval(pqb_ctx *ctx, int m, int count, const double *T, double *F, void *stream)
