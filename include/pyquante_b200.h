@@ -80,6 +80,13 @@ int pqb_num_pairs(const pqb_ctx *ctx);
  * {shell quartets, kept FP64, kept FP32, dropped}. */
 int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *counts);
 
+/* Tuning knobs (used by pyquante_b200.autotune): PQB_PARAM_CHUNK = the
+ * largest number of primitive quartets in one J/K work item, for class
+ * qclass (0..20, or -1 for all; effective at the next pqb_plan);
+ * PQB_PARAM_STREAMS = streams the class launches are spread over (1..8). */
+enum { PQB_PARAM_CHUNK = 0, PQB_PARAM_STREAMS = 1 };
+int pqb_set_param(pqb_ctx *ctx, int param, int qclass, int value);
+
 /* Per-class statistics of the current plan, arrays of 2*21 int64 indexed
  * [part*21 + class] (part 0 = FP64 list, 1 = FP32-eligible list; class =
  * bra*(bra+1)/2 + ket over pair classes ss ps pp ds dp dd): shell quartets and

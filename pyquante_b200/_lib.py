@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libpyquante_b200.so")
 PQB_OK, PQB_E_ARG, PQB_E_CLASS, PQB_E_NPRIM, PQB_E_SHAPE, PQB_E_CUDA, PQB_E_STATE, PQB_E_TIMEOUT, PQB_E_NOMEM = range(9)
 PQB_FP64, PQB_MIXED = 0, 1
 PQB_ENGINE_RYS, PQB_ENGINE_HGP = 0, 1
+PQB_PARAM_CHUNK, PQB_PARAM_STREAMS = 0, 1
 
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _c_dbl_p = ctypes.POINTER(ctypes.c_double)
@@ -31,6 +32,7 @@ SIGNATURES = {
     "pqb_schwarz": (ctypes.c_int, [_vp, _c_dbl_p, _vp]),
     "pqb_num_pairs": (ctypes.c_int, [_vp]),
     "pqb_plan": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _c_i64_p]),
+    "pqb_set_param": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "pqb_plan_stats": (ctypes.c_int, [_vp, _c_i64_p, _c_i64_p]),
     "pqb_plan_shard": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "pqb_fp64_peak": (ctypes.c_int, [_vp, ctypes.c_int, _c_dbl_p]),

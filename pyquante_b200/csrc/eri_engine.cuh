@@ -277,8 +277,13 @@ struct EpiSchwarz {
 };
 
 // ---------------------------------------------------------- thread mode --
+// Register cap per class (via the minimum resident blocks of 128 threads):
+// small classes are latency bound, so they trade registers for occupancy.
+__host__ __device__ constexpr int thread_min_blocks(int nabcd) { return nabcd == 1 ? 8 : (nabcd <= 9 ? 4 : 2); }
+
 template <int LA, int LB, int LC, int LD, typename R, class Epi>
-__global__ void __launch_bounds__(128) eri_thread_kernel(const int4 *__restrict__ list, int nq,
+__global__ void __launch_bounds__(128, thread_min_blocks(ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)))
+eri_thread_kernel(const int4 *__restrict__ list, int nq,
                                                          const PairInfo *__restrict__ pairs,
                                                          const PrimPair *__restrict__ prims, Epi epi)
 {
@@ -299,21 +304,18 @@ __global__ void __launch_bounds__(128) eri_thread_kernel(const int4 *__restrict_
         for (int c = 0; c < NAB * NCD; ++c) acc[c] = (R)0;
         const int npk = pk.nprim;
         int ib = e.z / npk, ik = e.z - (e.z / npk) * npk;
+        PrimPair P = prims[pb.prim_off + ib];
         for (int t = 0; t < e.w; ++t) {
-            const PrimPair P = prims[pb.prim_off + ib];
             const PrimPair Q = prims[pk.prim_off + ik];
-            if (++ik == npk) {
-                ik = 0;
-                ++ib;
-            }
             const double zpe = P.zeta + Q.zeta;
             const double PQx = P.P[0] - Q.P[0], PQy = P.P[1] - Q.P[1], PQz = P.P[2] - Q.P[2];
             const double T = P.zeta * Q.zeta / zpe * (PQx * PQx + PQy * PQy + PQz * PQz);
             const double pre = P.K * Q.K * rsqrt(zpe);
+            double uu[NR], ww[NR];
+            rys_roots<NR>(T, uu, ww);
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
-                double u, w;
-                rys_root(NR, r, T, u, w);
+                const double u = uu[r], w = ww[r];
                 R gx[G2D], gy[G2D], gz[G2D];
                 rys2d<LA, LB, LC, LD, R>(u, P.zeta, Q.zeta, P.P[0] - Ax, Q.P[0] - Cx, PQx, ABx, CDx, w * pre, gx);
                 rys2d<LA, LB, LC, LD, R>(u, P.zeta, Q.zeta, P.P[1] - Ay, Q.P[1] - Cy, PQy, ABy, CDy, 1.0, gy);
@@ -331,6 +333,11 @@ __global__ void __launch_bounds__(128) eri_thread_kernel(const int4 *__restrict_
                                            (LD + 1) + cart_lz(LD, id);
                         acc[ab * NCD + cd] += gx[ox] * gy[oy] * gz[oz];
                     }
+            }
+            if (++ik == npk) {
+                ik = 0;
+                ++ib;
+                if (t + 1 < e.w) P = prims[pb.prim_off + ib];
             }
         }
         const QCtx q{pb.fa, pb.fb, pk.fa, pk.fb, pb.sa, pb.sb, pk.sa, pk.sb, e.x, e.y};
@@ -442,7 +449,14 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
                     const double PQx = P.P[0] - Q.P[0], PQy = P.P[1] - Q.P[1], PQz = P.P[2] - Q.P[2];
                     const double T = P.zeta * Q.zeta / zpe * (PQx * PQx + PQy * PQy + PQz * PQz);
                     double u, w;
-                    rys_root(NR, r, T, u, w);
+                    if constexpr (NR == 1) {
+                        double uu[1], ww[1];
+                        rys_roots<1>(T, uu, ww);
+                        u = uu[0];
+                        w = ww[0];
+                    } else {
+                        rys_root(NR, r, T, u, w);
+                    }
                     su[s][r] = u;
                     sw[s][r] = w * P.K * Q.K * rsqrt(zpe);
                     if (r == 0) {
@@ -522,7 +536,7 @@ inline cudaError_t launch_eri_class(const int4 *list, int nq, const PairInfo *pa
     constexpr int NAB = ncart(LA) * ncart(LB), NCD = ncart(LC) * ncart(LD);
     if constexpr (NAB * NCD <= 36) {
         int grid = (nq + 127) / 128;
-        if (grid > nsm * 16) grid = nsm * 16;
+        if (grid > nsm * 32) grid = nsm * 32;
         eri_thread_kernel<LA, LB, LC, LD, R, Epi><<<grid, 128, 0, st>>>(list, nq, pairs, prims, epi);
     } else {
         using Lay = BlockLayout<LA, LB, LC, LD, R, Epi>;

@@ -20,6 +20,12 @@
 
 using namespace pqb;
 
+// Primitive-quartet chunk for the J/K work items: long contractions
+// (up to 1296 primitive quartets for a 6-primitive s shell to the fourth)
+// are cut so no thread or block slot runs a long serial chain.  Per class,
+// tunable with pqb_set_param(PQB_PARAM_CHUNK) (default 16).
+static const int kDefaultChunk = 16;
+
 struct pqb_ctx {
     int device = 0;
     int nsm = 148;
@@ -48,6 +54,8 @@ struct pqb_ctx {
     int64_t plan_off[2][kNumQuartetClass] = {{0}}, plan_cnt[2][kNumQuartetClass] = {{0}};
     int64_t plan_prims[2][kNumQuartetClass] = {{0}};
     std::vector<int4> plan_h;        // host copy of the plan (for sharding)
+    int chunk[kNumQuartetClass];     // primitive-quartet chunk per class
+    int nstreams = 8;
     // fork/join streams for concurrent class launches
     static constexpr int kStreams = 8;
     cudaStream_t streams[kStreams] = {nullptr};
@@ -525,6 +533,7 @@ int pqb_create(pqb_ctx **out, int device)
     *out = nullptr;
     pqb_ctx *ctx = new pqb_ctx();
     ctx->device = device;
+    for (int c = 0; c < kNumQuartetClass; ++c) ctx->chunk[c] = kDefaultChunk;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {
         delete ctx;
@@ -614,10 +623,6 @@ static void bucket_sorted(std::vector<std::vector<int4>> &cls, std::vector<int4>
     }
 }
 
-// Primitive-quartet chunk for the J/K work items: long contractions
-// (up to 1296 primitive quartets for a 6-primitive s shell to the fourth)
-// are cut so no thread or block slot runs a long serial chain.
-static const int kChunk = 16;
 
 static inline int4 oriented_quartet(const std::vector<PairInfo> &pairs, int p, int q, int &qc)
 {
@@ -767,7 +772,8 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
             int qc;
             int4 e = oriented_quartet(pairs, p, q, qc);
             auto &dst = (b < fp32_thresh ? c32 : c64)[qc];
-            for (int s0 = 0; s0 < e.w; s0 += kChunk) dst.push_back(make_int4(e.x, e.y, s0, std::min(kChunk, e.w - s0)));
+            const int ch = ctx->chunk[qc];
+            for (int s0 = 0; s0 < e.w; s0 += ch) dst.push_back(make_int4(e.x, e.y, s0, std::min(ch, e.w - s0)));
         }
     }
     std::vector<int4> f64, f32;
@@ -801,6 +807,29 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
         counts[3] = dropped;
     }
     return PQB_OK;
+}
+
+int pqb_set_param(pqb_ctx *ctx, int param, int qclass, int value)
+{
+    if (!ctx) return PQB_E_ARG;
+    switch (param) {
+    case PQB_PARAM_CHUNK:
+        if (value < 1 || value > 4096) return fail(ctx, PQB_E_ARG, "chunk %d out of range 1..4096", value);
+        if (qclass < 0) {
+            for (int c = 0; c < kNumQuartetClass; ++c) ctx->chunk[c] = value;
+        } else if (qclass < kNumQuartetClass) {
+            ctx->chunk[qclass] = value;
+        } else {
+            return fail(ctx, PQB_E_ARG, "class %d", qclass);
+        }
+        ctx->have_plan = false;   // takes effect at the next pqb_plan
+        return PQB_OK;
+    case PQB_PARAM_STREAMS:
+        if (value < 1 || value > pqb_ctx::kStreams) return fail(ctx, PQB_E_ARG, "streams %d out of range", value);
+        ctx->nstreams = value;
+        return PQB_OK;
+    }
+    return fail(ctx, PQB_E_ARG, "unknown parameter %d", param);
 }
 
 int pqb_plan_stats(const pqb_ctx *ctx, int64_t *quartets, int64_t *prim_quartets)
@@ -919,7 +948,7 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
         const int part = order[i] / kNumQuartetClass, c = order[i] % kNumQuartetClass;
         const int nq = (int)ctx->plan_cnt[part][c];
         if (nq == 0) continue;
-        cudaStream_t sk = ctx->streams[k++ % pqb_ctx::kStreams];
+        cudaStream_t sk = ctx->streams[k++ % ctx->nstreams];
         const int4 *list = ctx->d_plan + ctx->plan_off[part][c];
         if (part == 1 && mode == PQB_MIXED)
             PQB_CK(ctx, launch_jk_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, D, J, K, ctx->d_fscale, n, sk, ctx->nsm));

@@ -121,6 +121,22 @@ __device__ __forceinline__ void rys_root(int n, int r, double T, double &u, doub
     }
 }
 
+// All NR roots at T.  One root (total angular momentum <= 1) comes straight
+// from the Boys function: u = F_1/F_0, w = F_0 (8 table loads instead of 28).
+template <int NR>
+__device__ __forceinline__ void rys_roots(double T, double *u, double *w)
+{
+    if constexpr (NR == 1) {
+        double F[2];
+        boys<1>(T, F);
+        w[0] = F[0];
+        u[0] = F[1] / F[0];
+    } else {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) rys_root(NR, r, T, u[r], w[r]);
+    }
+}
+
 // ------------------------------------------------ 2-D Rys integrals (one axis)
 // For one root u and one cartesian axis: G(n,m) = I_x(n,0|m,0) by the Rys
 // recurrence (bra exponent sum zeta, ket eta), then the horizontal transfer

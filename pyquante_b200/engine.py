@@ -161,6 +161,8 @@ class BasisEngine:
                 self.ctx.h, ns, (I * ns)(*s["l"]), (I * ns)(*s["nprim"]), (I * ns)(*s["off"]), (I * ns)(*s["f0"]),
                 (D * (3 * ns))(*s["xyz"]), (D * len(s["exps"]))(*s["exps"]), (D * len(s["coefs"]))(*s["coefs"]),
                 self.nbf, (D * self.nbf)(*s["fscale"])))
+            from . import autotune
+            autotune.apply(self)
 
     @property
     def has_shells(self):
