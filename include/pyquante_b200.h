@@ -155,6 +155,21 @@ int pqb_oneint_noalloc(int n, const double *origin, const int *powers, const int
                        const double *cn, const double *norms, int natoms, const double *atom_xyz,
                        const double *atom_z, double *S, double *T, double *V, void *stream);
 
+/* RHF nuclear gradient (replaces PyQuante/force.py:48-70 with
+ * AnalyticDerivatives.py): dE/dR = 2 tr(D dh) + tr(D dG[D]) - 2 tr(W dS)
+ * + dE_nuc, D = C_occ C_occ^T, W = C_occ diag(e_occ) C_occ^T.
+ * pqb_set_shell_atoms: atom index of every uploaded shell (host array).
+ * pqb_grad_2e: adds tr(D dG[D]) to grad[3*natoms] (device), derivative
+ * integrals contracted with the density on the fly over the current plan;
+ * mode PQB_MIXED runs the FP32-eligible list in FP32.
+ * pqb_grad_1e: adds 2 tr(D d(T+V)) - 2 tr(W dS) over a function table
+ * (func_atom: device array, atom index per function; atoms on the host). */
+int pqb_set_shell_atoms(pqb_ctx *ctx, const int *shell_atom);
+int pqb_grad_2e(pqb_ctx *ctx, const double *D, double *grad, int mode, void *stream);
+int pqb_grad_1e(pqb_ctx *ctx, int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
+                const double *cn, const double *norms, const int *func_atom, int natoms, const double *atom_xyz,
+                const double *atom_z, const double *D, const double *W, double *grad, void *stream);
+
 /* Canonical packed index, 64-bit. */
 int64_t pqb_ijkl2intindex(int64_t i, int64_t j, int64_t k, int64_t l);
 

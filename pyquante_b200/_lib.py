@@ -46,6 +46,10 @@ SIGNATURES = {
                                   _c_dbl_p, _vp, _vp, _vp, _vp]),
     "pqb_oneint_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp,
                                           _vp, _vp, _vp, _vp]),
+    "pqb_set_shell_atoms": (ctypes.c_int, [_vp, _c_int_p]),
+    "pqb_grad_2e": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
+    "pqb_grad_1e": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _c_dbl_p,
+                                   _c_dbl_p, _vp, _vp, _vp, _vp]),
     "pqb_ijkl2intindex": (ctypes.c_int64, [ctypes.c_int64] * 4),
     "pqb_boys_eval": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "pqb_rys_eval": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),

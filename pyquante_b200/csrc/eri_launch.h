@@ -24,4 +24,10 @@ cudaError_t launch_jk_f32(int qc, const int4 *list, int nq, const PairInfo *pair
                           cudaStream_t st, int nsm);
 cudaError_t launch_schwarz_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                                unsigned long long *Q2bits, const double *fscale, cudaStream_t st, int nsm);
+cudaError_t launch_grad_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+                            const double *D, const double *fscale, const int *shell_atom, int n, double *grad,
+                            cudaStream_t st, int nsm);
+cudaError_t launch_grad_f32(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+                            const double *D, const double *fscale, const int *shell_atom, int n, double *grad,
+                            cudaStream_t st, int nsm);
 }  // namespace pqb

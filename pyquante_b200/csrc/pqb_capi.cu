@@ -54,6 +54,7 @@ struct pqb_ctx {
     int64_t plan_off[2][kNumQuartetClass] = {{0}}, plan_cnt[2][kNumQuartetClass] = {{0}};
     int64_t plan_prims[2][kNumQuartetClass] = {{0}};
     std::vector<int4> plan_h;        // host copy of the plan (for sharding)
+    int *d_shell_atom = nullptr;     // atom index of every shell (gradients)
     int chunk[kNumQuartetClass];     // primitive-quartet chunk per class
     int nstreams = 8;
     // fork/join streams for concurrent class launches
@@ -417,6 +418,133 @@ __global__ void oneint_kernel(int n, FuncTable ft, int natoms, const double *__r
     if (V) V[t] = nn * v_sum;
 }
 
+// ---- one-electron part of the RHF nuclear gradient, one thread per (i, j):
+//   2 D_ij d(T + V)_ij/dR - 2 W_ij dS_ij/dR            (PyQuante/force.py:61-64)
+// Basis-centre derivatives by raising/lowering each primitive,
+// d/dA_x g_a = 2 alpha g_{a+1x} - a_x g_{a-1x}; dS/dB = -dS/dA, dT/dB = -dT/dA;
+// for each nucleus C the Hellmann-Feynman term dV_C/dC = -(dV_C/dA + dV_C/dB).
+__device__ __forceinline__ double ov3(double (*Sx)[8][9], const int *li, const int *lj, int a0, int a1, int a2,
+                                      int b0, int b1, int b2)
+{
+    return Sx[0][li[0] + a0][lj[0] + b0] * Sx[1][li[1] + a1][lj[1] + b1] * Sx[2][li[2] + a2][lj[2] + b2];
+}
+
+__device__ double kin3(double (*Sx)[8][9], const int *li, const int *lj, double b, int a0, int a1, int a2)
+{
+    const int Lj = lj[0] + lj[1] + lj[2];
+    double t = b * (2 * Lj + 3) * ov3(Sx, li, lj, a0, a1, a2, 0, 0, 0) -
+               2.0 * b * b * (ov3(Sx, li, lj, a0, a1, a2, 2, 0, 0) + ov3(Sx, li, lj, a0, a1, a2, 0, 2, 0) +
+                              ov3(Sx, li, lj, a0, a1, a2, 0, 0, 2));
+    if (lj[0] >= 2) t -= 0.5 * lj[0] * (lj[0] - 1) * ov3(Sx, li, lj, a0, a1, a2, -2, 0, 0);
+    if (lj[1] >= 2) t -= 0.5 * lj[1] * (lj[1] - 1) * ov3(Sx, li, lj, a0, a1, a2, 0, -2, 0);
+    if (lj[2] >= 2) t -= 0.5 * lj[2] * (lj[2] - 1) * ov3(Sx, li, lj, a0, a1, a2, 0, 0, -2);
+    return t;
+}
+
+__global__ void oneint_grad_kernel(int n, FuncTable ft, int natoms, const double *__restrict__ atoms,
+                                   const int *__restrict__ func_atom, const double *__restrict__ Dm,
+                                   const double *__restrict__ Wm, double *grad)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)n * n) return;
+    const int i = (int)(t / n), j = (int)(t % n);
+    const double *A = ft.origin + 3 * i, *B = ft.origin + 3 * j;
+    int li[3], lj[3];
+    for (int x = 0; x < 3; ++x) {
+        li[x] = ft.powers[3 * i + x];
+        lj[x] = ft.powers[3 * j + x];
+    }
+    if (li[0] + li[1] + li[2] > 3 || lj[0] + lj[1] + lj[2] > 3) return;   // host rejects these first
+    const double nn = ft.norms[i] * ft.norms[j];
+    const double d2 = 2.0 * Dm[t] * nn, w2 = 2.0 * Wm[t] * nn;
+    double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0};
+    const int Ltot = li[0] + li[1] + li[2] + lj[0] + lj[1] + lj[2];
+    for (int p = ft.prim_off[i]; p < ft.prim_off[i + 1]; ++p)
+        for (int q = ft.prim_off[j]; q < ft.prim_off[j + 1]; ++q) {
+            const double a = ft.exps[p], b = ft.exps[q], g = a + b;
+            double P[3], rab2 = 0;
+            for (int x = 0; x < 3; ++x) {
+                P[x] = (a * A[x] + b * B[x]) / g;
+                rab2 += (A[x] - B[x]) * (A[x] - B[x]);
+            }
+            const double E = exp(-a * b / g * rab2);
+            const double cw = ft.cn[p] * ft.cn[q];
+            double Sx[3][8][9];
+            for (int x = 0; x < 3; ++x) {
+                const double pa = P[x] - A[x], pb = P[x] - B[x], o2g = 0.5 / g;
+                const int U = li[x] + 1, W = lj[x] + 2;
+                Sx[x][0][0] = 1.0;
+                for (int v = 0; v < W; ++v) Sx[x][0][v + 1] = pb * Sx[x][0][v] + (v > 0 ? v * o2g * Sx[x][0][v - 1] : 0.0);
+                for (int u = 0; u < U; ++u)
+                    for (int v = 0; v <= W; ++v)
+                        Sx[x][u + 1][v] = pa * Sx[x][u][v] + (u > 0 ? u * o2g * Sx[x][u - 1][v] : 0.0) +
+                                          (v > 0 ? v * o2g * Sx[x][u][v - 1] : 0.0);
+            }
+            const double pre = cw * pow(kPi / g, 1.5) * E;
+            for (int x = 0; x < 3; ++x) {
+                const int dp[3] = {x == 0, x == 1, x == 2};
+                double dS = 2.0 * a * ov3(Sx, li, lj, dp[0], dp[1], dp[2], 0, 0, 0);
+                double dT = 2.0 * a * kin3(Sx, li, lj, b, dp[0], dp[1], dp[2]);
+                if (li[x] > 0) {
+                    dS -= li[x] * ov3(Sx, li, lj, -dp[0], -dp[1], -dp[2], 0, 0, 0);
+                    dT -= li[x] * kin3(Sx, li, lj, b, -dp[0], -dp[1], -dp[2]);
+                }
+                const double c = pre * (d2 * dT - w2 * dS);
+                gA[x] += c;
+                gB[x] -= c;
+            }
+            // nuclear attraction: 1-D Rys integrals I(a', b') for a' in a-1..a+1, b' in b-1..b+1
+            const int nr = (Ltot + 1) / 2 + 1;
+            const double vpre = cw * 2.0 * kPi / g * E;
+            for (int cnuc = 0; cnuc < natoms; ++cnuc) {
+                const double *Cn = atoms + 4 * cnuc;
+                double pc2 = 0;
+                for (int x = 0; x < 3; ++x) pc2 += (P[x] - Cn[x]) * (P[x] - Cn[x]);
+                double vA[3] = {0, 0, 0}, vB[3] = {0, 0, 0};
+                for (int r = 0; r < nr; ++r) {
+                    double u, wr;
+                    rys_root(nr, r, g * pc2, u, wr);
+                    double I0[3], IA[3], IB[3];
+                    for (int x = 0; x < 3; ++x) {
+                        const double c00 = (P[x] - A[x]) - u * (P[x] - Cn[x]), b10 = 0.5 * (1.0 - u) / g;
+                        const int NB = li[x] + lj[x] + 2;
+                        double G[10];
+                        G[0] = 1.0;
+                        G[1] = c00;
+                        for (int k = 1; k < NB; ++k) G[k + 1] = k * b10 * G[k - 1] + c00 * G[k];
+                        const double ab = A[x] - B[x];
+                        // I(a', b') = sum_p C(b',p) ab^(b'-p) G[a'+p]
+                        auto Iab = [&](int ap, int bp) {
+                            double sx = 0.0;
+                            for (int pp = 0; pp <= bp; ++pp) sx += binom_d(bp, pp) * pow(ab, bp - pp) * G[ap + pp];
+                            return sx;
+                        };
+                        I0[x] = Iab(li[x], lj[x]);
+                        IA[x] = 2.0 * a * Iab(li[x] + 1, lj[x]) - (li[x] > 0 ? li[x] * Iab(li[x] - 1, lj[x]) : 0.0);
+                        IB[x] = 2.0 * b * Iab(li[x], lj[x] + 1) - (lj[x] > 0 ? lj[x] * Iab(li[x], lj[x] - 1) : 0.0);
+                    }
+                    vA[0] += wr * IA[0] * I0[1] * I0[2];
+                    vA[1] += wr * I0[0] * IA[1] * I0[2];
+                    vA[2] += wr * I0[0] * I0[1] * IA[2];
+                    vB[0] += wr * IB[0] * I0[1] * I0[2];
+                    vB[1] += wr * I0[0] * IB[1] * I0[2];
+                    vB[2] += wr * I0[0] * I0[1] * IB[2];
+                }
+                const double zf = -Cn[3] * vpre * d2;   // V_C = -Z_C <..>, times 2 D_ij
+                for (int x = 0; x < 3; ++x) {
+                    gA[x] += zf * vA[x];
+                    gB[x] += zf * vB[x];
+                    atomicAdd(grad + 3 * cnuc + x, -zf * (vA[x] + vB[x]));
+                }
+            }
+        }
+    const int ai = func_atom[i], aj = func_atom[j];
+    for (int x = 0; x < 3; ++x) {
+        atomicAdd(grad + 3 * ai + x, gA[x]);
+        atomicAdd(grad + 3 * aj + x, gB[x]);
+    }
+}
+
 // ---- allocation-free one-electron integrals (pqb_oneint_noalloc) --------
 // Scratch for the packed atom table {x, y, z, Z} that oneint_kernel reads:
 // a file-scope device array, so the entry point needs no cudaMalloc.  Every
@@ -565,6 +693,8 @@ static void release_basis(pqb_ctx *ctx)
     free_dev(ctx->d_full);
     free_dev(ctx->d_diag);
     free_dev(ctx->d_plan);
+    free_dev(ctx->d_shell_atom);
+    ctx->d_shell_atom = nullptr;
     ctx->d_pairs = nullptr;
     ctx->d_prims = nullptr;
     ctx->d_fscale = nullptr;
@@ -684,6 +814,7 @@ int pqb_shells_upload(pqb_ctx *ctx, int nshell, const int *shell_l, const int *s
                     pp.zeta = z;
                     for (int x = 0; x < 3; ++x) pp.P[x] = (al * A[x] + be * B[x]) / z;
                     pp.K = prim_coef[p] * prim_coef[q] * kPairPre / z * e;
+                    pp.alpha_a = al;
                     prims.push_back(pp);
                 }
             pi.nprim = (int)prims.size() - pi.prim_off;
@@ -1089,6 +1220,68 @@ int pqb_oneint_noalloc(int n, const double *origin, const int *powers, const int
     const int64_t nn = (int64_t)n * n;
     oneint_kernel<<<(unsigned)((nn + 127) / 128), 128, 0, st>>>(n, ft, natoms, atoms, S, T, V);
     return cudaGetLastError() == cudaSuccess ? PQB_OK : PQB_E_CUDA;
+}
+
+int pqb_set_shell_atoms(pqb_ctx *ctx, const int *shell_atom)
+{
+    if (!ctx || !shell_atom) return fail(ctx, PQB_E_ARG, "pqb_set_shell_atoms: bad arguments");
+    if (!ctx->d_pairs) return fail(ctx, PQB_E_STATE, "pqb_set_shell_atoms: no basis uploaded");
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    if (!ctx->d_shell_atom) PQB_CK(ctx, cudaMalloc(&ctx->d_shell_atom, sizeof(int) * ctx->nshell));
+    PQB_CK(ctx, cudaMemcpy(ctx->d_shell_atom, shell_atom, sizeof(int) * ctx->nshell, cudaMemcpyHostToDevice));
+    return PQB_OK;
+}
+
+int pqb_grad_2e(pqb_ctx *ctx, const double *D, double *grad, int mode, void *stream)
+{
+    if (!ctx || !D || !grad) return fail(ctx, PQB_E_ARG, "pqb_grad_2e: bad arguments");
+    if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_grad_2e: call pqb_plan first");
+    if (!ctx->d_shell_atom) return fail(ctx, PQB_E_STATE, "pqb_grad_2e: call pqb_set_shell_atoms first");
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int part = 0; part < 2; ++part)
+        for (int c = 0; c < kNumQuartetClass; ++c) {
+            const int nq = (int)ctx->plan_cnt[part][c];
+            if (nq == 0) continue;
+            const int4 *list = ctx->d_plan + ctx->plan_off[part][c];
+            if (part == 1 && mode == PQB_MIXED)
+                PQB_CK(ctx, launch_grad_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, D, ctx->d_fscale,
+                                            ctx->d_shell_atom, ctx->nbf, grad, st, ctx->nsm));
+            else
+                PQB_CK(ctx, launch_grad_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, D, ctx->d_fscale,
+                                            ctx->d_shell_atom, ctx->nbf, grad, st, ctx->nsm));
+        }
+    return PQB_OK;
+}
+
+int pqb_grad_1e(pqb_ctx *ctx, int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
+                const double *cn, const double *norms, const int *func_atom, int natoms, const double *atom_xyz,
+                const double *atom_z, const double *D, const double *W, double *grad, void *stream)
+{
+    if (!ctx || n <= 0 || !origin || !powers || !prim_off || !exps || !cn || !norms || !func_atom || natoms <= 0 ||
+        !atom_xyz || !atom_z || !D || !W || !grad)
+        return fail(ctx, PQB_E_ARG, "pqb_grad_1e: bad arguments");
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<double> at(4 * (size_t)natoms);
+    for (int a = 0; a < natoms; ++a) {
+        for (int x = 0; x < 3; ++x) at[4 * a + x] = atom_xyz[3 * a + x];
+        at[4 * a + 3] = atom_z[a];
+    }
+    if (at.size() > ctx->atoms_cap) {
+        free_dev(ctx->d_atoms);
+        ctx->d_atoms = nullptr;
+        PQB_CK(ctx, cudaMalloc(&ctx->d_atoms, sizeof(double) * at.size()));
+        ctx->atoms_cap = at.size();
+    }
+    PQB_CK(ctx, cudaMemcpyAsync(ctx->d_atoms, at.data(), sizeof(double) * at.size(), cudaMemcpyHostToDevice, st));
+    FuncTable ft{origin, powers, prim_off, exps, cn, norms};
+    const int64_t nn = (int64_t)n * n;
+    oneint_grad_kernel<<<(unsigned)((nn + 127) / 128), 128, 0, st>>>(n, ft, natoms, ctx->d_atoms, func_atom, D, W,
+                                                                     grad);
+    PQB_CK(ctx, cudaGetLastError());
+    PQB_CK(ctx, cudaStreamSynchronize(st));
+    return PQB_OK;
 }
 
 int pqb_boys_eval(pqb_ctx *ctx, int m, int count, const double *T, double *F, void *stream)

@@ -29,7 +29,7 @@ struct PrimPair {
     double zeta;       // alpha_a + alpha_b
     double P[3];       // Gaussian product centre
     double K;          // c_a c_b sqrt(2) pi^(5/4)/zeta exp(-alpha_a alpha_b/zeta |AB|^2)
-    double pad;
+    double alpha_a;    // exponent of the first shell's primitive (alpha_b = zeta - alpha_a)
 };
 
 __host__ __device__ inline int pair_class(int la, int lb)   // la >= lb
