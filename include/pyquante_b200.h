@@ -69,6 +69,17 @@ int pqb_shells_upload(pqb_ctx *ctx, int nshell, const int *shell_l, const int *s
                       const int *shell_f0, const double *shell_xyz, const double *prim_exp, const double *prim_coef,
                       int nbf, const double *fscale);
 
+/* Batched basis: nmol molecules, molecule m owning shells
+ * [mol_shell_off[m], mol_shell_off[m+1]) and the functions they cover
+ * (consecutive).  Shell pairs and quartets never mix molecules; D, J and K
+ * of pqb_jk_direct are then the molecules' dense blocks back to back
+ * (block m: nm x nm at offset sum_{m'<m} nm'^2, total pqb_dense_len).
+ * pqb_shells_upload is the nmol = 1 case.  Packed integrals need nmol = 1. */
+int pqb_shells_upload_batch(pqb_ctx *ctx, int nmol, const int *mol_shell_off, int nshell, const int *shell_l,
+                            const int *shell_nprim, const int *prim_off, const int *shell_f0, const double *shell_xyz,
+                            const double *prim_exp, const double *prim_coef, int nbf, const double *fscale);
+int pqb_dense_len(const pqb_ctx *ctx, int64_t *len);
+
 /* Schwarz factors Q_ab = sqrt(max |(ab|ab)|) for every shell pair, computed
  * on the device; copied to Q_host (length npairs) when it is not NULL. */
 int pqb_schwarz(pqb_ctx *ctx, double *Q_host, void *stream);

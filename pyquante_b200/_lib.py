@@ -29,6 +29,10 @@ SIGNATURES = {
     "pqb_last_error": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_size_t]),
     "pqb_shells_upload": (ctypes.c_int, [_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_dbl_p,
                                          _c_dbl_p, _c_dbl_p, ctypes.c_int, _c_dbl_p]),
+    "pqb_shells_upload_batch": (ctypes.c_int, [_vp, ctypes.c_int, _c_int_p, ctypes.c_int, _c_int_p, _c_int_p,
+                                               _c_int_p, _c_int_p, _c_dbl_p, _c_dbl_p, _c_dbl_p, ctypes.c_int,
+                                               _c_dbl_p]),
+    "pqb_dense_len": (ctypes.c_int, [_vp, _c_i64_p]),
     "pqb_schwarz": (ctypes.c_int, [_vp, _c_dbl_p, _vp]),
     "pqb_num_pairs": (ctypes.c_int, [_vp]),
     "pqb_plan": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _c_i64_p]),

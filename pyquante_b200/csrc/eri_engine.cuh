@@ -29,7 +29,14 @@ struct QCtx {
     int fa, fb, fc, fd;   // first function index of the four shells
     int sa, sb, sc, sd;   // shell indices
     int bra, ket;         // pair ids (bra == ket: diagonal quartet)
+    int nm;               // row length of the molecule's D/J/K block
+    long long bo;         // element (i, j) of that block: bo + i*nm + j
 };
+
+__device__ __forceinline__ QCtx make_qctx(const PairInfo &pb, const PairInfo &pk, int bra, int ket)
+{
+    return QCtx{pb.fa, pb.fb, pk.fa, pk.fb, pb.sa, pb.sb, pk.sa, pk.sb, bra, ket, pb.nm, pb.bo};
+}
 
 __device__ __forceinline__ int64_t fpair(int i, int j)
 {
@@ -102,7 +109,6 @@ struct EpiJK {
     const double *D;
     double *Jacc, *Kacc;
     const double *fscale;
-    int n;
     template <int LA, int LB, int LC, int LD>
     static constexpr int kScratch = ncart(LA) * ncart(LB) + ncart(LC) * ncart(LD) +
                                     (ncart(LA) + ncart(LB)) * (ncart(LC) + ncart(LD));
@@ -117,8 +123,10 @@ struct EpiJK {
         if (skip_bra(q, fi, fj)) return 0.0;
         const int64_t IJ = fpair(fi, fj);
         const double sij = fscale[fi] * fscale[fj] * (fi == fj ? 0.5 : 1.0);
-        const double Dij = __ldg(D + (int64_t)fi * n + fj);
-        const double *Di = D + (int64_t)fi * n, *Dj = D + (int64_t)fj * n;
+        const double *Db = D + q.bo;
+        const int nm = q.nm;
+        const double Dij = __ldg(Db + (int64_t)fi * nm + fj);
+        const double *Di = Db + (int64_t)fi * nm, *Dj = Db + (int64_t)fj * nm;
         double jij = 0.0;
 #pragma unroll
         for (int ic = 0; ic < NC; ++ic) {
@@ -131,7 +139,7 @@ struct EpiJK {
                 if (q.bra == q.ket && IJ < KL) continue;
                 const double v = (double)acc[ic * ND + id] * sij * fscale[fk] * fscale[fl] *
                                  (fk == fl ? 0.5 : 1.0) * (IJ == KL ? 0.5 : 1.0);
-                jij += v * __ldg(D + (int64_t)fk * n + fl);
+                jij += v * __ldg(Db + (int64_t)fk * nm + fl);
                 sink.jcd(ic * ND + id, 2.0 * v * Dij);
                 kik += v * __ldg(Dj + fl);
                 kjk += v * __ldg(Di + fl);
@@ -175,27 +183,27 @@ struct EpiJK {
 #pragma unroll
             for (int ib = 0; ib < NB; ++ib) {
                 const double jij = ab<LC, LD, R>(q, ia, ib, acc + (ia * NB + ib) * NCD, r);
-                if (jij != 0.0) atomicAdd(Jacc + (int64_t)(q.fa + ia) * n + q.fb + ib, jij);
+                if (jij != 0.0) atomicAdd(Jacc + q.bo + (int64_t)(q.fa + ia) * q.nm + q.fb + ib, jij);
             }
 #pragma unroll
             for (int c = 0; c < NC; ++c)
-                if (r.kac_[c] != 0.0) atomicAdd(Kacc + (int64_t)(q.fa + ia) * n + q.fc + c, r.kac_[c]);
+                if (r.kac_[c] != 0.0) atomicAdd(Kacc + q.bo + (int64_t)(q.fa + ia) * q.nm + q.fc + c, r.kac_[c]);
 #pragma unroll
             for (int d = 0; d < ND; ++d)
-                if (r.kad_[d] != 0.0) atomicAdd(Kacc + (int64_t)(q.fa + ia) * n + q.fd + d, r.kad_[d]);
+                if (r.kad_[d] != 0.0) atomicAdd(Kacc + q.bo + (int64_t)(q.fa + ia) * q.nm + q.fd + d, r.kad_[d]);
         }
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
 #pragma unroll
             for (int c = 0; c < NC; ++c)
-                if (r.kbc_[b][c] != 0.0) atomicAdd(Kacc + (int64_t)(q.fb + b) * n + q.fc + c, r.kbc_[b][c]);
+                if (r.kbc_[b][c] != 0.0) atomicAdd(Kacc + q.bo + (int64_t)(q.fb + b) * q.nm + q.fc + c, r.kbc_[b][c]);
 #pragma unroll
             for (int d = 0; d < ND; ++d)
-                if (r.kbd_[b][d] != 0.0) atomicAdd(Kacc + (int64_t)(q.fb + b) * n + q.fd + d, r.kbd_[b][d]);
+                if (r.kbd_[b][d] != 0.0) atomicAdd(Kacc + q.bo + (int64_t)(q.fb + b) * q.nm + q.fd + d, r.kbd_[b][d]);
         }
 #pragma unroll
         for (int c = 0; c < NCD; ++c)
-            if (r.jcd_[c] != 0.0) atomicAdd(Jacc + (int64_t)(q.fc + c / ND) * n + q.fd + c % ND, r.jcd_[c]);
+            if (r.jcd_[c] != 0.0) atomicAdd(Jacc + q.bo + (int64_t)(q.fc + c / ND) * q.nm + q.fd + c % ND, r.jcd_[c]);
     }
 
     // block mode: scratch layout [jab NAB | jcd NCD | kac NA*NC | kad NA*ND | kbc NB*NC | kbd NB*ND]
@@ -236,7 +244,7 @@ struct EpiJK {
             else if (e < O4) { row = q.fa + (e - O3) / ND; col = q.fd + (e - O3) % ND; }
             else if (e < O5) { row = q.fb + (e - O4) / NC; col = q.fc + (e - O4) % NC; }
             else { row = q.fb + (e - O5) / ND; col = q.fd + (e - O5) % ND; }
-            atomicAdd(M + (int64_t)row * n + col, v);
+            atomicAdd(M + q.bo + (int64_t)row * q.nm + col, v);
         }
     }
 };
@@ -340,7 +348,7 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
                 if (t + 1 < e.w) P = prims[pb.prim_off + ib];
             }
         }
-        const QCtx q{pb.fa, pb.fb, pk.fa, pk.fb, pb.sa, pb.sb, pk.sa, pk.sb, e.x, e.y};
+        const QCtx q = make_qctx(pb, pk, e.x, e.y);
         epi.template thread_quartet<LA, LB, LC, LD, R>(q, acc);
     }
 }
@@ -405,7 +413,7 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
                 const int4 e = list[qi];
                 const PairInfo &pb = pairs[e.x];
                 const PairInfo &pk = pairs[e.y];
-                s.q = QCtx{pb.fa, pb.fb, pk.fa, pk.fb, pb.sa, pb.sb, pk.sa, pk.sb, e.x, e.y};
+                s.q = make_qctx(pb, pk, e.x, e.y);
                 s.npk = pk.nprim;
                 s.pp0 = e.z;
                 s.npp = e.w;

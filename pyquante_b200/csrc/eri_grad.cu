@@ -56,9 +56,11 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(const int4 *__restrict__ 
                 if (!((q.sa == q.sb && fi < fj) || (q.sc == q.sd && fk < fl) || (q.bra == q.ket && IJ < KL))) {
                     const double s = 8.0 * (fi == fj ? 0.5 : 1.0) * (fk == fl ? 0.5 : 1.0) * (IJ == KL ? 0.5 : 1.0) *
                                      fscale[fi] * fscale[fj] * fscale[fk] * fscale[fl];
-                    const double dij = __ldg(D + (int64_t)fi * n + fj), dkl = __ldg(D + (int64_t)fk * n + fl);
-                    const double dik = __ldg(D + (int64_t)fi * n + fk), djl = __ldg(D + (int64_t)fj * n + fl);
-                    const double dil = __ldg(D + (int64_t)fi * n + fl), djk = __ldg(D + (int64_t)fj * n + fk);
+                    const double *Db = D + q.bo;
+                    const int nm = q.nm;
+                    const double dij = __ldg(Db + (int64_t)fi * nm + fj), dkl = __ldg(Db + (int64_t)fk * nm + fl);
+                    const double dik = __ldg(Db + (int64_t)fi * nm + fk), djl = __ldg(Db + (int64_t)fj * nm + fl);
+                    const double dil = __ldg(Db + (int64_t)fi * nm + fl), djk = __ldg(Db + (int64_t)fj * nm + fk);
                     g = s * (2.0 * dij * dkl - 0.5 * (dik * djl + dil * djk));
                 }
                 gam[ab * NCD + cd] = g;

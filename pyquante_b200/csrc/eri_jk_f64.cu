@@ -7,7 +7,8 @@ cudaError_t launch_jk_f64(int qc, const int4 *list, int nq, const PairInfo *pair
                           const double *D, double *Jacc, double *Kacc, const double *fscale, int n,
                           cudaStream_t st, int nsm)
 {
-    EpiJK epi{D, Jacc, Kacc, fscale, n};
+    (void)n;
+    EpiJK epi{D, Jacc, Kacc, fscale};
     return launch_eri<double>(qc, list, nq, pairs, prims, epi, st, nsm);
 }
 }  // namespace pqb

@@ -55,6 +55,14 @@ struct pqb_ctx {
     int64_t plan_prims[2][kNumQuartetClass] = {{0}};
     std::vector<int4> plan_h;        // host copy of the plan (for sharding)
     int *d_shell_atom = nullptr;     // atom index of every shell (gradients)
+    // batched bases: molecules own consecutive shells/functions; D/J/K hold
+    // one dense nm x nm block per molecule, back to back
+    int nmol = 1;
+    std::vector<int> mol_f0, mol_n, pair_first;   // per molecule; per pair: first pair of its molecule
+    std::vector<long long> mol_off;
+    long long dense_len = 0;
+    long long *d_mol_off = nullptr;
+    int *d_mol_n = nullptr;
     int chunk[kNumQuartetClass];     // primitive-quartet chunk per class
     int nstreams = 8;
     // fork/join streams for concurrent class launches
@@ -107,6 +115,20 @@ __global__ void symmetrize_kernel(double *M, int n)
     double s = M[(int64_t)i * n + j] + M[(int64_t)j * n + i];
     M[(int64_t)i * n + j] = s;
     M[(int64_t)j * n + i] = s;
+}
+
+// Batched form: one CUDA block per molecule block of a block-diagonal layout.
+__global__ void symmetrize_blocks_kernel(double *M, const long long *__restrict__ off, const int *__restrict__ nm)
+{
+    const int m = blockIdx.x, n = nm[m];
+    double *B = M + off[m];
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+        const int i = t / n, j = t - i * n;
+        if (j > i) continue;
+        const double s = B[(int64_t)i * n + j] + B[(int64_t)j * n + i];
+        B[(int64_t)i * n + j] = s;
+        B[(int64_t)j * n + i] = s;
+    }
 }
 
 __device__ __forceinline__ double binom_d(int n, int k)
@@ -694,7 +716,11 @@ static void release_basis(pqb_ctx *ctx)
     free_dev(ctx->d_diag);
     free_dev(ctx->d_plan);
     free_dev(ctx->d_shell_atom);
+    free_dev(ctx->d_mol_off);
+    free_dev(ctx->d_mol_n);
     ctx->d_shell_atom = nullptr;
+    ctx->d_mol_off = nullptr;
+    ctx->d_mol_n = nullptr;
     ctx->d_pairs = nullptr;
     ctx->d_prims = nullptr;
     ctx->d_fscale = nullptr;
@@ -769,9 +795,22 @@ int pqb_shells_upload(pqb_ctx *ctx, int nshell, const int *shell_l, const int *s
                       const int *shell_f0, const double *shell_xyz, const double *prim_exp, const double *prim_coef,
                       int nbf, const double *fscale)
 {
-    if (!ctx || nshell <= 0 || !shell_l || !shell_nprim || !prim_off || !shell_f0 || !shell_xyz || !prim_exp ||
-        !prim_coef || !fscale || nbf <= 0)
+    const int mol_shell_off[2] = {0, nshell};
+    return pqb_shells_upload_batch(ctx, 1, mol_shell_off, nshell, shell_l, shell_nprim, prim_off, shell_f0, shell_xyz,
+                                   prim_exp, prim_coef, nbf, fscale);
+}
+
+int pqb_shells_upload_batch(pqb_ctx *ctx, int nmol, const int *mol_shell_off, int nshell, const int *shell_l,
+                            const int *shell_nprim, const int *prim_off, const int *shell_f0, const double *shell_xyz,
+                            const double *prim_exp, const double *prim_coef, int nbf, const double *fscale)
+{
+    if (!ctx || nmol <= 0 || !mol_shell_off || nshell <= 0 || !shell_l || !shell_nprim || !prim_off || !shell_f0 ||
+        !shell_xyz || !prim_exp || !prim_coef || !fscale || nbf <= 0)
         return fail(ctx, PQB_E_ARG, "pqb_shells_upload: bad arguments");
+    if (mol_shell_off[0] != 0 || mol_shell_off[nmol] != nshell)
+        return fail(ctx, PQB_E_SHAPE, "molecule shell offsets must run from 0 to nshell");
+    for (int m = 0; m < nmol; ++m)
+        if (mol_shell_off[m + 1] <= mol_shell_off[m]) return fail(ctx, PQB_E_SHAPE, "molecule %d has no shells", m);
     PQB_CK(ctx, cudaSetDevice(ctx->device));
     release_basis(ctx);
     int nf = 0;
@@ -787,12 +826,28 @@ int pqb_shells_upload(pqb_ctx *ctx, int nshell, const int *shell_l, const int *s
     if (nf != nbf) return fail(ctx, PQB_E_SHAPE, "shells cover %d functions, nbf = %d", nf, nbf);
     ctx->nbf = nbf;
     ctx->nshell = nshell;
+    ctx->nmol = nmol;
+    ctx->mol_f0.assign(nmol, 0);
+    ctx->mol_n.assign(nmol, 0);
+    ctx->mol_off.assign(nmol, 0);
+    long long off = 0;
+    std::vector<int> shell_mol(nshell);
+    for (int m = 0; m < nmol; ++m) {
+        const int s0 = mol_shell_off[m], s1 = mol_shell_off[m + 1];
+        ctx->mol_f0[m] = shell_f0[s0];
+        ctx->mol_n[m] = shell_f0[s1 - 1] + ncart(shell_l[s1 - 1]) - shell_f0[s0];
+        ctx->mol_off[m] = off;
+        off += (long long)ctx->mol_n[m] * ctx->mol_n[m];
+        for (int sh = s0; sh < s1; ++sh) shell_mol[sh] = m;
+    }
+    ctx->dense_len = off;
     // pairs
     std::vector<PairInfo> pairs;
     std::vector<PrimPair> prims;
     pairs.reserve((size_t)nshell * (nshell + 1) / 2);
+    ctx->pair_first.clear();
     for (int a = 0; a < nshell; ++a)
-        for (int b = 0; b <= a; ++b) {
+        for (int b = mol_shell_off[shell_mol[a]]; b <= a; ++b) {
             int s1 = a, s2 = b;
             if (shell_l[s2] > shell_l[s1]) std::swap(s1, s2);
             PairInfo pi{};
@@ -825,8 +880,21 @@ int pqb_shells_upload(pqb_ctx *ctx, int nshell, const int *shell_l, const int *s
             pi.la = shell_l[s1];
             pi.lb = shell_l[s2];
             pi.cls = pair_class(pi.la, pi.lb);
+            const int m = shell_mol[a];
+            pi.nm = ctx->mol_n[m];
+            pi.bo = ctx->mol_off[m] - (long long)ctx->mol_f0[m] * (ctx->mol_n[m] + 1);
             pairs.push_back(pi);
         }
+    // first pair of each molecule (pairs are generated molecule by molecule)
+    {
+        std::vector<int> first_of_mol(nmol, -1);
+        ctx->pair_first.resize(pairs.size());
+        for (size_t p = 0; p < pairs.size(); ++p) {
+            const int m = shell_mol[pairs[p].sa];
+            if (first_of_mol[m] < 0) first_of_mol[m] = (int)p;
+            ctx->pair_first[p] = first_of_mol[m];
+        }
+    }
     if (prims.empty()) prims.push_back(PrimPair{});
     ctx->pairs = pairs;
     const int np = (int)pairs.size();
@@ -843,11 +911,16 @@ int pqb_shells_upload(pqb_ctx *ctx, int nshell, const int *shell_l, const int *s
         int qc;
         dcls[quartet_class(pairs[p].cls, pairs[p].cls)].push_back(
             make_int4(p, p, 0, pairs[p].nprim * pairs[p].nprim));
+        if (nmol > 1) continue;   // packed integrals are a single-molecule product
         for (int q = 0; q <= p; ++q) {
             int4 e = oriented_quartet(pairs, p, q, qc);
             cls[qc].push_back(e);
         }
     }
+    PQB_CK(ctx, cudaMalloc(&ctx->d_mol_off, sizeof(long long) * nmol));
+    PQB_CK(ctx, cudaMalloc(&ctx->d_mol_n, sizeof(int) * nmol));
+    PQB_CK(ctx, cudaMemcpy(ctx->d_mol_off, ctx->mol_off.data(), sizeof(long long) * nmol, cudaMemcpyHostToDevice));
+    PQB_CK(ctx, cudaMemcpy(ctx->d_mol_n, ctx->mol_n.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice));
     std::vector<int4> flat;
     bucket_sorted(cls, flat, ctx->full_off, ctx->full_cnt);
     PQB_CK(ctx, cudaMalloc(&ctx->d_full, sizeof(int4) * std::max<size_t>(flat.size(), 1)));
@@ -893,8 +966,9 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
     std::vector<std::vector<int4>> c64(kNumQuartetClass), c32(kNumQuartetClass);
     int64_t total = 0, dropped = 0;
     for (int p = 0; p < np; ++p) {
-        total += p + 1;
-        for (int q = 0; q <= p; ++q) {
+        const int q0 = ctx->pair_first[p];
+        total += p - q0 + 1;
+        for (int q = q0; q <= p; ++q) {
             const double b = Q[p] * Q[q];
             if (b < schwarz_thresh) {
                 ++dropped;
@@ -1033,6 +1107,7 @@ int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
 {
     if (!ctx || !out) return fail(ctx, PQB_E_ARG, "pqb_eri_packed: bad arguments");
     if (!ctx->d_pairs) return fail(ctx, PQB_E_STATE, "pqb_eri_packed: no basis uploaded");
+    if (ctx->nmol != 1) return fail(ctx, PQB_E_STATE, "pqb_eri_packed: batched basis (use pqb_jk_direct)");
     const int64_t P = (int64_t)ctx->nbf * (ctx->nbf + 1) / 2;
     if (len != P * (P + 1) / 2) return fail(ctx, PQB_E_SHAPE, "pqb_eri_packed: len %lld != %lld", (long long)len, (long long)(P * (P + 1) / 2));
     PQB_CK(ctx, cudaSetDevice(ctx->device));
@@ -1061,8 +1136,8 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
     PQB_CK(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;
     const int n = ctx->nbf;
-    PQB_CK(ctx, cudaMemsetAsync(J, 0, sizeof(double) * n * n, st));
-    PQB_CK(ctx, cudaMemsetAsync(K, 0, sizeof(double) * n * n, st));
+    PQB_CK(ctx, cudaMemsetAsync(J, 0, sizeof(double) * ctx->dense_len, st));
+    PQB_CK(ctx, cudaMemsetAsync(K, 0, sizeof(double) * ctx->dense_len, st));
     PQB_CK(ctx, ensure_streams(ctx));
     // fork: class launches spread over the context's streams, heaviest first
     PQB_CK(ctx, cudaEventRecord(ctx->ev_fork, st));
@@ -1091,10 +1166,22 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
         PQB_CK(ctx, cudaEventRecord(ctx->ev_join[k], ctx->streams[k]));
         PQB_CK(ctx, cudaStreamWaitEvent(st, ctx->ev_join[k], 0));
     }
-    const int64_t P = (int64_t)n * (n + 1) / 2;
-    symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, n);
-    symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K, n);
+    if (ctx->nmol == 1) {
+        const int64_t P = (int64_t)n * (n + 1) / 2;
+        symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, n);
+        symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K, n);
+    } else {
+        symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(J, ctx->d_mol_off, ctx->d_mol_n);
+        symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(K, ctx->d_mol_off, ctx->d_mol_n);
+    }
     PQB_CK(ctx, cudaGetLastError());
+    return PQB_OK;
+}
+
+int pqb_dense_len(const pqb_ctx *ctx, int64_t *len)
+{
+    if (!ctx || !len) return PQB_E_ARG;
+    *len = ctx->dense_len;
     return PQB_OK;
 }
 

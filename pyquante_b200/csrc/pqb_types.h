@@ -22,7 +22,9 @@ struct PairInfo {
     int sa, sb;        // shell indices
     int cls;           // pair class: index of (La, Lb) in ss ps pp ds dp dd
     int la, lb;
-    int pad;
+    int nm;            // functions of the pair's molecule (batched bases; else nbf)
+    long long bo;      // D/J/K element (i, j) of the molecule is at bo + i*nm + j
+                       // (global function indices; 0 for a single molecule)
 };
 
 struct PrimPair {

@@ -1,0 +1,52 @@
+"""Batched SCF: many molecules in one device basis.  The batched J/K of
+every block must equal each molecule's own J/K (1e-10), and the batched
+SCF energies the single-molecule ones."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from pyquante_b200 import geometries  # noqa: E402
+from pyquante_b200.Basis.basis import BasisSet  # noqa: E402
+from pyquante_b200.batch import BatchEngine, batched_rhf  # noqa: E402
+from pyquante_b200.engine import BasisEngine  # noqa: E402
+from pyquante_b200.hartree_fock import rhf  # noqa: E402
+
+
+def _systems():
+    return [(geometries.water_cluster(k, seed=10 + k), b)
+            for k, b in [(1, "sto-3g"), (2, "6-31g*"), (3, "sto-3g"), (1, "6-31g*"), (2, "6-31g**")]]
+
+
+def test_batched_jk_blocks_equal_single_molecule_jk():
+    systems = _systems()
+    beng = BatchEngine(systems)
+    beng.plan(schwarz=0.0, fp32_threshold=0.0)
+    rng = np.random.default_rng(0)
+    Ds = []
+    for n in beng.n:
+        C = rng.standard_normal((n, max(1, n // 3))) * 0.3
+        Ds.append(C @ C.T)
+    Dflat = torch.tensor(np.concatenate([d.reshape(-1) for d in Ds]), dtype=torch.float64, device="cuda")
+    assert Dflat.numel() == beng.dense_len
+    J = torch.zeros_like(Dflat)
+    K = torch.zeros_like(Dflat)
+    beng.jk(Dflat, J, K, "fp64")
+    for b, ((mol, basis), n, off) in enumerate(zip(systems, beng.n, beng.block_off)):
+        e = BasisEngine(BasisSet(mol, basis).bfs)
+        Js, Ks = e.jk(torch.as_tensor(Ds[b], device="cuda"), "fp64", schwarz=0.0)
+        Jb = J[off:off + n * n].view(n, n)
+        Kb = K[off:off + n * n].view(n, n)
+        assert float((Jb - Js).abs().max()) < 1e-10
+        assert float((Kb - Ks).abs().max()) < 1e-10
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_batched_rhf_matches_single_solves(graph):
+    systems = _systems()
+    res = batched_rhf(systems, precision="fp64", conv=1e-10, maxiter=80, graph=graph)
+    assert res["converged"].all()
+    for (mol, basis), e in zip(systems, res["energies"]):
+        es, _, _ = rhf(mol, basis_data=basis, ConvCriteria=1e-10, MaxIter=100, DoAveraging=True)
+        assert abs(es - e) < 1e-8, (basis, es, e)
