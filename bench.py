@@ -45,6 +45,11 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--workload", default="h2o8", choices=["h2o8", "c16h34", "h2o4-grad", "batch"],
+                   help="h2o8: the headline Fock build; the others are the secondary workloads "
+                        "(C16H34 threshold sweep, (H2O)4 gradient, batched SCF)")
+    p.add_argument("--batch-count", type=int, default=512)
+    p.add_argument("--single-sample", type=int, default=64)
     p.add_argument("--profile-builds", type=int, default=0,
                    help="run this many untimed Fock builds after setup and exit (for ncu captures)")
     return p.parse_args()
@@ -174,10 +179,137 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- GPU arm --
+# --------------------------------------------------- secondary workloads --
+def run_c16h34(a):
+    """C16H34 / 6-31G* (N = 308): FP64 vs mixed Fock build and SCF energy for
+    FP32 thresholds 1e-7 .. 1e-4 (Schwarz 1e-12)."""
+    import torch
+
+    from pyquante_b200 import geometries
+    from pyquante_b200.Basis.basis import BasisSet
+    from pyquante_b200.engine import BasisEngine
+    from pyquante_b200.hartree_fock import rhf
+    mol = geometries.alkane(16)
+    bs = BasisSet(mol, "6-31g*")
+    n = len(bs)
+    out = {"workload": "all-trans C16H34, 6-31G* cartesian, N=%d" % n, "nominal_quartets": nominal_quartets(n)}
+    e64, _, _ = rhf(mol, bfs=bs, direct=True, precision="fp64", ConvCriteria=1e-9, MaxIter=60, DoAveraging=True)
+    out["energy_fp64"] = e64
+    eng = bs._pqb_engine
+    D = torch.eye(n, dtype=torch.float64, device="cuda") * 0.1
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def time_build(mode, thr):
+        for _ in range(a.warmup):
+            eng.jk(D, mode, SCHWARZ, thr)
+        ts = []
+        for _ in range(a.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            eng.jk(D, mode, SCHWARZ, thr)
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    out["fp64_ms_per_build"] = time_build("fp64", 1e-5)
+    sweep = []
+    for thr in (1e-7, 1e-6, 1e-5, 1e-4):
+        em, _, _ = rhf(mol, bfs=bs, direct=True, precision="mixed", fp32_threshold=thr, ConvCriteria=1e-9,
+                       MaxIter=60, DoAveraging=True)
+        ms = time_build("mixed", thr)
+        c = eng.plan_counts
+        sweep.append({"fp32_threshold": thr, "energy": em, "abs_dE": abs(em - e64), "ms_per_build": ms,
+                      "speedup_vs_fp64": out["fp64_ms_per_build"] / ms, "kept_fp64": c["fp64"], "kept_fp32": c["fp32"]})
+    out["sweep"] = sweep
+    print(json.dumps({"metric": "C16H34 mixed-precision threshold sweep", "unit": "ms/Fock build, Eh",
+                      "config": out, "data": "synthetic"}))
+
+
+def run_h2o4_grad(a):
+    """(H2O)4 / 6-31G* perturbed +-0.05 bohr (seed 7): analytic gradient,
+    FP64 and mixed, against central finite differences (step 1e-4 bohr)."""
+    from pyquante_b200 import geometries
+    from pyquante_b200.Molecule import Molecule
+    from pyquante_b200.force import rhf_with_gradient
+    from pyquante_b200.hartree_fock import rhf
+    mol = geometries.perturbed(geometries.water_cluster(4, seed=0), 0.05, seed=7)
+    opts = dict(ConvCriteria=1e-11, MaxIter=200, DoAveraging=True)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        rhf_with_gradient(mol, "6-31g*", precision=prec, **opts)          # warm-up
+        t0 = time.perf_counter()
+        e, g, _, _ = rhf_with_gradient(mol, "6-31g*", precision=prec, **opts)
+        res[prec] = (e, g, time.perf_counter() - t0)
+    h = 1e-4
+    fd = np.zeros_like(res["fp64"][1])
+    atoms = [(at.atno, tuple(at.r)) for at in mol.atoms]
+    for i in range(len(atoms)):
+        for x in range(3):
+            vals = []
+            for d in (h, -h):
+                r = list(atoms[i][1])
+                r[x] += d
+                at2 = list(atoms)
+                at2[i] = (atoms[i][0], tuple(r))
+                vals.append(rhf(Molecule("m", at2, units="bohr"), basis_data="6-31g*", **opts)[0])
+            fd[i, x] = (vals[0] - vals[1]) / (2 * h)
+    print(json.dumps({"metric": "(H2O)4 RHF gradient error vs central differences", "unit": "Eh/bohr",
+                      "data": "synthetic",
+                      "config": {"workload": "(H2O)4 6-31G*, N=76, +-0.05 bohr perturbation seed 7",
+                                 "fp64_max_err": float(np.abs(res["fp64"][1] - fd).max()),
+                                 "mixed_max_err": float(np.abs(res["mixed"][1] - fd).max()),
+                                 "mixed_vs_fp64_energy": abs(res["mixed"][0] - res["fp64"][0]),
+                                 "fp64_scf_plus_gradient_s": res["fp64"][2],
+                                 "mixed_scf_plus_gradient_s": res["mixed"][2]}}))
+
+
+def run_batch(a):
+    """512 water clusters, k ~ U{1..12}, basis 50/50 STO-3G / 6-31G*: one
+    batched mixed-precision SCF (DIIS, conv 1e-8, CUDA graph) vs a loop of
+    single solves over a random sample."""
+    from pyquante_b200 import geometries
+    from pyquante_b200.batch import batched_rhf
+    from pyquante_b200.hartree_fock import rhf
+    systems = geometries.cluster_batch(a.batch_count, seed=0)
+    batched_rhf(systems[:8], precision="mixed", conv=1e-8)          # warm-up (compile, allocator)
+    res = batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=80, graph=True)
+    rng = np.random.default_rng(1)
+    pick = rng.choice(len(systems), size=min(a.single_sample, len(systems)), replace=False)
+    single = []
+    for i in pick:
+        mol, basis = systems[i]
+        t0 = time.perf_counter()
+        e, _, _ = rhf(mol, basis_data=basis, direct=True, precision="mixed", ConvCriteria=1e-8, MaxIter=80,
+                      DoAveraging=True)
+        single.append((time.perf_counter() - t0, abs(e - res["energies"][i])))
+    st = np.array([s[0] for s in single])
+    print(json.dumps({
+        "metric": "batched RHF molecules/s", "value": len(systems) / res["scf_seconds"], "unit": "molecules/s",
+        "data": "synthetic",
+        "config": {"workload": "%d water clusters, k~U{1..12}, 50/50 STO-3G/6-31G*, seed 0" % len(systems),
+                   "nbf_min_max": [int(res["nbf"].min()), int(res["nbf"].max())],
+                   "converged": int(res["converged"].sum()), "iterations_max": int(res["iterations"].max()),
+                   "scf_seconds": res["scf_seconds"], "setup_seconds": res["total_seconds"] - res["scf_seconds"],
+                   "per_molecule_scf_s_p50": float(np.percentile(res["scf_times"], 50)),
+                   "per_molecule_scf_s_p99": float(np.percentile(res["scf_times"], 99)),
+                   "cuda_graph": res["graph"], "plan": res["plan"],
+                   "single_solve_loop": {"sample": len(pick), "molecules_per_s": len(pick) / st.sum(),
+                                         "p50_s": float(np.percentile(st, 50)), "p99_s": float(np.percentile(st, 99)),
+                                         "max_abs_dE_vs_batched": float(max(s[1] for s in single))}}}))
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+        return
+    if a.workload != "h2o8":
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        {"c16h34": run_c16h34, "h2o4-grad": run_h2o4_grad, "batch": run_batch}[a.workload](a)
         return
     import torch
     import torch.distributed as dist

@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(128) eri_grad_kernel(const int4 *__restrict__ 
         const int4 e = list[qi];
         const PairInfo &pb = pairs[e.x];
         const PairInfo &pk = pairs[e.y];
-        const QCtx q{pb.fa, pb.fb, pk.fa, pk.fb, pb.sa, pb.sb, pk.sa, pk.sb, e.x, e.y};
+        const QCtx q = make_qctx(pb, pk, e.x, e.y);
         // Gamma for every component of the quartet (0 for non-canonical ones)
         double gam[NAB * NCD];
 #pragma unroll 1

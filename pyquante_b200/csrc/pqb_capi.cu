@@ -906,25 +906,14 @@ int pqb_shells_upload_batch(pqb_ctx *ctx, int nmol, const int *mol_shell_off, in
     PQB_CK(ctx, cudaMemcpy(ctx->d_prims, prims.data(), sizeof(PrimPair) * prims.size(), cudaMemcpyHostToDevice));
     PQB_CK(ctx, cudaMemcpy(ctx->d_fscale, fscale, sizeof(double) * nbf, cudaMemcpyHostToDevice));
     // unscreened quartet list (packed integrals) and diagonal list (Schwarz)
-    std::vector<std::vector<int4>> cls(kNumQuartetClass), dcls(kNumQuartetClass);
-    for (int p = 0; p < np; ++p) {
-        int qc;
-        dcls[quartet_class(pairs[p].cls, pairs[p].cls)].push_back(
-            make_int4(p, p, 0, pairs[p].nprim * pairs[p].nprim));
-        if (nmol > 1) continue;   // packed integrals are a single-molecule product
-        for (int q = 0; q <= p; ++q) {
-            int4 e = oriented_quartet(pairs, p, q, qc);
-            cls[qc].push_back(e);
-        }
-    }
+    std::vector<std::vector<int4>> dcls(kNumQuartetClass);
+    for (int p = 0; p < np; ++p)
+        dcls[quartet_class(pairs[p].cls, pairs[p].cls)].push_back(make_int4(p, p, 0, pairs[p].nprim * pairs[p].nprim));
     PQB_CK(ctx, cudaMalloc(&ctx->d_mol_off, sizeof(long long) * nmol));
     PQB_CK(ctx, cudaMalloc(&ctx->d_mol_n, sizeof(int) * nmol));
     PQB_CK(ctx, cudaMemcpy(ctx->d_mol_off, ctx->mol_off.data(), sizeof(long long) * nmol, cudaMemcpyHostToDevice));
     PQB_CK(ctx, cudaMemcpy(ctx->d_mol_n, ctx->mol_n.data(), sizeof(int) * nmol, cudaMemcpyHostToDevice));
     std::vector<int4> flat;
-    bucket_sorted(cls, flat, ctx->full_off, ctx->full_cnt);
-    PQB_CK(ctx, cudaMalloc(&ctx->d_full, sizeof(int4) * std::max<size_t>(flat.size(), 1)));
-    PQB_CK(ctx, cudaMemcpy(ctx->d_full, flat.data(), sizeof(int4) * flat.size(), cudaMemcpyHostToDevice));
     bucket_sorted(dcls, flat, ctx->diag_off, ctx->diag_cnt);
     PQB_CK(ctx, cudaMalloc(&ctx->d_diag, sizeof(int4) * std::max<size_t>(flat.size(), 1)));
     PQB_CK(ctx, cudaMemcpy(ctx->d_diag, flat.data(), sizeof(int4) * flat.size(), cudaMemcpyHostToDevice));
@@ -1103,6 +1092,27 @@ int pqb_fp64_peak(pqb_ctx *ctx, int iters, double *flops)
     return PQB_OK;
 }
 
+// Unscreened list of every unique shell quartet (packed integrals), built
+// on first use: P(P+1)/2 items, 16 bytes each.
+static int ensure_full_list(pqb_ctx *ctx)
+{
+    if (ctx->d_full) return PQB_OK;
+    const auto &pairs = ctx->pairs;
+    const int np = (int)pairs.size();
+    std::vector<std::vector<int4>> cls(kNumQuartetClass);
+    for (int p = 0; p < np; ++p)
+        for (int q = 0; q <= p; ++q) {
+            int qc;
+            int4 e = oriented_quartet(pairs, p, q, qc);
+            cls[qc].push_back(e);
+        }
+    std::vector<int4> flat;
+    bucket_sorted(cls, flat, ctx->full_off, ctx->full_cnt);
+    PQB_CK(ctx, cudaMalloc(&ctx->d_full, sizeof(int4) * std::max<size_t>(flat.size(), 1)));
+    PQB_CK(ctx, cudaMemcpy(ctx->d_full, flat.data(), sizeof(int4) * flat.size(), cudaMemcpyHostToDevice));
+    return PQB_OK;
+}
+
 int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
 {
     if (!ctx || !out) return fail(ctx, PQB_E_ARG, "pqb_eri_packed: bad arguments");
@@ -1112,6 +1122,10 @@ int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
     if (len != P * (P + 1) / 2) return fail(ctx, PQB_E_SHAPE, "pqb_eri_packed: len %lld != %lld", (long long)len, (long long)(P * (P + 1) / 2));
     PQB_CK(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;
+    {
+        const int rc = ensure_full_list(ctx);
+        if (rc != PQB_OK) return rc;
+    }
     PQB_CK(ctx, ensure_streams(ctx));
     PQB_CK(ctx, cudaEventRecord(ctx->ev_fork, st));
     for (int k = 0; k < pqb_ctx::kStreams; ++k) PQB_CK(ctx, cudaStreamWaitEvent(ctx->streams[k], ctx->ev_fork, 0));
