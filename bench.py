@@ -477,7 +477,7 @@ def main():
     peak_tf = peak.value / 1e12
     dom = max(per_class, key=lambda r: r["ms"])
     tot_fl = sum(r["flops"] for r in per_class)
-    tot_ms = sum(r["ms"] for r in per_class)
+    build_tflops = tot_fl / (ms_fp64 * 1e-3) / 1e12
     if rank == 0:
         line = {
             "metric": "ERI quartets/s (2J-K Fock build, nominal unique (ij|kl))",
@@ -493,11 +493,14 @@ def main():
             "e2e": {"value": Q / (e2e_ms * 1e-3), "unit": "quartets/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": int(D.numel() * 8), "d2h_bytes_per_step": int(D.numel() * 8),
                     "api": "pyquante_b200.Ints.DirectInts.jk (the get2JmK path) from pinned host D"},
-            "roofline": {"bound": "fp64", "achieved": dom["tflops"], "peak": peak_tf, "unit": "TFLOP/s",
-                         "frac": dom["tflops"] / peak_tf, "traffic": None,
-                         "kernel": "eri_*_kernel class (%d%d|%d%d) FP64 J/K" % tuple(dom["cls"]),
+            "roofline": {"bound": "fp64", "achieved": build_tflops, "peak": peak_tf, "unit": "TFLOP/s",
+                         "frac": build_tflops / peak_tf, "traffic": None,
+                         "kernel": "eri_thread_kernel/eri_block_kernel<class, EpiJK>: all class instantiations "
+                                   "of one FP64 Fock build, launched together by pqb_jk_direct",
+                         "flops_per_build": tot_fl, "fp64_build_ms": ms_fp64,
                          "peak_source": "measured DFMA probe (pqb_fp64_peak) on this GPU",
-                         "all_classes_frac": tot_fl / (tot_ms * 1e-3) / 1e12 / peak_tf},
+                         "slowest_class_alone": "(%d%d|%d%d)" % tuple(dom["cls"]),
+                         "slowest_class_alone_tflops": dom["tflops"]},
             "gpu_launches": launches * a.steps,
             "clocks": clk.summary(),
         }

@@ -94,8 +94,10 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
 /* Tuning knobs (used by pyquante_b200.autotune): PQB_PARAM_CHUNK = the
  * largest number of primitive quartets in one J/K work item, for class
  * qclass (0..20, or -1 for all; effective at the next pqb_plan);
- * PQB_PARAM_STREAMS = streams the class launches are spread over (1..8). */
-enum { PQB_PARAM_CHUNK = 0, PQB_PARAM_STREAMS = 1 };
+ * PQB_PARAM_STREAMS = streams the class launches are spread over (1..16);
+ * PQB_PARAM_ORDER = class launch order (0 by estimated cost, 1 highest
+ * angular momentum first, the default). */
+enum { PQB_PARAM_CHUNK = 0, PQB_PARAM_STREAMS = 1, PQB_PARAM_ORDER = 2 };
 int pqb_set_param(pqb_ctx *ctx, int param, int qclass, int value);
 
 /* Per-class statistics of the current plan, arrays of 2*21 int64 indexed

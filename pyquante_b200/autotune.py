@@ -39,6 +39,8 @@ def apply(eng, tuned=None):
         eng.ctx.check(eng.ctx.lib.pqb_set_param(eng.ctx.h, _lib.PQB_PARAM_CHUNK, qc, int(ch)))
     if "streams" in tuned:
         eng.ctx.check(eng.ctx.lib.pqb_set_param(eng.ctx.h, _lib.PQB_PARAM_STREAMS, 0, int(tuned["streams"])))
+    if "order" in tuned:
+        eng.ctx.check(eng.ctx.lib.pqb_set_param(eng.ctx.h, _lib.PQB_PARAM_ORDER, 0, int(tuned["order"])))
     return True
 
 
@@ -67,10 +69,13 @@ def tune(eng, D, mode="mixed", schwarz=1e-12, fp32_threshold=1e-5, verbose=True)
     flush = torch.empty(64 << 20, dtype=torch.float32, device=D.device)
     lib, h = eng.ctx.lib, eng.ctx.h
 
+    order = 1
+
     def evaluate(chunk, streams):
         for qc, ch in enumerate(chunk):
             eng.ctx.check(lib.pqb_set_param(h, _lib.PQB_PARAM_CHUNK, qc, int(ch)))
         eng.ctx.check(lib.pqb_set_param(h, _lib.PQB_PARAM_STREAMS, 0, int(streams)))
+        eng.ctx.check(lib.pqb_set_param(h, _lib.PQB_PARAM_ORDER, 0, int(order)))
         eng._plan_key = None
         eng.plan(schwarz, fp32_threshold)
         return _build_ms(eng, D, J, K, mode, schwarz, fp32_threshold, flush)
@@ -99,12 +104,21 @@ def tune(eng, D, mode="mixed", schwarz=1e-12, fp32_threshold=1e-5, verbose=True)
             t = evaluate(trial, streams)
             if t < 0.99 * best_t:
                 best_t, chunk = t, trial
-    for ns in (2, 4, 6, 8):
+    for ns in (2, 4, 8, 12, 16):
         t = evaluate(chunk, ns)
         if t < 0.99 * best_t or (ns == streams and t < best_t):
             best_t, streams = t, ns
+    times = {}
+    for od in (0, 1):
+        order = od
+        times[od] = evaluate(chunk, streams)
+        if verbose:
+            print("order %d: %.4f ms" % (od, times[od]))
+    order = min(times, key=times.get)
+    best_t = min(best_t, times[order])
     evaluate(chunk, streams)
-    result = {"chunk": [int(c) for c in chunk], "streams": int(streams), "build_ms": best_t, "mode": mode,
+    result = {"chunk": [int(c) for c in chunk], "streams": int(streams), "order": int(order), "build_ms": best_t,
+              "mode": mode,
               "workload": "(H2O)8 6-31G** seed 0"}
     if verbose:
         print(json.dumps(result))

@@ -8,7 +8,7 @@
 // crys.contr_coulomb does (Src/crys.c:34-54).
 //
 // Two execution modes:
-//  * thread mode (small classes, NAB*NCD <= 36): one thread per quartet,
+//  * thread mode (NAB*NCD <= 54 in FP64, <= 81 in FP32): one thread per quartet,
 //    2-D integrals and all contracted components live in registers.
 //  * block mode (larger classes): a 256-thread block holds NSQ = 256/NAB
 //    quartets; per primitive quartet the roots (NSQ*NR tasks) and the 2-D
@@ -542,7 +542,9 @@ inline cudaError_t launch_eri_class(const int4 *list, int nq, const PairInfo *pa
 {
     if (nq <= 0) return cudaSuccess;
     constexpr int NAB = ncart(LA) * ncart(LB), NCD = ncart(LC) * ncart(LD);
-    if constexpr (NAB * NCD <= 36) {
+    // thread mode while the contracted components fit in registers
+    constexpr int kThreadMax = 81;
+    if constexpr (NAB * NCD <= kThreadMax) {
         int grid = (nq + 127) / 128;
         if (grid > nsm * 32) grid = nsm * 32;
         eri_thread_kernel<LA, LB, LC, LD, R, Epi><<<grid, 128, 0, st>>>(list, nq, pairs, prims, epi);

@@ -65,8 +65,9 @@ struct pqb_ctx {
     int *d_mol_n = nullptr;
     int chunk[kNumQuartetClass];     // primitive-quartet chunk per class
     int nstreams = 8;
+    int order = 1;                   // class launch order: 0 by cost, 1 high angular momentum first
     // fork/join streams for concurrent class launches
-    static constexpr int kStreams = 8;
+    static constexpr int kStreams = 16;
     cudaStream_t streams[kStreams] = {nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[kStreams] = {nullptr};
     bool have_plan = false;
@@ -1022,6 +1023,10 @@ int pqb_set_param(pqb_ctx *ctx, int param, int qclass, int value)
         if (value < 1 || value > pqb_ctx::kStreams) return fail(ctx, PQB_E_ARG, "streams %d out of range", value);
         ctx->nstreams = value;
         return PQB_OK;
+    case PQB_PARAM_ORDER:
+        if (value < 0 || value > 1) return fail(ctx, PQB_E_ARG, "order %d out of range", value);
+        ctx->order = value;
+        return PQB_OK;
     }
     return fail(ctx, PQB_E_ARG, "unknown parameter %d", param);
 }
@@ -1161,7 +1166,10 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
     for (int i = 0; i < 2 * kNumQuartetClass; ++i) {
         order[i] = i;
         const int part = i / kNumQuartetClass, c = i % kNumQuartetClass;
-        cost[i] = (double)ctx->plan_prims[part][c] * (1 + c) * (part == 1 && mode == PQB_MIXED ? 0.5 : 1.0);
+        // order 1: classes with the longest per-item latency (high angular
+        // momentum) start first so they do not form the tail of the build
+        cost[i] = ctx->order == 1 ? (double)(c * 2 + (1 - part))
+                                  : (double)ctx->plan_prims[part][c] * (1 + c) * (part == 1 && mode == PQB_MIXED ? 0.5 : 1.0);
     }
     std::sort(order, order + 2 * kNumQuartetClass, [&](int a, int b) { return cost[a] > cost[b]; });
     for (int i = 0, k = 0; i < 2 * kNumQuartetClass; ++i) {
