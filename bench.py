@@ -44,8 +44,10 @@ def parse():
     p.add_argument("--impl", default="pqb", choices=["pqb", "reference"])
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-graph", action="store_true", help="launch the timed builds eagerly instead of replaying "
+                                                             "a captured CUDA graph")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="h2o8", choices=["h2o8", "c16h34", "h2o4-grad", "batch"],
+    p.add_argument("--workload", default="h2o8", choices=["h2o8", "stored", "c16h34", "h2o4-grad", "batch"],
                    help="h2o8: the headline Fock build; the others are the secondary workloads "
                         "(C16H34 threshold sweep, (H2O)4 gradient, batched SCF)")
     p.add_argument("--batch-count", type=int, default=512)
@@ -180,6 +182,57 @@ class ClockSampler:
 
 # --------------------------------------------------------------- GPU arm --
 # --------------------------------------------------- secondary workloads --
+def measured_hbm_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def run_stored(a):
+    """Stored-integral 2J-K (PyQuante/Ints.py:225-238) on (H2O)8 / 6-31G**:
+    the packed array (Q doubles, 1.6 GB) is built once, then each step is
+    one pqb_jk_packed over it.  Algorithmic bytes per build: 8 Q + 3 * 8 N^2
+    (D in, J and K out).  The packed array is 13x the L2, so no flush."""
+    import torch
+
+    from pyquante_b200 import Ints
+    from pyquante_b200.Basis.basis import BasisSet
+    from pyquante_b200.engine import BasisEngine, jk_packed
+    mol = molecule()
+    bs = BasisSet(mol, "6-31g**")
+    n = len(bs)
+    eng = BasisEngine(bs.bfs)
+    ints = eng.eri_packed()
+    S, h = Ints.get1ints(bs, mol)
+    D = torch.eye(n, dtype=torch.float64, device="cuda") * 0.05
+    for _ in range(a.warmup):
+        jk_packed(ints, D, eng.ctx)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(a.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        jk_packed(ints, D, eng.ctx)
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = float(np.mean(ts))
+    Q = ints.numel()
+    nbytes = 8 * Q + 3 * 8 * n * n
+    peak, src = measured_hbm_gbs()
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    print(json.dumps({"metric": "stored-integral 2J-K build (get2JmK on packed Ints)", "value": Q / (ms * 1e-3),
+                      "unit": "integrals/s", "ms_per_step": ms, "steps": a.steps, "warmup": a.warmup,
+                      "data": "synthetic", "dtype": "f64",
+                      "config": {"workload": WORKLOAD, "packed_integrals": Q, "bytes_per_build": nbytes,
+                                 "l2": "packed array 1.6 GB > L2, no flush"},
+                      "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                   "frac": gbs / peak, "traffic": None, "peak_source": src,
+                                   "kernel": "jk_packed_tiled_kernel"}}))
+
 def run_c16h34(a):
     """C16H34 / 6-31G* (N = 308): FP64 vs mixed Fock build and SCF energy for
     FP32 thresholds 1e-7 .. 1e-4 (Schwarz 1e-12)."""
@@ -309,7 +362,8 @@ def main():
     if a.workload != "h2o8":
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        {"c16h34": run_c16h34, "h2o4-grad": run_h2o4_grad, "batch": run_batch}[a.workload](a)
+        {"stored": run_stored, "c16h34": run_c16h34, "h2o4-grad": run_h2o4_grad,
+         "batch": run_batch}[a.workload](a)
         return
     import torch
     import torch.distributed as dist
@@ -340,10 +394,10 @@ def main():
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         # before any CUDA work in this process: the baseline forks workers
         cpu = reference_rate(bs, a.cpu_seconds)
+    from pyquante_b200.parallel import allreduce_jk, shard_plan
     eng = BasisEngine(bs.bfs, device=local)
     counts = eng.plan(SCHWARZ, FP32_THRESH)
-    if world > 1:
-        eng.ctx.check(eng.ctx.lib.pqb_plan_shard(eng.ctx.h, rank, world))
+    shard_plan(eng, rank, world)
     # a realistic density: a few SCF iterations from the core guess
     S, h = Ints.get1ints(bs, mol)
     St = torch.as_tensor(S, device="cuda")
@@ -353,9 +407,7 @@ def main():
     for _ in range(3):
         D = mkdens(C, 0, nocc).contiguous()
         J, K = eng.jk(D, "fp64", SCHWARZ, FP32_THRESH)
-        if world > 1:
-            dist.all_reduce(J)
-            dist.all_reduce(K)
+        allreduce_jk(J, K)
         _, C = geigh(ht + 2 * J - K, St)
     D = mkdens(C, 0, nocc).contiguous()
     if a.profile_builds:
@@ -372,10 +424,32 @@ def main():
 
     def build(mode):
         eng.jk(D, mode, SCHWARZ, FP32_THRESH, J=J, K=K)
-        if world > 1:
-            dist.all_reduce(J)
-            dist.all_reduce(K)
+        allreduce_jk(J, K)
         torch.sub(J.mul(2.0), K, out=G)
+
+    use_graph = world == 1 and not a.no_graph
+    graphs = {}
+
+    def capture(mode):
+        # one Fock build (memsets, 42 class launches over the context's
+        # streams, symmetrisation, G) captured once and replayed per step
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            build(mode)
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            build(mode)
+        torch.cuda.synchronize()
+        return g
+
+    def run_build(mode):
+        if use_graph:
+            graphs[mode].replay()
+        else:
+            build(mode)
 
     def timed(mode, steps):
         tot = 0.0
@@ -384,7 +458,7 @@ def main():
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            build(mode)
+            run_build(mode)
             e1.record(stream)
             e1.synchronize()
             tot += e0.elapsed_time(e1)
@@ -393,6 +467,13 @@ def main():
     for _ in range(a.warmup):
         build(a.precision)
         build("fp64")
+    torch.cuda.synchronize()
+    if use_graph:
+        for mode in {a.precision, "fp64"}:
+            graphs[mode] = capture(mode)
+        for _ in range(a.warmup):
+            run_build(a.precision)
+            run_build("fp64")
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -415,9 +496,7 @@ def main():
     def e2e_step():
         Dd = Dh.to("cuda", non_blocking=True)
         Jd, Kd = direct.jk(Dd)
-        if world > 1:
-            dist.all_reduce(Jd)
-            dist.all_reduce(Kd)
+        allreduce_jk(Jd, Kd)
         Gh.copy_(2.0 * Jd - Kd, non_blocking=True)
 
     for _ in range(a.warmup):
@@ -488,6 +567,7 @@ def main():
                        "fp32_threshold": FP32_THRESH, "nominal_quartets": Q,
                        "shell_quartets": counts["shell_quartets"], "kept_fp64": counts["fp64"],
                        "kept_fp32": counts["fp32"], "l2": "256 MiB buffer zeroed between timed builds",
+                       "cuda_graph": use_graph,
                        "fp64_ms_per_step": ms_fp64, "mixed_speedup_vs_fp64": ms_fp64 / ms,
                        "parallelism": "quartet shards x%d + NCCL all-reduce of J,K" % world if world > 1 else "1 GPU"},
             "e2e": {"value": Q / (e2e_ms * 1e-3), "unit": "quartets/s", "ms_per_step": e2e_ms,

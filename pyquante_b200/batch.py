@@ -4,7 +4,7 @@ All molecules share one device basis (``pqb_shells_upload_batch``): shell
 pairs and quartets stay inside a molecule, and every class kernel of a Fock
 build serves all molecules in one launch.  D, J, K live as the molecules'
 dense blocks back to back; the SCF linear algebra (FP64, cuSOLVER through
-torch) runs on the blocks padded to the largest basis:
+torch) runs on the blocks padded per size bucket:
 
     per iteration (all molecules at once)
       D = C_occ C_occ^T                  (PyQuante/LA2.py:127-131)
@@ -13,11 +13,14 @@ torch) runs on the blocks padded to the largest basis:
       Pulay DIIS per molecule            (Convergence.py:73-136)
       F' = X^T F X, eigh, C = X C'        Cholesky X (LA2.py:47-75,113-116)
 
-The Fock-build part of an iteration (density, block gather/scatter, the
-multi-stream J/K launches, F and E) is captured once in a CUDA graph and
-replayed; DIIS and the eigensolve run eagerly.  A molecule is converged when
-its energy changes by less than ``conv`` (its SCF time is the time of that
-iteration); converged molecules keep their last solution.
+The molecules are grouped into at most 8 buckets of similar basis size
+for the dense work, so small molecules are not padded to the largest one.
+The Fock-build part of an iteration (densities, block gather/scatter, the
+multi-stream J/K launches, F and E of every bucket) is captured once in a
+CUDA graph and replayed; DIIS and the eigensolves run eagerly per bucket.
+A molecule is converged when its energy changes by less than ``conv`` (its
+SCF time is the time of that iteration); converged molecules keep their
+last solution.
 """
 import ctypes
 import time
@@ -82,72 +85,102 @@ class BatchEngine:
                                                   _lib.stream_ptr()))
 
 
-def _padded_index(n_list, nmax, device):
-    """Flat block-layout position k -> position in the (B, nmax, nmax) padding."""
-    idx = []
-    for b, n in enumerate(n_list):
-        r = torch.arange(n, device=device)
-        idx.append((b * nmax * nmax + r[:, None] * nmax + r[None, :]).reshape(-1))
-    return torch.cat(idx)
+def _bucket_edges(sizes, max_buckets=8):
+    """Padded sizes: split the sorted basis sizes into at most max_buckets
+    groups of similar size (equal counts), each padded to its largest."""
+    order = np.argsort(sizes, kind="stable")
+    groups = [g for g in np.array_split(order, min(max_buckets, len(sizes))) if len(g)]
+    return [np.sort(g) for g in groups]
+
+
+class _Bucket:
+    """Molecules of similar basis size, padded to nb for the dense FP64 work."""
+
+    def __init__(self, idx, eng, S_list, h_list, dev):
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.idx = idx
+        self.n = [eng.n[b] for b in idx]
+        nb = max(self.n)
+        B = len(idx)
+        self.nb = nb
+        S = torch.zeros((B, nb, nb), **f64)
+        h = torch.zeros_like(S)
+        for t, b in enumerate(idx):
+            n = eng.n[b]
+            S[t, :n, :n] = S_list[b]
+            h[t, :n, :n] = h_list[b]
+        nvec = torch.tensor(self.n, device=dev)
+        self.pad = torch.arange(nb, device=dev)[None, :] >= nvec[:, None]
+        self.padmask = self.pad[:, :, None] | self.pad[:, None, :]
+        eye = torch.eye(nb, **f64).expand(B, nb, nb)
+        self.S = torch.where(self.padmask, eye, S)
+        self.h = h
+        self.X = torch.linalg.inv(torch.linalg.cholesky(self.S)).transpose(1, 2)
+        self.shift = torch.diag_embed(self.pad.to(torch.float64) * PAD_SHIFT)
+        nocc = torch.tensor([eng.mols[b].get_closedopen()[0] for b in idx], device=dev)
+        self.occ = (torch.arange(nb, device=dev)[None, :] < nocc[:, None]).to(torch.float64)
+        self.enuc = torch.tensor([eng.mols[b].get_enuke() for b in idx], **f64)
+        # padded position <-> position in the flat block layout
+        pos, flat = [], []
+        for t, b in enumerate(idx):
+            n = eng.n[b]
+            r = torch.arange(n, device=dev)
+            pos.append((t * nb * nb + r[:, None] * nb + r[None, :]).reshape(-1))
+            flat.append(int(eng.block_off[b]) + torch.arange(n * n, device=dev))
+        self.pos = torch.cat(pos)
+        self.flat = torch.cat(flat)
+        # static buffers of the captured Fock build
+        self.C = torch.zeros_like(self.S)
+        self.D = torch.zeros_like(self.S)
+        self.J = torch.zeros_like(self.S)
+        self.K = torch.zeros_like(self.S)
+        self.F = torch.zeros_like(self.S)
+        self.E = torch.zeros(B, **f64)
+        self.Fs, self.Es = [], []
+
+    def solve(self, Fm):
+        e, V = torch.linalg.eigh(self.X.transpose(1, 2) @ Fm @ self.X + self.shift)
+        return self.X @ V
 
 
 def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, graph=True, schwarz=1e-12,
-                fp32_threshold=1e-5, device=None):
+                fp32_threshold=1e-5, device=None, max_buckets=8):
     """Solve RHF for every (molecule, basis) in ``systems`` together.
 
-    Returns a dict: energies, iterations, per-molecule SCF times (s), total
-    time (s), and the plan counts."""
+    The Fock build of every iteration is one engine call for all molecules;
+    the dense FP64 algebra runs per size bucket (molecules padded to the
+    bucket's largest basis).  Returns a dict: energies, iterations,
+    per-molecule SCF times (s), total time (s), and the plan counts."""
     t_start = time.perf_counter()
     eng = BatchEngine(systems, device)
     dev = eng.device
     f64 = dict(dtype=torch.float64, device=dev)
-    B, nmax = len(systems), max(eng.n)
+    B = len(systems)
     counts = eng.plan(schwarz, fp32_threshold)
-    # one-electron integrals per molecule, padded
-    S = torch.zeros((B, nmax, nmax), **f64)
-    h = torch.zeros_like(S)
-    for b, (bs, mol) in enumerate(zip(eng.bases, eng.mols)):
+    S_list, h_list = [], []
+    for bs, mol in zip(eng.bases, eng.mols):
         ft = FunctionTable(bs.bfs, dev.index)
         Sb, Tb, Vb = oneint(ft, mol.atoms, eng.ctx)
-        n = eng.n[b]
-        S[b, :n, :n] = Sb
-        h[b, :n, :n] = Tb + Vb
-    nvec = torch.tensor(eng.n, device=dev)
-    pad = torch.arange(nmax, device=dev)[None, :] >= nvec[:, None]              # (B, nmax)
-    eye = torch.eye(nmax, **f64).expand(B, nmax, nmax)
-    S = torch.where(pad[:, :, None] | pad[:, None, :], eye, S)
-    X = torch.linalg.inv(torch.linalg.cholesky(S)).transpose(1, 2)            # S^-1/2 by Cholesky
-    shift = torch.diag_embed(pad.to(torch.float64) * PAD_SHIFT)
-    nocc = torch.tensor([m.get_closedopen()[0] for m in eng.mols], device=dev)
-    occ = (torch.arange(nmax, device=dev)[None, :] < nocc[:, None]).to(torch.float64)   # (B, nmax)
-    enuc = torch.tensor([m.get_enuke() for m in eng.mols], **f64)
-    pidx = _padded_index(eng.n, nmax, dev)
-
-    def solve(Fm):
-        e, V = torch.linalg.eigh(X.transpose(1, 2) @ Fm @ X + shift)
-        return X @ V
-
-    C = solve(h)
-    # static buffers for the captured Fock build
-    Cs = C.clone()
-    D = torch.zeros_like(S)
+        S_list.append(Sb)
+        h_list.append(Tb + Vb)
+    buckets = [_Bucket(idx, eng, S_list, h_list, dev) for idx in _bucket_edges(np.array(eng.n), max_buckets)]
+    for bk in buckets:
+        bk.C.copy_(bk.solve(bk.h))
     Dflat = torch.zeros(eng.dense_len, **f64)
     Jf = torch.zeros_like(Dflat)
     Kf = torch.zeros_like(Dflat)
-    J = torch.zeros_like(S)
-    K = torch.zeros_like(S)
-    F = torch.zeros_like(S)
-    E = torch.zeros(B, **f64)
 
     def fock_build():
-        Co = Cs * occ[:, None, :]
-        D.copy_(Co @ Co.transpose(1, 2))
-        torch.take(D.reshape(-1), pidx, out=Dflat)
+        for bk in buckets:
+            Co = bk.C * bk.occ[:, None, :]
+            bk.D.copy_(Co @ Co.transpose(1, 2))
+            Dflat.index_copy_(0, bk.flat, bk.D.reshape(-1).index_select(0, bk.pos))
         eng.jk(Dflat, Jf, Kf, precision)
-        J.view(-1).index_copy_(0, pidx, Jf)
-        K.view(-1).index_copy_(0, pidx, Kf)
-        F.copy_(h + 2.0 * J - K)
-        E.copy_((D * h).sum(dim=(1, 2)) + (D * F).sum(dim=(1, 2)) + enuc)
+        for bk in buckets:
+            bk.J.view(-1).index_copy_(0, bk.pos, Jf.index_select(0, bk.flat))
+            bk.K.view(-1).index_copy_(0, bk.pos, Kf.index_select(0, bk.flat))
+            bk.F.copy_(bk.h + 2.0 * bk.J - bk.K)
+            bk.E.copy_((bk.D * bk.h).sum(dim=(1, 2)) + (bk.D * bk.F).sum(dim=(1, 2)) + bk.enuc)
 
     fock_build()                       # warm-up (kernel attributes, allocator)
     torch.cuda.synchronize()
@@ -162,56 +195,60 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
             fock_build()
-    Fs, Es = [], []
-    eold = torch.zeros(B, **f64)
-    done = torch.zeros(B, dtype=torch.bool, device=dev)
-    iters = torch.zeros(B, dtype=torch.int64, device=dev)
+    energies = np.zeros(B)
+    iters = np.zeros(B, dtype=np.int64)
+    done = np.zeros(B, dtype=bool)
     times = np.zeros(B)
+    eold = [torch.zeros(len(bk.idx), **f64) for bk in buckets]
+    bdone = [torch.zeros(len(bk.idx), dtype=torch.bool, device=dev) for bk in buckets]
     t0 = time.perf_counter()
     for it in range(maxiter):
-        Cs.copy_(C)
         if g is not None:
             g.replay()
         else:
             fock_build()
-        # Pulay DIIS per molecule on the error FDS - SDF
-        err = F @ D @ S - S @ D @ F
-        err = torch.where(pad[:, :, None] | pad[:, None, :], torch.zeros_like(err), err)
-        Fs.append(F.clone())
-        Es.append(err.reshape(B, -1))
-        if len(Fs) > diis_size:
-            Fs.pop(0)
-            Es.pop(0)
-        k = len(Fs)
-        Em = torch.stack(Es, dim=1)                                   # (B, k, n^2)
-        A = torch.zeros((B, k + 1, k + 1), **f64)
-        A[:, :k, :k] = Em @ Em.transpose(1, 2)
-        A[:, :k, k] = -1.0
-        A[:, k, :k] = -1.0
-        rhs = torch.zeros((B, k + 1), **f64)
-        rhs[:, k] = -1.0
-        scale = A[:, :k, :k].diagonal(dim1=1, dim2=2).abs().amax(dim=1).clamp(min=1e-300)
-        A[:, :k, :k] /= scale[:, None, None]
-        c, info = torch.linalg.solve_ex(A, rhs)
-        c = torch.where((info == 0)[:, None], c, torch.nn.functional.one_hot(
-            torch.full((B,), k - 1, device=dev), k + 1).to(torch.float64))
-        Fd = (c[:, :k, None, None] * torch.stack(Fs, dim=1)).sum(dim=1)
-        Cn = solve(Fd)
-        energy = E.clone()
-        newly = (~done) & ((energy - eold).abs() < conv)
-        iters = torch.where(done, iters, torch.full_like(iters, it + 1))
-        C = torch.where(done[:, None, None], C, Cn)
-        done = done | newly
-        eold = torch.where(done & ~newly, eold, energy)
-        nd = newly.cpu().numpy()
-        if nd.any():
-            torch.cuda.synchronize()
-            times[nd] = time.perf_counter() - t0
-        if bool(done.all()):
+        for q, bk in enumerate(buckets):
+            nb, Bb = bk.nb, len(bk.idx)
+            err = bk.F @ bk.D @ bk.S - bk.S @ bk.D @ bk.F
+            err = torch.where(bk.padmask, torch.zeros_like(err), err)
+            bk.Fs.append(bk.F.clone())
+            bk.Es.append(err.reshape(Bb, -1))
+            if len(bk.Fs) > diis_size:
+                bk.Fs.pop(0)
+                bk.Es.pop(0)
+            k = len(bk.Fs)
+            Em = torch.stack(bk.Es, dim=1)
+            A = torch.zeros((Bb, k + 1, k + 1), **f64)
+            A[:, :k, :k] = Em @ Em.transpose(1, 2)
+            scale = A[:, :k, :k].diagonal(dim1=1, dim2=2).abs().amax(dim=1).clamp(min=1e-300)
+            A[:, :k, :k] /= scale[:, None, None]
+            A[:, :k, k] = -1.0
+            A[:, k, :k] = -1.0
+            rhs = torch.zeros((Bb, k + 1), **f64)
+            rhs[:, k] = -1.0
+            c, info = torch.linalg.solve_ex(A, rhs)
+            c = torch.where((info == 0)[:, None], c, torch.nn.functional.one_hot(
+                torch.full((Bb,), k - 1, device=dev), k + 1).to(torch.float64))
+            Fd = (c[:, :k, None, None] * torch.stack(bk.Fs, dim=1)).sum(dim=1)
+            Cn = bk.solve(Fd)
+            energy = bk.E.clone()
+            newly = (~bdone[q]) & ((energy - eold[q]).abs() < conv)
+            bk.C.copy_(torch.where(bdone[q][:, None, None], bk.C, Cn))
+            eold[q] = torch.where(bdone[q], eold[q], energy)
+            bdone[q] = bdone[q] | newly
+        flags = [(bd.cpu().numpy(), e.cpu().numpy()) for bd, e in zip(bdone, eold)]
+        now = time.perf_counter() - t0
+        for bk, (bd, e) in zip(buckets, flags):
+            fresh = bd & ~done[bk.idx]
+            times[bk.idx[fresh]] = now
+            iters[bk.idx[~done[bk.idx]]] = it + 1
+            done[bk.idx] = bd
+            energies[bk.idx] = e
+        if done.all():
             break
     torch.cuda.synchronize()
     t_end = time.perf_counter()
     times[times == 0] = t_end - t0
-    return dict(energies=eold.cpu().numpy(), iterations=iters.cpu().numpy(), converged=done.cpu().numpy(),
-                scf_times=times, scf_seconds=t_end - t0, total_seconds=t_end - t_start, plan=counts,
-                nbf=np.array(eng.n), graph=g is not None)
+    return dict(energies=energies, iterations=iters, converged=done, scf_times=times, scf_seconds=t_end - t0,
+                total_seconds=t_end - t_start, plan=counts, nbf=np.array(eng.n), graph=g is not None,
+                buckets=[bk.nb for bk in buckets])
