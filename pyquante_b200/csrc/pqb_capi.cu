@@ -55,6 +55,8 @@ struct pqb_ctx {
     int64_t plan_prims[2][kNumQuartetClass] = {{0}};
     std::vector<int4> plan_h;        // host copy of the plan (for sharding)
     int *d_shell_atom = nullptr;     // atom index of every shell (gradients)
+    int2 *d_pk_tiles = nullptr;      // (i, j0) tiles of the stored-integral J/K kernel
+    int pk_tiles_n = 0, pk_tiles_nbf = -1;
     // batched bases: molecules own consecutive shells/functions; D/J/K hold
     // one dense nm x nm block per molecule, back to back
     int nmol = 1;
@@ -625,6 +627,123 @@ __global__ void jk_packed_kernel(const double *__restrict__ ints, const double *
     }
 }
 
+// ---- tiled stored-integral J/K (the HBM-bound path).  A CTA owns the
+// packed rows IJ = (i, j) for j in [j0, j0+32) of one i and streams them once
+// (coalesced, 32 consecutive KL per warp instruction).  With v' the
+// degeneracy-weighted integral, the EpiJK updates become:
+//   Jacc[i,j] += 2 v' D_kl   row sums, one atomic per row
+//   Jacc[k,l] += 2 v' D_ij   summed over the CTA's rows per 32-column chunk
+//   Kacc[i,k], Kacc[i,l]     into a shared row Ki (same i for the whole CTA)
+//   Kacc[j,k], Kacc[j,l]     into shared rows Kj[j - j0]
+// Lanes of a chunk that share k form contiguous runs; k-indexed sums are
+// reduced over each run with shuffles before one shared add.  (A variant
+// with one warp per column range and per-element shared adds of Kacc[j,l]
+// measured slower: FP64 shared-memory atomics dominate it.)
+constexpr int kPkRows = 32, kPkWarps = 8;
+
+__device__ __forceinline__ double run_sum(double x, int key, int lane)
+{
+    // inclusive segmented scan over runs of equal `key` (contiguous lanes)
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, x, o);
+        const int ky = __shfl_up_sync(0xffffffffu, key, o);
+        if (lane >= o && ky == key) x += y;
+    }
+    return x;
+}
+
+__global__ void __launch_bounds__(kPkWarps * 32) jk_packed_tiled_kernel(const double *__restrict__ ints,
+                                                                        const double *__restrict__ D, double *Jacc,
+                                                                        double *Kacc, int n,
+                                                                        const int2 *__restrict__ tiles, int ntiles)
+{
+    extern __shared__ double smem[];
+    double *Ki = smem;                          // [n]
+    double *Kj = smem + n;                      // [kPkRows][n]
+    double *jc = smem + n + kPkRows * n;        // [kPkWarps][32]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int i = tiles[t].x, j0 = tiles[t].y;
+        const int nrows = min(kPkRows, i + 1 - j0);
+        for (int x = tid; x < n + kPkRows * n; x += blockDim.x) smem[x] = 0.0;
+        __syncthreads();
+        const int64_t I0 = (int64_t)i * (i + 1) / 2;
+        const int64_t KLmax = I0 + j0 + nrows - 1;
+        const double *Di = D + (int64_t)i * n;
+        double jrow[kPkRows / kPkWarps];
+#pragma unroll
+        for (int q = 0; q < kPkRows / kPkWarps; ++q) jrow[q] = 0.0;
+        for (int64_t c0 = 0; c0 <= KLmax; c0 += 32) {
+            const int64_t KL = c0 + lane;
+            const bool colok = KL <= KLmax;
+            int k = (int)((sqrt(8.0 * (double)KL + 1.0) - 1.0) * 0.5);
+            while ((int64_t)k * (k + 1) / 2 > KL) --k;
+            while ((int64_t)(k + 1) * (k + 2) / 2 <= KL) ++k;
+            const int l = (int)(KL - (int64_t)k * (k + 1) / 2);
+            const int kk = colok ? k : -1;
+            const double Dkl = colok ? __ldg(D + (int64_t)k * n + l) : 0.0;
+            const double Dil = colok ? __ldg(Di + l) : 0.0, Dik = colok ? __ldg(Di + k) : 0.0;
+            const double skl = (k == l ? 0.5 : 1.0);
+            double kik = 0.0, kil = 0.0, jcol = 0.0;
+#pragma unroll
+            for (int q = 0; q < kPkRows / kPkWarps; ++q) {
+                const int r = warp + kPkWarps * q;
+                const int j = j0 + r;
+                const int64_t IJ = I0 + j;
+                double kjk = 0.0;
+                if (r < nrows && colok && KL <= IJ) {
+                    const double v = __ldg(ints + IJ * (IJ + 1) / 2 + KL) * (i == j ? 0.5 : 1.0) * skl *
+                                     (IJ == KL ? 0.5 : 1.0);
+                    const double *Dj = D + (int64_t)j * n;
+                    jrow[q] += v * Dkl;
+                    jcol += 2.0 * v * __ldg(Di + j);
+                    kik += v * __ldg(Dj + l);
+                    kil += v * __ldg(Dj + k);
+                    kjk = v * Dil;
+                    atomicAdd(Kj + r * n + l, v * Dik);
+                }
+                // Kacc[j,k] += v' D_il: reduce over the run of lanes with this k
+                if (r < nrows) {
+                    const double sum = run_sum(kjk, kk, lane);
+                    const int knext = __shfl_down_sync(0xffffffffu, kk, 1);
+                    if (kk >= 0 && (lane == 31 || knext != kk) && sum != 0.0) atomicAdd(Kj + r * n + kk, sum);
+                }
+            }
+            {
+                const double sum = run_sum(kik, kk, lane);
+                const int knext = __shfl_down_sync(0xffffffffu, kk, 1);
+                if (kk >= 0 && (lane == 31 || knext != kk) && sum != 0.0) atomicAdd(Ki + kk, sum);
+            }
+            if (kil != 0.0) atomicAdd(Ki + l, kil);
+            jc[warp * 32 + lane] = jcol;
+            __syncthreads();
+            if (warp == 0) {
+                double s = 0.0;
+#pragma unroll
+                for (int w = 0; w < kPkWarps; ++w) s += jc[w * 32 + lane];
+                if (colok && s != 0.0) atomicAdd(Jacc + (int64_t)k * n + l, s);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int q = 0; q < kPkRows / kPkWarps; ++q) {
+            double x = jrow[q];
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            const int r = warp + kPkWarps * q;
+            if (lane == 0 && r < nrows && x != 0.0) atomicAdd(Jacc + (int64_t)i * n + j0 + r, 2.0 * x);
+        }
+        __syncthreads();
+        for (int x = tid; x <= i; x += blockDim.x)
+            if (Ki[x] != 0.0) atomicAdd(Kacc + (int64_t)i * n + x, Ki[x]);
+        for (int x = tid; x < nrows * n; x += blockDim.x) {
+            const int r = x / n, c = x - r * n;
+            if (c <= i && Kj[x] != 0.0) atomicAdd(Kacc + (int64_t)(j0 + r) * n + c, Kj[x]);
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void boys_eval_kernel(int m, int count, const double *T, double *F)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -737,6 +856,7 @@ void pqb_destroy(pqb_ctx *ctx)
     cudaSetDevice(ctx->device);
     release_basis(ctx);
     free_dev(ctx->d_atoms);
+    free_dev(ctx->d_pk_tiles);
     for (int k = 0; k < pqb_ctx::kStreams; ++k) {
         if (ctx->streams[k]) cudaStreamDestroy(ctx->streams[k]);
         if (ctx->ev_join[k]) cudaEventDestroy(ctx->ev_join[k]);
@@ -1237,7 +1357,29 @@ int pqb_jk_packed(pqb_ctx *ctx, const double *ints, int64_t len, const double *D
     cudaStream_t st = (cudaStream_t)stream;
     PQB_CK(ctx, cudaMemsetAsync(J, 0, sizeof(double) * nbf * nbf, st));
     PQB_CK(ctx, cudaMemsetAsync(K, 0, sizeof(double) * nbf * nbf, st));
-    jk_packed_kernel<<<(unsigned)P, 256, 0, st>>>(ints, D, J, K, nbf);
+    const size_t smem = sizeof(double) * ((size_t)(1 + kPkRows) * nbf + kPkWarps * 32);
+    if (smem <= 200 * 1024) {
+        if (ctx->pk_tiles_nbf != nbf) {
+            // tiles (i, j0), heaviest (largest i) first
+            std::vector<int2> tiles;
+            for (int i = nbf - 1; i >= 0; --i)
+                for (int j0 = 0; j0 <= i; j0 += kPkRows) tiles.push_back(make_int2(i, j0));
+            free_dev(ctx->d_pk_tiles);
+            ctx->d_pk_tiles = nullptr;
+            PQB_CK(ctx, cudaMalloc(&ctx->d_pk_tiles, sizeof(int2) * tiles.size()));
+            PQB_CK(ctx, cudaMemcpy(ctx->d_pk_tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
+            ctx->pk_tiles_n = (int)tiles.size();
+            ctx->pk_tiles_nbf = nbf;
+            PQB_CK(ctx, cudaFuncSetAttribute(jk_packed_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             200 * 1024));
+        }
+        int grid = ctx->pk_tiles_n;
+        if (grid > ctx->nsm * 8) grid = ctx->nsm * 8;
+        jk_packed_tiled_kernel<<<grid, kPkWarps * 32, smem, st>>>(ints, D, J, K, nbf, ctx->d_pk_tiles,
+                                                                  ctx->pk_tiles_n);
+    } else {
+        jk_packed_kernel<<<(unsigned)P, 256, 0, st>>>(ints, D, J, K, nbf);
+    }
     symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, nbf);
     symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K, nbf);
     PQB_CK(ctx, cudaGetLastError());
