@@ -671,10 +671,25 @@ __global__ void __launch_bounds__(kPkWarps * 32) jk_packed_tiled_kernel(const do
         const int64_t I0 = (int64_t)i * (i + 1) / 2;
         const int64_t KLmax = I0 + j0 + nrows - 1;
         const double *Di = D + (int64_t)i * n;
-        double jrow[kPkRows / kPkWarps];
+        double jrow[kPkRows / kPkWarps], vnext[kPkRows / kPkWarps];
 #pragma unroll
         for (int q = 0; q < kPkRows / kPkWarps; ++q) jrow[q] = 0.0;
+        // the integrals of the next chunk are loaded while this one is digested
+        auto load_chunk = [&](int64_t c, double *v) {
+            const int64_t kl = c + lane;
+#pragma unroll
+            for (int q = 0; q < kPkRows / kPkWarps; ++q) {
+                const int r = warp + kPkWarps * q;
+                const int64_t IJ = I0 + j0 + r;
+                v[q] = (r < nrows && kl <= KLmax && kl <= IJ) ? __ldg(ints + IJ * (IJ + 1) / 2 + kl) : 0.0;
+            }
+        };
+        load_chunk(0, vnext);
         for (int64_t c0 = 0; c0 <= KLmax; c0 += 32) {
+            double vcur[kPkRows / kPkWarps];
+#pragma unroll
+            for (int q = 0; q < kPkRows / kPkWarps; ++q) vcur[q] = vnext[q];
+            if (c0 + 32 <= KLmax) load_chunk(c0 + 32, vnext);
             const int64_t KL = c0 + lane;
             const bool colok = KL <= KLmax;
             int k = (int)((sqrt(8.0 * (double)KL + 1.0) - 1.0) * 0.5);
@@ -693,8 +708,7 @@ __global__ void __launch_bounds__(kPkWarps * 32) jk_packed_tiled_kernel(const do
                 const int64_t IJ = I0 + j;
                 double kjk = 0.0;
                 if (r < nrows && colok && KL <= IJ) {
-                    const double v = __ldg(ints + IJ * (IJ + 1) / 2 + KL) * (i == j ? 0.5 : 1.0) * skl *
-                                     (IJ == KL ? 0.5 : 1.0);
+                    const double v = vcur[q] * (i == j ? 0.5 : 1.0) * skl * (IJ == KL ? 0.5 : 1.0);
                     const double *Dj = D + (int64_t)j * n;
                     jrow[q] += v * Dkl;
                     jcol += 2.0 * v * __ldg(Di + j);
