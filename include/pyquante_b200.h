@@ -125,7 +125,9 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
 
 /* One class list of the plan only (part 0 FP64 list / 1 FP32-eligible list,
  * class 0..20), accumulating unsymmetrised contributions into Jacc/Kacc
- * (not cleared).  For per-class timing and tuning. */
+ * (not cleared).  The contributions are those of the element-scaled density
+ * D_kl r_k r_l (r = the per-function scales of pqb_shells_upload); the full
+ * pqb_jk_direct applies r_i r_j to J and K.  For per-class timing and tuning. */
 int pqb_jk_direct_class(pqb_ctx *ctx, const double *D, double *Jacc, double *Kacc, int part, int qclass, int mode,
                         void *stream);
 

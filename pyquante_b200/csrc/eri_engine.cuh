@@ -46,20 +46,44 @@ __device__ __forceinline__ int64_t fpair(int i, int j)
 // ------------------------------------------------------------ epilogues --
 // Every epilogue offers
 //   thread_quartet<LA,LB,LC,LD>(q, acc[NAB*NCD])   whole quartet, thread mode
-//   block_ab<LA,LB,LC,LD>(q, ia, ib, acc[NCD], scr) one bra component pair,
-//                                                    block mode (scr: per-slot
-//                                                    shared scratch)
-//   block_flush<LA,LB,LC,LD>(q, scr, t, nt)          after a block barrier
-//   kScratch<LA,LB,LC,LD>                            doubles of scr per slot
+//   kTile                                          false: block mode calls
+//     block_ab<LA,LB,LC,LD>(q, ia, ib, acc[NCD])     per bra component pair;
+//                                                  true: block mode stores the
+//     tile_store<LA,LB,LC,LD>(q, ia, ib, acc, V)     quartet's weighted integrals
+//     tile_reduce<LA,LB,LC,LD>(q, V, t, nt)          in a shared tile V and reduces
+//                                                    them after a block barrier
 
 __device__ __forceinline__ bool skip_bra(const QCtx &q, int fi, int fj) { return q.sa == q.sb && fi < fj; }
+
+// 1 if (x0, y0) > (x1, y1) lexicographically, 1/2 if equal, 0 if less.
+__host__ __device__ constexpr double lex_weight(int x0, int y0, int x1, int y1)
+{
+    return x0 != x1 ? (x0 > x1 ? 1.0 : 0.0) : (y0 != y1 ? (y0 > y1 ? 1.0 : 0.0) : 0.5);
+}
+
+// Degeneracy weight of component (ia ib|ic id) of a unique shell quartet:
+// 0 outside the canonical ranges i >= j, k >= l, ij >= kl; a factor 1/2 for
+// each of i == j, k == l, ij == kl; else 1.  Only the flags are runtime:
+//   bd: the bra's two shells are one shell (then i - j = ia - ib),
+//   kd: the same for the ket,
+//   qd: bra pair == ket pair (then IJ vs KL orders (ia, ib) vs (ic, id)
+//       lexicographically when the first shell holds the higher function
+//       indices, af, or bd; otherwise (ib, ia) vs (id, ic)).
+// In the unrolled loops the component indices are constants, so each weight
+// is a few selects: no branches and no 64-bit pair indices per component.
+__device__ __forceinline__ double comp_weight(int ia, int ib, int ic, int id, bool bd, bool kd, bool qd, bool af)
+{
+    const double wb = ia > ib ? 1.0 : (ia == ib ? 0.5 : 0.0);
+    const double wk = ic > id ? 1.0 : (ic == id ? 0.5 : 0.0);
+    const double wq = (bd || af) ? lex_weight(ia, ib, ic, id) : lex_weight(ib, ia, id, ic);
+    return (bd ? wb : 1.0) * (kd ? wk : 1.0) * (qd ? wq : 1.0);
+}
 
 // Packed canonical integrals at ijkl2intindex (Src/cints.c:413-425), 64-bit.
 struct EpiPacked {
     double *out;
     const double *fscale;
-    template <int LA, int LB, int LC, int LD>
-    static constexpr int kScratch = 0;
+    static constexpr bool kTile = false;
     template <int LC, int LD, typename R>
     __device__ __forceinline__ void ab(const QCtx &q, int ia, int ib, const R *acc) const
     {
@@ -88,163 +112,232 @@ struct EpiPacked {
         for (int ab = 0; ab < ncart(LA) * NB; ++ab) this->ab<LC, LD, R>(q, ab / NB, ab % NB, acc + ab * NCD);
     }
     template <int LA, int LB, int LC, int LD, typename R>
-    __device__ __forceinline__ void block_ab(const QCtx &q, int ia, int ib, const R *acc, double *) const
+    __device__ __forceinline__ void block_ab(const QCtx &q, int ia, int ib, const R *acc) const
     {
         ab<LC, LD, R>(q, ia, ib, acc);
     }
-    template <int LA, int LB, int LC, int LD>
-    __device__ __forceinline__ void block_flush(const QCtx &, double *, int, int) const {}
 };
 
 // Direct J/K digestion of unique quartets with 8-fold degeneracy weights:
 //   Jacc[i,j] += 2 v' D_kl,  Jacc[k,l] += 2 v' D_ij,
 //   Kacc[i,k] += v' D_jl, Kacc[i,l] += v' D_jk, Kacc[j,k] += v' D_il, Kacc[j,l] += v' D_ik,
-// v' = v * (1/2 if i==j) (1/2 if k==l) (1/2 if ij==kl); then J = Jacc + Jacc^T,
-// K = Kacc + Kacc^T reproduce J_ij = sum_kl (ij|kl) D_kl and
-// K_ij = sum_kl (ik|jl) D_kl of PyQuante/Ints.py:195-223 for symmetric D.
-// Contributions are first summed per quartet into its six J/K blocks
-// (ab, cd, ac, ad, bc, bd) and then added to global memory once per block
-// element, so a quartet costs NA NB + NC ND + (NA+NB)(NC+ND) atomics.
+// v' = v * comp_weight; then J = Jacc + Jacc^T, K = Kacc + Kacc^T reproduce
+// J_ij = sum_kl (ij|kl) D_kl and K_ij = sum_kl (ik|jl) D_kl of
+// PyQuante/Ints.py:195-223 for symmetric D.
+//
+// The integrals here are those of the shells' common contraction (no
+// per-component scale r_f): D is the pre-scaled density D'_kl = r_k r_l D_kl
+// and the caller multiplies J and K by r_i r_j afterwards, which gives the
+// same J and K as digesting the scaled integrals with D.
+//
+// Thread mode: the quartet's six D blocks are loaded once, the six J/K
+// blocks (ab, cd, ac, ad, bc, bd) are summed in registers, and each block
+// element goes to global memory with one atomic.  Block mode: the weighted
+// integrals go to a shared tile; each output element is then one thread's
+// reduction over the tile (no shared-memory atomics).
 struct EpiJK {
-    const double *D;
+    const double *D;        // pre-scaled density
     double *Jacc, *Kacc;
-    const double *fscale;
-    template <int LA, int LB, int LC, int LD>
-    static constexpr int kScratch = ncart(LA) * ncart(LB) + ncart(LC) * ncart(LD) +
-                                    (ncart(LA) + ncart(LB)) * (ncart(LC) + ncart(LD));
+    static constexpr bool kTile = true;
 
-    // digest one bra component pair: returns 2*sum_kl v' D_kl (the Jacc[i,j]
-    // term) and adds the other five block contributions through the sinks
-    template <int LC, int LD, typename R, class Sink>
-    __device__ __forceinline__ double ab(const QCtx &q, int ia, int ib, const R *acc, Sink &&sink) const
-    {
-        constexpr int NC = ncart(LC), ND = ncart(LD);
-        const int fi = q.fa + ia, fj = q.fb + ib;
-        if (skip_bra(q, fi, fj)) return 0.0;
-        const int64_t IJ = fpair(fi, fj);
-        const double sij = fscale[fi] * fscale[fj] * (fi == fj ? 0.5 : 1.0);
-        const double *Db = D + q.bo;
-        const int nm = q.nm;
-        const double Dij = __ldg(Db + (int64_t)fi * nm + fj);
-        const double *Di = Db + (int64_t)fi * nm, *Dj = Db + (int64_t)fj * nm;
-        double jij = 0.0;
-#pragma unroll
-        for (int ic = 0; ic < NC; ++ic) {
-            double kik = 0.0, kjk = 0.0;
-#pragma unroll
-            for (int id = 0; id < ND; ++id) {
-                const int fk = q.fc + ic, fl = q.fd + id;
-                if (q.sc == q.sd && fk < fl) continue;
-                const int64_t KL = fpair(fk, fl);
-                if (q.bra == q.ket && IJ < KL) continue;
-                const double v = (double)acc[ic * ND + id] * sij * fscale[fk] * fscale[fl] *
-                                 (fk == fl ? 0.5 : 1.0) * (IJ == KL ? 0.5 : 1.0);
-                jij += v * __ldg(Db + (int64_t)fk * nm + fl);
-                sink.jcd(ic * ND + id, 2.0 * v * Dij);
-                kik += v * __ldg(Dj + fl);
-                kjk += v * __ldg(Di + fl);
-                sink.kad(ia, id, v * __ldg(Dj + fk));
-                sink.kbd(ib, id, v * __ldg(Di + fk));
-            }
-            sink.kac(ia, ic, kik);
-            sink.kbc(ib, ic, kjk);
-        }
-        return 2.0 * jij;
-    }
-
-    // thread mode: block sums in registers, then one atomic per element
     template <int LA, int LB, int LC, int LD, typename R>
     __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc) const
     {
         constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NCD = NC * ND;
-        struct Regs {
-            double jcd_[NCD], kac_[NC], kad_[ND], kbc_[NB][NC], kbd_[NB][ND];
-            __device__ void jcd(int c, double v) { jcd_[c] += v; }
-            __device__ void kac(int, int c, double v) { kac_[c] += v; }
-            __device__ void kad(int, int d, double v) { kad_[d] += v; }
-            __device__ void kbc(int b, int c, double v) { kbc_[b][c] += v; }
-            __device__ void kbd(int b, int d, double v) { kbd_[b][d] += v; }
-        } r;
+        const bool bd = q.sa == q.sb, kd = q.sc == q.sd, qd = q.bra == q.ket, af = q.fa > q.fb;
+        const double *Db = D + q.bo;
+        double *Jb = Jacc + q.bo, *Kb = Kacc + q.bo;
+        const int64_t nm = q.nm;
+        const double *Da = Db + q.fa * nm, *Dbr = Db + q.fb * nm, *Dc = Db + q.fc * nm;
+        // Coulomb: Jacc[a,b] and Jacc[c,d]
+        {
+            double dab[NA][NB], dcd[NC][ND], jcd[NC][ND];
 #pragma unroll
-        for (int c = 0; c < NCD; ++c) r.jcd_[c] = 0.0;
+            for (int a = 0; a < NA; ++a)
 #pragma unroll
-        for (int b = 0; b < NB; ++b) {
+                for (int b = 0; b < NB; ++b) dab[a][b] = __ldg(Da + a * nm + q.fb + b);
 #pragma unroll
-            for (int c = 0; c < NC; ++c) r.kbc_[b][c] = 0.0;
+            for (int c = 0; c < NC; ++c)
 #pragma unroll
-            for (int d = 0; d < ND; ++d) r.kbd_[b][d] = 0.0;
+                for (int d = 0; d < ND; ++d) {
+                    dcd[c][d] = __ldg(Dc + c * nm + q.fd + d);
+                    jcd[c][d] = 0.0;
+                }
+#pragma unroll
+            for (int a = 0; a < NA; ++a)
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    double jab = 0.0;
+#pragma unroll
+                    for (int c = 0; c < NC; ++c)
+#pragma unroll
+                        for (int d = 0; d < ND; ++d) {
+                            const double v = (double)acc[(a * NB + b) * NCD + c * ND + d] *
+                                             comp_weight(a, b, c, d, bd, kd, qd, af);
+                            jab = fma(v, dcd[c][d], jab);
+                            jcd[c][d] = fma(v, dab[a][b], jcd[c][d]);
+                        }
+                    if (jab != 0.0) atomicAdd(Jb + (q.fa + a) * nm + q.fb + b, 2.0 * jab);
+                }
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+#pragma unroll
+                for (int d = 0; d < ND; ++d)
+                    if (jcd[c][d] != 0.0) atomicAdd(Jb + (q.fc + c) * nm + q.fd + d, 2.0 * jcd[c][d]);
         }
+        // exchange rows of the bra's first shell: Kacc[a,c] += v D_bd, Kacc[a,d] += v D_bc
+        {
+            double dbd[NB][ND], dbc[NB][NC];
 #pragma unroll
-        for (int ia = 0; ia < NA; ++ia) {
+            for (int b = 0; b < NB; ++b) {
 #pragma unroll
-            for (int c = 0; c < NC; ++c) r.kac_[c] = 0.0;
+                for (int d = 0; d < ND; ++d) dbd[b][d] = __ldg(Dbr + b * nm + q.fd + d);
 #pragma unroll
-            for (int d = 0; d < ND; ++d) r.kad_[d] = 0.0;
-#pragma unroll
-            for (int ib = 0; ib < NB; ++ib) {
-                const double jij = ab<LC, LD, R>(q, ia, ib, acc + (ia * NB + ib) * NCD, r);
-                if (jij != 0.0) atomicAdd(Jacc + q.bo + (int64_t)(q.fa + ia) * q.nm + q.fb + ib, jij);
+                for (int c = 0; c < NC; ++c) dbc[b][c] = __ldg(Dbr + b * nm + q.fc + c);
             }
 #pragma unroll
-            for (int c = 0; c < NC; ++c)
-                if (r.kac_[c] != 0.0) atomicAdd(Kacc + q.bo + (int64_t)(q.fa + ia) * q.nm + q.fc + c, r.kac_[c]);
+            for (int a = 0; a < NA; ++a) {
+                double kac[NC], kad[ND];
 #pragma unroll
-            for (int d = 0; d < ND; ++d)
-                if (r.kad_[d] != 0.0) atomicAdd(Kacc + q.bo + (int64_t)(q.fa + ia) * q.nm + q.fd + d, r.kad_[d]);
+                for (int c = 0; c < NC; ++c) kac[c] = 0.0;
+#pragma unroll
+                for (int d = 0; d < ND; ++d) kad[d] = 0.0;
+#pragma unroll
+                for (int b = 0; b < NB; ++b)
+#pragma unroll
+                    for (int c = 0; c < NC; ++c)
+#pragma unroll
+                        for (int d = 0; d < ND; ++d) {
+                            const double v = (double)acc[(a * NB + b) * NCD + c * ND + d] *
+                                             comp_weight(a, b, c, d, bd, kd, qd, af);
+                            kac[c] = fma(v, dbd[b][d], kac[c]);
+                            kad[d] = fma(v, dbc[b][c], kad[d]);
+                        }
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+                    if (kac[c] != 0.0) atomicAdd(Kb + (q.fa + a) * nm + q.fc + c, kac[c]);
+#pragma unroll
+                for (int d = 0; d < ND; ++d)
+                    if (kad[d] != 0.0) atomicAdd(Kb + (q.fa + a) * nm + q.fd + d, kad[d]);
+            }
         }
+        // exchange rows of the bra's second shell: Kacc[b,c] += v D_ad, Kacc[b,d] += v D_ac
+        {
+            double dad[NA][ND], dac[NA][NC];
 #pragma unroll
-        for (int b = 0; b < NB; ++b) {
+            for (int a = 0; a < NA; ++a) {
 #pragma unroll
-            for (int c = 0; c < NC; ++c)
-                if (r.kbc_[b][c] != 0.0) atomicAdd(Kacc + q.bo + (int64_t)(q.fb + b) * q.nm + q.fc + c, r.kbc_[b][c]);
+                for (int d = 0; d < ND; ++d) dad[a][d] = __ldg(Da + a * nm + q.fd + d);
 #pragma unroll
-            for (int d = 0; d < ND; ++d)
-                if (r.kbd_[b][d] != 0.0) atomicAdd(Kacc + q.bo + (int64_t)(q.fb + b) * q.nm + q.fd + d, r.kbd_[b][d]);
+                for (int c = 0; c < NC; ++c) dac[a][c] = __ldg(Da + a * nm + q.fc + c);
+            }
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                double kbc[NC], kbd[ND];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) kbc[c] = 0.0;
+#pragma unroll
+                for (int d = 0; d < ND; ++d) kbd[d] = 0.0;
+#pragma unroll
+                for (int a = 0; a < NA; ++a)
+#pragma unroll
+                    for (int c = 0; c < NC; ++c)
+#pragma unroll
+                        for (int d = 0; d < ND; ++d) {
+                            const double v = (double)acc[(a * NB + b) * NCD + c * ND + d] *
+                                             comp_weight(a, b, c, d, bd, kd, qd, af);
+                            kbc[c] = fma(v, dad[a][d], kbc[c]);
+                            kbd[d] = fma(v, dac[a][c], kbd[d]);
+                        }
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+                    if (kbc[c] != 0.0) atomicAdd(Kb + (q.fb + b) * nm + q.fc + c, kbc[c]);
+#pragma unroll
+                for (int d = 0; d < ND; ++d)
+                    if (kbd[d] != 0.0) atomicAdd(Kb + (q.fb + b) * nm + q.fd + d, kbd[d]);
+            }
         }
-#pragma unroll
-        for (int c = 0; c < NCD; ++c)
-            if (r.jcd_[c] != 0.0) atomicAdd(Jacc + q.bo + (int64_t)(q.fc + c / ND) * q.nm + q.fd + c % ND, r.jcd_[c]);
     }
 
-    // block mode: scratch layout [jab NAB | jcd NCD | kac NA*NC | kad NA*ND | kbc NB*NC | kbd NB*ND]
-    template <int LA, int LB, int LC, int LD, typename R>
-    __device__ __forceinline__ void block_ab(const QCtx &q, int ia, int ib, const R *acc, double *scr) const
-    {
-        constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-        struct Smem {
-            double *s;
-            __device__ void jcd(int c, double v) { atomicAdd(s + NA * NB + c, v); }
-            __device__ void kac(int a, int c, double v) { atomicAdd(s + NA * NB + NC * ND + a * NC + c, v); }
-            __device__ void kad(int a, int d, double v) { atomicAdd(s + NA * NB + NC * ND + NA * NC + a * ND + d, v); }
-            __device__ void kbc(int b, int c, double v)
-            {
-                atomicAdd(s + NA * NB + NC * ND + NA * NC + NA * ND + b * NC + c, v);
-            }
-            __device__ void kbd(int b, int d, double v)
-            {
-                atomicAdd(s + NA * NB + NC * ND + NA * NC + NA * ND + NB * NC + b * ND + d, v);
-            }
-        } sm{scr};
-        scr[ia * NB + ib] = ab<LC, LD, R>(q, ia, ib, acc, sm);
-    }
+    // block mode: the tile row of bra component (ia, ib) holds its NCD
+    // weighted integrals (row stride NCD + 1 spreads the rows over the banks)
     template <int LA, int LB, int LC, int LD>
-    __device__ __forceinline__ void block_flush(const QCtx &q, const double *scr, int t, int nt) const
+    static constexpr int kTileStride = ncart(LC) * ncart(LD) + 1;
+
+    template <int LA, int LB, int LC, int LD, typename R>
+    __device__ __forceinline__ void tile_store(const QCtx &q, int ia, int ib, const R *acc, double *V) const
     {
-        constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-        constexpr int O1 = NA * NB, O2 = O1 + NC * ND, O3 = O2 + NA * NC, O4 = O3 + NA * ND, O5 = O4 + NB * NC,
-                      O6 = O5 + NB * ND;
-        for (int e = t; e < O6; e += nt) {
-            const double v = scr[e];
-            if (v == 0.0) continue;
-            int row, col;
-            double *M = Kacc;
-            if (e < O1) { row = q.fa + e / NB; col = q.fb + e % NB; M = Jacc; }
-            else if (e < O2) { row = q.fc + (e - O1) / ND; col = q.fd + (e - O1) % ND; M = Jacc; }
-            else if (e < O3) { row = q.fa + (e - O2) / NC; col = q.fc + (e - O2) % NC; }
-            else if (e < O4) { row = q.fa + (e - O3) / ND; col = q.fd + (e - O3) % ND; }
-            else if (e < O5) { row = q.fb + (e - O4) / NC; col = q.fc + (e - O4) % NC; }
-            else { row = q.fb + (e - O5) / ND; col = q.fd + (e - O5) % ND; }
-            atomicAdd(M + q.bo + (int64_t)row * q.nm + col, v);
+        constexpr int NC = ncart(LC), ND = ncart(LD), NB = ncart(LB);
+        constexpr int ST = kTileStride<LA, LB, LC, LD>;
+        const bool bd = q.sa == q.sb, kd = q.sc == q.sd, qd = q.bra == q.ket, af = q.fa > q.fb;
+        const int64_t nm = q.nm;
+        const double *Dc = D + q.bo + q.fc * nm + q.fd;
+        // runtime bra indices: the bra and quartet factors of comp_weight in closed form
+        const double wb = bd ? (ia > ib ? 1.0 : (ia == ib ? 0.5 : 0.0)) : 1.0;
+        const int x0 = (bd || af) ? ia : ib, y0 = (bd || af) ? ib : ia;
+        double jab = 0.0;
+        double *row = V + (ia * NB + ib) * ST;
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+                const double wk = kd ? (c > d ? 1.0 : (c == d ? 0.5 : 0.0)) : 1.0;
+                const int x1 = (bd || af) ? c : d, y1 = (bd || af) ? d : c;
+                const double wq = qd ? (x0 != x1 ? (x0 > x1 ? 1.0 : 0.0) : (y0 != y1 ? (y0 > y1 ? 1.0 : 0.0) : 0.5))
+                                     : 1.0;
+                const double v = (double)acc[c * ND + d] * (wb * wk * wq);
+                jab = fma(v, __ldg(Dc + c * nm + d), jab);
+                row[c * ND + d] = v;
+            }
+        if (jab != 0.0) atomicAdd(Jacc + q.bo + (q.fa + ia) * nm + q.fb + ib, 2.0 * jab);
+    }
+
+    // outputs of one quartet: Jacc[c,d] (NCD), Kacc[a,c], Kacc[a,d],
+    // Kacc[b,c], Kacc[b,d]; threads t, t + nt, ... of the quartet's slot
+    template <int LA, int LB, int LC, int LD>
+    __device__ __forceinline__ void tile_reduce(const QCtx &q, const double *V, int t, int nt) const
+    {
+        constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NCD = NC * ND;
+        constexpr int ST = kTileStride<LA, LB, LC, LD>;
+        constexpr int O1 = NCD, O2 = O1 + NA * NC, O3 = O2 + NA * ND, O4 = O3 + NB * NC, O5 = O4 + NB * ND;
+        const int64_t nm = q.nm;
+        const double *Db = D + q.bo;
+        for (int o = t; o < O5; o += nt) {
+            double s = 0.0;
+            double *dst;
+            if (o < O1) {                     // Jacc[c,d] = 2 sum_ab v D_ab
+                const int c = o / ND, d = o - (o / ND) * ND;
+                for (int a = 0; a < NA; ++a)
+                    for (int b = 0; b < NB; ++b)
+                        s = fma(V[(a * NB + b) * ST + c * ND + d], __ldg(Db + (q.fa + a) * nm + q.fb + b), s);
+                s *= 2.0;
+                dst = Jacc + q.bo + (q.fc + c) * nm + q.fd + d;
+            } else if (o < O2) {              // Kacc[a,c] = sum_bd v D_bd
+                const int a = (o - O1) / NC, c = (o - O1) - ((o - O1) / NC) * NC;
+                for (int b = 0; b < NB; ++b)
+                    for (int d = 0; d < ND; ++d)
+                        s = fma(V[(a * NB + b) * ST + c * ND + d], __ldg(Db + (q.fb + b) * nm + q.fd + d), s);
+                dst = Kacc + q.bo + (q.fa + a) * nm + q.fc + c;
+            } else if (o < O3) {              // Kacc[a,d] = sum_bc v D_bc
+                const int a = (o - O2) / ND, d = (o - O2) - ((o - O2) / ND) * ND;
+                for (int b = 0; b < NB; ++b)
+                    for (int c = 0; c < NC; ++c)
+                        s = fma(V[(a * NB + b) * ST + c * ND + d], __ldg(Db + (q.fb + b) * nm + q.fc + c), s);
+                dst = Kacc + q.bo + (q.fa + a) * nm + q.fd + d;
+            } else if (o < O4) {              // Kacc[b,c] = sum_ad v D_ad
+                const int b = (o - O3) / NC, c = (o - O3) - ((o - O3) / NC) * NC;
+                for (int a = 0; a < NA; ++a)
+                    for (int d = 0; d < ND; ++d)
+                        s = fma(V[(a * NB + b) * ST + c * ND + d], __ldg(Db + (q.fa + a) * nm + q.fd + d), s);
+                dst = Kacc + q.bo + (q.fb + b) * nm + q.fc + c;
+            } else {                          // Kacc[b,d] = sum_ac v D_ac
+                const int b = (o - O4) / ND, d = (o - O4) - ((o - O4) / ND) * ND;
+                for (int a = 0; a < NA; ++a)
+                    for (int c = 0; c < NC; ++c)
+                        s = fma(V[(a * NB + b) * ST + c * ND + d], __ldg(Db + (q.fa + a) * nm + q.fc + c), s);
+                dst = Kacc + q.bo + (q.fb + b) * nm + q.fd + d;
+            }
+            if (s != 0.0) atomicAdd(dst, s);
         }
     }
 };
@@ -253,8 +346,7 @@ struct EpiJK {
 struct EpiSchwarz {
     unsigned long long *Q2bits;   // bit patterns of non-negative doubles
     const double *fscale;
-    template <int LA, int LB, int LC, int LD>
-    static constexpr int kScratch = 0;
+    static constexpr bool kTile = false;
     template <int LC, int LD, typename R>
     __device__ __forceinline__ void ab(const QCtx &q, int ia, int ib, const R *acc) const
     {
@@ -276,12 +368,10 @@ struct EpiSchwarz {
         for (int ab = 0; ab < ncart(LA) * NB; ++ab) this->ab<LC, LD, R>(q, ab / NB, ab % NB, acc + ab * NCD);
     }
     template <int LA, int LB, int LC, int LD, typename R>
-    __device__ __forceinline__ void block_ab(const QCtx &q, int ia, int ib, const R *acc, double *) const
+    __device__ __forceinline__ void block_ab(const QCtx &q, int ia, int ib, const R *acc) const
     {
         ab<LC, LD, R>(q, ia, ib, acc);
     }
-    template <int LA, int LB, int LC, int LD>
-    __device__ __forceinline__ void block_flush(const QCtx &, double *, int, int) const {}
 };
 
 // ---------------------------------------------------------- thread mode --
@@ -311,42 +401,51 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
 #pragma unroll
         for (int c = 0; c < NAB * NCD; ++c) acc[c] = (R)0;
         const int npk = pk.nprim;
+        const PrimPair *pbp = prims + pb.prim_off, *pkp = prims + pk.prim_off;
         int ib = e.z / npk, ik = e.z - (e.z / npk) * npk;
-        PrimPair P = prims[pb.prim_off + ib];
+        PrimJK P = load_prim_jk(pbp + ib);
+        PrimJK Qn = load_prim_jk(pkp + ik);
         for (int t = 0; t < e.w; ++t) {
-            const PrimPair Q = prims[pk.prim_off + ik];
-            const double zpe = P.zeta + Q.zeta;
+            const PrimJK Q = Qn;
+            // next primitive quartet's ket pair is fetched while this one computes
+            int ik2 = ik + 1, ib2 = ib;
+            if (ik2 == npk) {
+                ik2 = 0;
+                ++ib2;
+            }
+            if (t + 1 < e.w) Qn = load_prim_jk(pkp + ik2);
+            const double zeta = P.zeta, eta = Q.zeta;
             const double PQx = P.P[0] - Q.P[0], PQy = P.P[1] - Q.P[1], PQz = P.P[2] - Q.P[2];
-            const double T = P.zeta * Q.zeta / zpe * (PQx * PQx + PQy * PQy + PQz * PQz);
-            const double pre = P.K * Q.K * rsqrt(zpe);
+            const double rs = rsqrt_nr(zeta + eta);
+            const double izpe = rs * rs;
+            const double T = zeta * eta * izpe * (PQx * PQx + PQy * PQy + PQz * PQz);
+            const double pre = P.K * Q.K * rs;
             double uu[NR], ww[NR];
-            rys_roots<NR>(T, uu, ww);
+            rys_roots_fast<NR>(T, uu, ww);
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
-                const double u = uu[r], w = ww[r];
+                const RysCoef k = rys_coef(uu[r], zeta, eta, P.izeta, Q.izeta, izpe);
                 R gx[G2D], gy[G2D], gz[G2D];
-                rys2d<LA, LB, LC, LD, R>(u, P.zeta, Q.zeta, P.P[0] - Ax, Q.P[0] - Cx, PQx, ABx, CDx, w * pre, gx);
-                rys2d<LA, LB, LC, LD, R>(u, P.zeta, Q.zeta, P.P[1] - Ay, Q.P[1] - Cy, PQy, ABy, CDy, 1.0, gy);
-                rys2d<LA, LB, LC, LD, R>(u, P.zeta, Q.zeta, P.P[2] - Az, Q.P[2] - Cz, PQz, ABz, CDz, 1.0, gz);
+                rys2d_c<LA, LB, LC, LD, R>(k, P.P[0] - Ax, Q.P[0] - Cx, PQx, ABx, CDx, ww[r] * pre, gx);
+                rys2d_c<LA, LB, LC, LD, R>(k, P.P[1] - Ay, Q.P[1] - Cy, PQy, ABy, CDy, 1.0, gy);
+                rys2d_c<LA, LB, LC, LD, R>(k, P.P[2] - Az, Q.P[2] - Cz, PQz, ABz, CDz, 1.0, gz);
 #pragma unroll
                 for (int ab = 0; ab < NAB; ++ab)
 #pragma unroll
                     for (int cd = 0; cd < NCD; ++cd) {
-                        const int ia = ab / NB, ib2 = ab % NB, ic = cd / ND, id = cd % ND;
-                        const int ox = ((cart_lx(LA, ia) * (LB + 1) + cart_lx(LB, ib2)) * (LC + 1) + cart_lx(LC, ic)) *
+                        const int ia = ab / NB, ib3 = ab % NB, ic = cd / ND, id = cd % ND;
+                        const int ox = ((cart_lx(LA, ia) * (LB + 1) + cart_lx(LB, ib3)) * (LC + 1) + cart_lx(LC, ic)) *
                                            (LD + 1) + cart_lx(LD, id);
-                        const int oy = ((cart_ly(LA, ia) * (LB + 1) + cart_ly(LB, ib2)) * (LC + 1) + cart_ly(LC, ic)) *
+                        const int oy = ((cart_ly(LA, ia) * (LB + 1) + cart_ly(LB, ib3)) * (LC + 1) + cart_ly(LC, ic)) *
                                            (LD + 1) + cart_ly(LD, id);
-                        const int oz = ((cart_lz(LA, ia) * (LB + 1) + cart_lz(LB, ib2)) * (LC + 1) + cart_lz(LC, ic)) *
+                        const int oz = ((cart_lz(LA, ia) * (LB + 1) + cart_lz(LB, ib3)) * (LC + 1) + cart_lz(LC, ic)) *
                                            (LD + 1) + cart_lz(LD, id);
                         acc[ab * NCD + cd] += gx[ox] * gy[oy] * gz[oz];
                     }
             }
-            if (++ik == npk) {
-                ik = 0;
-                ++ib;
-                if (t + 1 < e.w) P = prims[pb.prim_off + ib];
-            }
+            if (ib2 != ib && t + 1 < e.w) P = load_prim_jk(pbp + ib2);
+            ib = ib2;
+            ik = ik2;
         }
         const QCtx q = make_qctx(pb, pk, e.x, e.y);
         epi.template thread_quartet<LA, LB, LC, LD, R>(q, acc);
@@ -363,10 +462,10 @@ struct BlockLayout {
     static constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
     static constexpr int G2D = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
     static constexpr int NSQ = kBlockThreads / NAB;
-    static constexpr int SCR = Epi::template kScratch<LA, LB, LC, LD>;
     static constexpr size_t g_bytes = ((size_t)NSQ * 3 * NR * G2D * sizeof(R) + 15) / 16 * 16;
-    static constexpr size_t scr_bytes = (size_t)NSQ * SCR * sizeof(double);
-    static constexpr size_t bytes = g_bytes + scr_bytes;
+    // the integral tile of a tiled epilogue reuses the 2-D integral buffer
+    static constexpr size_t tile_bytes = Epi::kTile ? (size_t)NSQ * NAB * (NCD + 1) * sizeof(double) : 0;
+    static constexpr size_t bytes = g_bytes > tile_bytes ? g_bytes : tile_bytes;
 };
 
 struct SlotData {
@@ -385,10 +484,9 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
 {
     using Lay = BlockLayout<LA, LB, LC, LD, R, Epi>;
     constexpr int NB = Lay::NB, NC = Lay::NC, ND = Lay::ND, NAB = Lay::NAB, NCD = Lay::NCD;
-    constexpr int NR = Lay::NR, G2D = Lay::G2D, NSQ = Lay::NSQ, SCR = Lay::SCR;
+    constexpr int NR = Lay::NR, G2D = Lay::G2D, NSQ = Lay::NSQ;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *sg = reinterpret_cast<R *>(smem_raw);
-    double *sscr = reinterpret_cast<double *>(smem_raw + Lay::g_bytes);
     __shared__ SlotData sd[NSQ];
     __shared__ SlotPrim sp[NSQ];
     __shared__ double su[NSQ][NR], sw[NSQ][NR];
@@ -434,8 +532,6 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
                 for (int x = 0; x < 3; ++x) s.A[x] = s.AB[x] = s.C[x] = s.CD[x] = 0.0;
             }
         }
-        if constexpr (SCR > 0)
-            for (int t = tid; t < NSQ * SCR; t += kBlockThreads) sscr[t] = 0.0;
         __syncthreads();
         const int maxpp = s_maxpp;
 
@@ -517,13 +613,15 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
             }
         }
 
-        if (active && sd[slot].q.bra >= 0)
-            epi.template block_ab<LA, LB, LC, LD, R>(sd[slot].q, ia, ib, acc, sscr + slot * SCR);
-        if constexpr (SCR > 0) {
+        if constexpr (Epi::kTile) {
+            constexpr int ST = NCD + 1;
+            double *V = reinterpret_cast<double *>(smem_raw) + (size_t)slot * NAB * ST;
+            __syncthreads();   // the tile overwrites the 2-D integrals
+            if (active && sd[slot].q.bra >= 0) epi.template tile_store<LA, LB, LC, LD, R>(sd[slot].q, ia, ib, acc, V);
             __syncthreads();
-            // flush: NAB threads per slot walk the slot's scratch
-            if (active && sd[slot].q.bra >= 0)
-                epi.template block_flush<LA, LB, LC, LD>(sd[slot].q, sscr + slot * SCR, ab, NAB);
+            if (active && sd[slot].q.bra >= 0) epi.template tile_reduce<LA, LB, LC, LD>(sd[slot].q, V, ab, NAB);
+        } else {
+            if (active && sd[slot].q.bra >= 0) epi.template block_ab<LA, LB, LC, LD, R>(sd[slot].q, ia, ib, acc);
         }
         __syncthreads();
     }

@@ -4,11 +4,10 @@
 
 namespace pqb {
 cudaError_t launch_jk_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
-                          const double *D, double *Jacc, double *Kacc, const double *fscale, int n,
-                          cudaStream_t st, int nsm)
+                          const double *Dscaled, double *Jacc, double *Kacc, int n, cudaStream_t st, int nsm)
 {
     (void)n;
-    EpiJK epi{D, Jacc, Kacc, fscale};
+    EpiJK epi{Dscaled, Jacc, Kacc};
     return launch_eri<double>(qc, list, nq, pairs, prims, epi, st, nsm);
 }
 }  // namespace pqb

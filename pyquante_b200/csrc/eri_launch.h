@@ -1,7 +1,8 @@
 // Work items are int4 {bra pair, ket pair, first primitive quartet, count}:
 // a shell quartet's primitive quartets (bra-major, ket-minor) may be split
 // over several items whose contributions add (J/K digestion is linear).
-// Host-side entry points into the class-templated ERI engine, one per
+// Host-side entry points into the class-templated ERI engine (the direct J/K
+// ones take the pre-scaled density D'_kl = r_k r_l D_kl; see EpiJK), one per
 // (epilogue, precision) combination; each lives in its own translation unit
 // so the 21 class instantiations compile in parallel.
 #pragma once
@@ -17,11 +18,9 @@ struct EpiSchwarz;
 cudaError_t launch_packed_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                               double *out, const double *fscale, cudaStream_t st, int nsm);
 cudaError_t launch_jk_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
-                          const double *D, double *Jacc, double *Kacc, const double *fscale, int n,
-                          cudaStream_t st, int nsm);
+                          const double *Dscaled, double *Jacc, double *Kacc, int n, cudaStream_t st, int nsm);
 cudaError_t launch_jk_f32(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
-                          const double *D, double *Jacc, double *Kacc, const double *fscale, int n,
-                          cudaStream_t st, int nsm);
+                          const double *Dscaled, double *Jacc, double *Kacc, int n, cudaStream_t st, int nsm);
 cudaError_t launch_schwarz_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                                unsigned long long *Q2bits, const double *fscale, cudaStream_t st, int nsm);
 cudaError_t launch_grad_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,

@@ -38,6 +38,10 @@ struct pqb_ctx {
     PairInfo *d_pairs = nullptr;
     PrimPair *d_prims = nullptr;
     double *d_fscale = nullptr;
+    // direct J/K digest the shells' common-contraction integrals: the density
+    // is pre-scaled element-wise by escale[(i,j)] = r_i r_j (r = fscale) into
+    // d_Dscaled, and J, K are scaled by the same factors when symmetrised
+    double *d_escale = nullptr, *d_Dscaled = nullptr;
     unsigned long long *d_q2 = nullptr;
     std::vector<PairInfo> pairs;
     std::vector<double> Q;           // Schwarz factors (host)
@@ -105,8 +109,8 @@ static void free_dev(void *p)
 // ===================================================================== kernels
 
 // In-place M = M + M^T (the J/K accumulators hold one triangle's worth of
-// each unique contribution; see EpiJK).
-__global__ void symmetrize_kernel(double *M, int n)
+// each unique contribution; see EpiJK), times S element-wise when S is given.
+__global__ void symmetrize_kernel(double *M, int n, const double *__restrict__ S)
 {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t P = (int64_t)n * (n + 1) / 2;
@@ -116,22 +120,34 @@ __global__ void symmetrize_kernel(double *M, int n)
     while ((int64_t)(i + 1) * (i + 2) / 2 <= t) ++i;
     int j = (int)(t - (int64_t)i * (i + 1) / 2);
     double s = M[(int64_t)i * n + j] + M[(int64_t)j * n + i];
+    if (S) s *= S[(int64_t)i * n + j];
     M[(int64_t)i * n + j] = s;
     M[(int64_t)j * n + i] = s;
 }
 
 // Batched form: one CUDA block per molecule block of a block-diagonal layout.
-__global__ void symmetrize_blocks_kernel(double *M, const long long *__restrict__ off, const int *__restrict__ nm)
+__global__ void symmetrize_blocks_kernel(double *M, const long long *__restrict__ off, const int *__restrict__ nm,
+                                         const double *__restrict__ S)
 {
     const int m = blockIdx.x, n = nm[m];
     double *B = M + off[m];
+    const double *SB = S ? S + off[m] : nullptr;
     for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
         const int i = t / n, j = t - i * n;
         if (j > i) continue;
-        const double s = B[(int64_t)i * n + j] + B[(int64_t)j * n + i];
+        double s = B[(int64_t)i * n + j] + B[(int64_t)j * n + i];
+        if (SB) s *= SB[(int64_t)i * n + j];
         B[(int64_t)i * n + j] = s;
         B[(int64_t)j * n + i] = s;
     }
+}
+
+// Y = X * S element-wise (the pre-scaled density of the direct J/K kernels).
+__global__ void scale_elements_kernel(const double *__restrict__ X, const double *__restrict__ S, double *__restrict__ Y,
+                                      int64_t len)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < len; t += (int64_t)gridDim.x * blockDim.x)
+        Y[t] = X[t] * S[t];
 }
 
 __device__ __forceinline__ double binom_d(int n, int k)
@@ -771,7 +787,19 @@ __global__ void rys_eval_kernel(int nr, int count, const double *T, double *u, d
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
-    for (int r = 0; r < nr; ++r) rys_root(nr, r, T[t], u[(int64_t)t * nr + r], w[(int64_t)t * nr + r]);
+    double uu[5], ww[5];
+    // the same evaluation the Fock-build kernels use (moments for 1-2 roots, tables above)
+    switch (nr) {
+    case 1: rys_roots_fast<1>(T[t], uu, ww); break;
+    case 2: rys_roots_fast<2>(T[t], uu, ww); break;
+    case 3: rys_roots_fast<3>(T[t], uu, ww); break;
+    case 4: rys_roots_fast<4>(T[t], uu, ww); break;
+    default: rys_roots_fast<5>(T[t], uu, ww); break;
+    }
+    for (int r = 0; r < nr; ++r) {
+        u[(int64_t)t * nr + r] = uu[r];
+        w[(int64_t)t * nr + r] = ww[r];
+    }
 }
 
 // FP64 FMA probe: 8 independent chains per thread keep the DFMA pipe full.
@@ -845,6 +873,10 @@ static void release_basis(pqb_ctx *ctx)
     free_dev(ctx->d_pairs);
     free_dev(ctx->d_prims);
     free_dev(ctx->d_fscale);
+    free_dev(ctx->d_escale);
+    free_dev(ctx->d_Dscaled);
+    ctx->d_escale = nullptr;
+    ctx->d_Dscaled = nullptr;
     free_dev(ctx->d_q2);
     free_dev(ctx->d_full);
     free_dev(ctx->d_diag);
@@ -1002,6 +1034,7 @@ int pqb_shells_upload_batch(pqb_ctx *ctx, int nmol, const int *mol_shell_off, in
                     if (fabs(prim_coef[p] * prim_coef[q]) * e * pow(kPi / z, 1.5) < 1e-20) continue;
                     PrimPair pp{};
                     pp.zeta = z;
+                    pp.izeta = 1.0 / z;
                     for (int x = 0; x < 3; ++x) pp.P[x] = (al * A[x] + be * B[x]) / z;
                     pp.K = prim_coef[p] * prim_coef[q] * kPairPre / z * e;
                     pp.alpha_a = al;
@@ -1040,6 +1073,17 @@ int pqb_shells_upload_batch(pqb_ctx *ctx, int nmol, const int *mol_shell_off, in
     PQB_CK(ctx, cudaMemcpy(ctx->d_pairs, pairs.data(), sizeof(PairInfo) * np, cudaMemcpyHostToDevice));
     PQB_CK(ctx, cudaMemcpy(ctx->d_prims, prims.data(), sizeof(PrimPair) * prims.size(), cudaMemcpyHostToDevice));
     PQB_CK(ctx, cudaMemcpy(ctx->d_fscale, fscale, sizeof(double) * nbf, cudaMemcpyHostToDevice));
+    {
+        std::vector<double> es((size_t)ctx->dense_len);
+        for (int m = 0; m < nmol; ++m) {
+            const int f0 = ctx->mol_f0[m], n = ctx->mol_n[m];
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j) es[(size_t)ctx->mol_off[m] + (size_t)i * n + j] = fscale[f0 + i] * fscale[f0 + j];
+        }
+        PQB_CK(ctx, cudaMalloc(&ctx->d_escale, sizeof(double) * std::max<size_t>(es.size(), 1)));
+        PQB_CK(ctx, cudaMalloc(&ctx->d_Dscaled, sizeof(double) * std::max<size_t>(es.size(), 1)));
+        PQB_CK(ctx, cudaMemcpy(ctx->d_escale, es.data(), sizeof(double) * es.size(), cudaMemcpyHostToDevice));
+    }
     // unscreened quartet list (packed integrals) and diagonal list (Schwarz)
     std::vector<std::vector<int4>> dcls(kNumQuartetClass);
     for (int p = 0; p < np; ++p)
@@ -1291,6 +1335,8 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
     const int n = ctx->nbf;
     PQB_CK(ctx, cudaMemsetAsync(J, 0, sizeof(double) * ctx->dense_len, st));
     PQB_CK(ctx, cudaMemsetAsync(K, 0, sizeof(double) * ctx->dense_len, st));
+    scale_elements_kernel<<<ctx->nsm * 4, 256, 0, st>>>(D, ctx->d_escale, ctx->d_Dscaled, ctx->dense_len);
+    const double *Ds = ctx->d_Dscaled;
     PQB_CK(ctx, ensure_streams(ctx));
     // fork: class launches spread over the context's streams, heaviest first
     PQB_CK(ctx, cudaEventRecord(ctx->ev_fork, st));
@@ -1313,9 +1359,9 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
         cudaStream_t sk = ctx->streams[k++ % ctx->nstreams];
         const int4 *list = ctx->d_plan + ctx->plan_off[part][c];
         if (part == 1 && mode == PQB_MIXED)
-            PQB_CK(ctx, launch_jk_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, D, J, K, ctx->d_fscale, n, sk, ctx->nsm));
+            PQB_CK(ctx, launch_jk_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, J, K, n, sk, ctx->nsm));
         else
-            PQB_CK(ctx, launch_jk_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, D, J, K, ctx->d_fscale, n, sk, ctx->nsm));
+            PQB_CK(ctx, launch_jk_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, J, K, n, sk, ctx->nsm));
     }
     // join
     for (int k = 0; k < pqb_ctx::kStreams; ++k) {
@@ -1324,11 +1370,11 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
     }
     if (ctx->nmol == 1) {
         const int64_t P = (int64_t)n * (n + 1) / 2;
-        symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, n);
-        symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K, n);
+        symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, n, ctx->d_escale);
+        symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K, n, ctx->d_escale);
     } else {
-        symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(J, ctx->d_mol_off, ctx->d_mol_n);
-        symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(K, ctx->d_mol_off, ctx->d_mol_n);
+        symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(J, ctx->d_mol_off, ctx->d_mol_n, ctx->d_escale);
+        symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(K, ctx->d_mol_off, ctx->d_mol_n, ctx->d_escale);
     }
     PQB_CK(ctx, cudaGetLastError());
     return PQB_OK;
@@ -1351,11 +1397,12 @@ int pqb_jk_direct_class(pqb_ctx *ctx, const double *D, double *Jacc, double *Kac
     cudaStream_t st = (cudaStream_t)stream;
     const int4 *list = ctx->d_plan + ctx->plan_off[part][qclass];
     const int nq = (int)ctx->plan_cnt[part][qclass];
+    scale_elements_kernel<<<ctx->nsm * 4, 256, 0, st>>>(D, ctx->d_escale, ctx->d_Dscaled, ctx->dense_len);
     if (mode == PQB_MIXED && part == 1)
-        PQB_CK(ctx, launch_jk_f32(qclass, list, nq, ctx->d_pairs, ctx->d_prims, D, Jacc, Kacc, ctx->d_fscale, ctx->nbf,
+        PQB_CK(ctx, launch_jk_f32(qclass, list, nq, ctx->d_pairs, ctx->d_prims, ctx->d_Dscaled, Jacc, Kacc, ctx->nbf,
                                   st, ctx->nsm));
     else
-        PQB_CK(ctx, launch_jk_f64(qclass, list, nq, ctx->d_pairs, ctx->d_prims, D, Jacc, Kacc, ctx->d_fscale, ctx->nbf,
+        PQB_CK(ctx, launch_jk_f64(qclass, list, nq, ctx->d_pairs, ctx->d_prims, ctx->d_Dscaled, Jacc, Kacc, ctx->nbf,
                                   st, ctx->nsm));
     return PQB_OK;
 }
@@ -1394,8 +1441,8 @@ int pqb_jk_packed(pqb_ctx *ctx, const double *ints, int64_t len, const double *D
     } else {
         jk_packed_kernel<<<(unsigned)P, 256, 0, st>>>(ints, D, J, K, nbf);
     }
-    symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, nbf);
-    symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K, nbf);
+    symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, nbf, nullptr);
+    symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K, nbf, nullptr);
     PQB_CK(ctx, cudaGetLastError());
     return PQB_OK;
 }

@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "pqb_types.h"
+
 #ifndef PQB_TABQ
 #define PQB_TABQ static __device__ const
 #endif
@@ -22,6 +24,36 @@ constexpr double kPi = 3.14159265358979323846;
 // sqrt(2) * pi^(5/4): K_ab = sqrt(2) pi^(5/4)/zeta exp(-mu R^2) so that
 // K_ab K_cd / sqrt(zeta+eta) = 2 pi^(5/2)/(zeta eta sqrt(zeta+eta)) exp(...)
 constexpr double kPairPre = 5.9149671727956128778;
+
+// ---------------------------------------------- reciprocal and 1/sqrt --
+// Newton--Raphson from the single-precision hardware estimates
+// (rcp.approx.ftz.f32 and rsqrt.approx.ftz.f32, relative error < 2^-22):
+// one third-order step each.  For 1/x with e = 1 - x r:
+//   r' = r (1 + e + e^2)                     (remaining error ~ e^3 ~ 2^-66);
+// for 1/sqrt(x) with e = 1 - x y^2:
+//   y' = y (1 + e/2 + 3 e^2/8)               (remaining error ~ 5 e^3/16).
+// Both end within a couple of ulps of the exact value.  x must be positive
+// and inside single-precision range (about 1e-37 .. 1e37); every caller here
+// passes exponent sums, Boys values or Rys discriminants, which are.
+__device__ __forceinline__ double rcp_nr(double x)
+{
+    const float xf = (float)x;
+    float rf;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rf) : "f"(xf));
+    const double r = (double)rf;
+    const double e = fma(-x, r, 1.0);
+    return fma(r, fma(e, e, e), r);
+}
+
+__device__ __forceinline__ double rsqrt_nr(double x)
+{
+    const float xf = (float)x;
+    float yf;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
+    const double y = (double)yf;
+    const double e = fma(-x * y, y, 1.0);
+    return fma(y * e, fma(e, 0.375, 0.5), y);
+}
 
 __host__ __device__ constexpr int ncart(int L) { return (L + 1) * (L + 2) / 2; }
 // x / y / z exponent of cartesian component i of a shell of angular momentum L,
@@ -137,6 +169,66 @@ __device__ __forceinline__ void rys_roots(double T, double *u, double *w)
     }
 }
 
+// All NR roots at T for the integral kernels.  NR = 1 and NR = 2 come from
+// one Boys-table row: the n-point rule is the Gauss rule of the moments
+// F_0..F_(2n-1)(T) (sum_r w_r u_r^k = F_k), so
+//   n = 1:  u = F1/F0, w = F0;
+//   n = 2:  the monic orthogonal polynomial u^2 + a1 u + a0 solves
+//           F2 + a1 F1 + a0 F0 = 0, F3 + a1 F2 + a0 F1 = 0; its larger root
+//           u_b = (-a1 + s)/2 (s^2 = a1^2 - 4 a0), the smaller u_s = a0/u_b,
+//           and w_s = (u_b F0 - F1)/s, w_b = F0 - w_s.
+// This 2x2 moment problem is well conditioned for every T (checked against
+// 40-digit Golub--Welsch rules: 3e-15 relative), and costs one table row and
+// an exp instead of 4 Chebyshev series.  NR >= 3 uses the tables.
+template <int NR>
+__device__ __forceinline__ void rys_roots_fast(double T, double *u, double *w)
+{
+    if constexpr (NR == 1) {
+        double F[2];
+        boys<1>(T, F);
+        w[0] = F[0];
+        u[0] = F[1] * rcp_nr(F[0]);
+    } else if constexpr (NR == 2) {
+        double F[4];
+        boys<3>(T, F);
+        const double id = rcp_nr(fma(F[0], F[2], -F[1] * F[1]));
+        const double a1 = fma(F[1], F[2], -F[0] * F[3]) * id;
+        const double a0 = fma(F[1], F[3], -F[2] * F[2]) * id;
+        const double disc = fma(a1, a1, -4.0 * a0);
+        const double rs = rsqrt_nr(disc);
+        const double ub = 0.5 * fma(disc, rs, -a1);
+        u[0] = a0 * rcp_nr(ub);
+        u[1] = ub;
+        w[0] = fma(ub, F[0], -F[1]) * rs;
+        w[1] = F[0] - w[0];
+    } else {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) rys_root(NR, r, T, u[r], w[r]);
+    }
+}
+
+// Per-root coefficients of the 2-D recurrence (no divisions: izeta, ieta and
+// izpe = 1/(zeta+eta) come precomputed):
+//   b00 = u/(2(zeta+eta)),  b10 = (1 - eta u/(zeta+eta))/(2 zeta),
+//   b01 = (1 - zeta u/(zeta+eta))/(2 eta),
+//   c00 = PA - ce PQ, c01 = QC + cz PQ with ce = eta u/(zeta+eta), cz = zeta u/(zeta+eta).
+struct RysCoef {
+    double b00, b10, b01, ce, cz;
+};
+
+__device__ __forceinline__ RysCoef rys_coef(double u, double zeta, double eta, double izeta, double ieta,
+                                            double izpe)
+{
+    const double ue = u * izpe;
+    RysCoef k;
+    k.b00 = 0.5 * ue;
+    k.ce = eta * ue;
+    k.cz = zeta * ue;
+    k.b10 = 0.5 * izeta * (1.0 - k.ce);
+    k.b01 = 0.5 * ieta * (1.0 - k.cz);
+    return k;
+}
+
 // ------------------------------------------------ 2-D Rys integrals (one axis)
 // For one root u and one cartesian axis: G(n,m) = I_x(n,0|m,0) by the Rys
 // recurrence (bra exponent sum zeta, ket eta), then the horizontal transfer
@@ -146,16 +238,13 @@ __device__ __forceinline__ void rys_roots(double T, double *u, double *w)
 // prefactor goes on one axis).  All sizes are compile-time: fully unrolled,
 // register resident.
 template <int LA, int LB, int LC, int LD, typename R>
-__device__ __forceinline__ void rys2d(double u, double zeta, double eta, double PA, double QC, double PQ,
-                                      double AB, double CD, double scale, R *out)
+__device__ __forceinline__ void rys2d_c(const RysCoef &k, double PA, double QC, double PQ, double AB, double CD,
+                                        double scale, R *out)
 {
     constexpr int NB = LA + LB, MK = LC + LD;
-    const double zpe = zeta + eta;
-    const double b00 = 0.5 * u / zpe;
-    const double b10 = (0.5 - 0.5 * eta / zpe * u) / zeta;
-    const double b01 = (0.5 - 0.5 * zeta / zpe * u) / eta;
-    const double c00 = PA - eta / zpe * u * PQ;
-    const double c01 = QC + zeta / zpe * u * PQ;
+    const double b00 = k.b00, b10 = k.b10, b01 = k.b01;
+    const double c00 = fma(-k.ce, PQ, PA);
+    const double c01 = fma(k.cz, PQ, QC);
     R g[NB + 1][MK + 1];
     g[0][0] = (R)scale;
     if (NB > 0) g[1][0] = (R)(c00 * scale);
@@ -202,6 +291,41 @@ __device__ __forceinline__ void rys2d(double u, double zeta, double eta, double 
 #pragma unroll
                 for (int b = 0; b <= LB; ++b) out[((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d] = t[a][b];
         }
+}
+
+// The same from (u, zeta, eta) with the divisions done here (general and
+// gradient kernels, which are not on the Fock-build path).
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void rys2d(double u, double zeta, double eta, double PA, double QC, double PQ,
+                                      double AB, double CD, double scale, R *out)
+{
+    const double zpe = zeta + eta;
+    RysCoef k;
+    k.b00 = 0.5 * u / zpe;
+    k.b10 = (0.5 - 0.5 * eta / zpe * u) / zeta;
+    k.b01 = (0.5 - 0.5 * zeta / zpe * u) / eta;
+    k.ce = eta / zpe * u;
+    k.cz = zeta / zpe * u;
+    rys2d_c<LA, LB, LC, LD, R>(k, PA, QC, PQ, AB, CD, scale, out);
+}
+
+// The Fock-build fields of a PrimPair (zeta, 1/zeta, P, K) in three 128-bit loads.
+struct PrimJK {
+    double zeta, izeta, P[3], K;
+};
+
+__device__ __forceinline__ PrimJK load_prim_jk(const PrimPair *p)
+{
+    const double2 *v = reinterpret_cast<const double2 *>(p);
+    const double2 a = __ldg(v), b = __ldg(v + 1), c = __ldg(v + 2);
+    PrimJK r;
+    r.zeta = a.x;
+    r.izeta = a.y;
+    r.P[0] = b.x;
+    r.P[1] = b.y;
+    r.P[2] = c.x;
+    r.K = c.y;
+    return r;
 }
 
 }  // namespace pqb

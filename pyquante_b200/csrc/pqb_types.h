@@ -27,11 +27,14 @@ struct PairInfo {
                        // (global function indices; 0 for a single molecule)
 };
 
-struct PrimPair {
+// 64 bytes, 16-byte aligned: the kernels fetch one with four 128-bit loads.
+struct __align__(16) PrimPair {
     double zeta;       // alpha_a + alpha_b
+    double izeta;      // 1 / zeta (the recurrences multiply; no division per quartet)
     double P[3];       // Gaussian product centre
     double K;          // c_a c_b sqrt(2) pi^(5/4)/zeta exp(-alpha_a alpha_b/zeta |AB|^2)
     double alpha_a;    // exponent of the first shell's primitive (alpha_b = zeta - alpha_a)
+    double pad_;
 };
 
 __host__ __device__ inline int pair_class(int la, int lb)   // la >= lb
