@@ -2,7 +2,8 @@
 
 Writes ``rys_tables.inc`` next to this file.  Run once (takes ~1 min):
 
-    python -m pyquante_b200.csrc.gen_tables
+    python -m pyquante_b200.csrc.gen_tables              # rys_tables.inc
+    python -m pyquante_b200.csrc.gen_tables --boys-rows  # boys_rows.inc
 
 Two tables are produced, both from 40-digit mpmath arithmetic:
 
@@ -199,5 +200,39 @@ def main():
     print("worst relative error:", worst)
 
 
+# Compact Boys rows for the 1- and 2-root Fock-build kernels: for each order
+# M in BOYSROW_ORDERS and grid point T_k = k/32 (k = 0..BOYSROW_NGRID-1) one
+# 64-byte row [F_M(T_k), ..., F_{M+6}(T_k), exp(-T_k)], so a lane fetches
+# everything for F_M(T) (7-term Taylor, |T - T_k| <= 1/64) and exp(-T)
+# with two 256-bit loads.
+BOYSROW_STEP_INV = 32
+BOYSROW_ORDERS = (1, 3)
+BOYSROW_NGRID = int(BOYS_TMAX * BOYSROW_STEP_INV) + 2
+
+
+def main_boys_rows():
+    here = os.path.dirname(os.path.abspath(__file__))
+    lines = ["// Generated by gen_tables.py --boys-rows -- do not edit.",
+             "// Row k of pqb_boys_rowM: F_M(T_k) .. F_(M+6)(T_k), exp(-T_k) at T_k = k/%d (40-digit mpmath)."
+             % BOYSROW_STEP_INV,
+             "#pragma once",
+             "#define PQB_BOYSROW_STEP_INV %d" % BOYSROW_STEP_INV,
+             "#define PQB_BOYSROW_NGRID %d" % BOYSROW_NGRID,
+             "#define PQB_BOYSROW_TMAX %.1f" % BOYS_TMAX]
+    for M in BOYSROW_ORDERS:
+        lines.append("PQB_TABQ __align__(64) double pqb_boys_row%d[PQB_BOYSROW_NGRID * 8] = {" % M)
+        for k in range(BOYSROW_NGRID):
+            T = mp.mpf(k) / BOYSROW_STEP_INV
+            row = [boys(M + j, T) for j in range(7)] + [mp.exp(-T)]
+            lines.append("  " + ", ".join("%.17e" % float(v) for v in row) + ",")
+        lines.append("};")
+    with open(os.path.join(here, "boys_rows.inc"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
 if __name__ == "__main__":
-    main()
+    import sys
+    if "--boys-rows" in sys.argv:
+        main_boys_rows()
+    else:
+        main()

@@ -17,6 +17,7 @@
 #define PQB_CTABQ static __constant__ const
 #endif
 #include "rys_tables.inc"
+#include "boys_rows.inc"
 
 namespace pqb {
 
@@ -123,6 +124,50 @@ __device__ __forceinline__ void boys_rt(int M, double T, double *F)
     }
 }
 
+// Four doubles from 32-byte aligned global memory with one 256-bit load.
+__device__ __forceinline__ void ld4(const double *p, double &a, double &b, double &c, double &d)
+{
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(a), "=d"(b), "=d"(c), "=d"(d)
+        : "l"(__cvta_generic_to_global(p)));
+}
+
+// F_m(T), m = 0..M for M = 1 or 3, from one 64-byte row of pqb_boys_rowM
+// (boys_rows.inc: F_M .. F_(M+6) and exp(-T_k) at T_k = k/32): F_M by a
+// 7-term Taylor series about the nearest T_k (|T - T_k| <= 1/64, remainder
+// below 5e-17 F_M), exp(-T) = exp(-T_k) exp(-(T - T_k)) with an 8-term
+// series, then the downward recursion F_m = (2T F_(m+1) + exp(-T))/(2m+1).
+// T >= PQB_BOYSROW_TMAX uses the large-T forms of boys<M>.
+template <int M>
+__device__ __forceinline__ void boys_row(double T, double *F)
+{
+    static_assert(M == 1 || M == 3, "rows exist for M = 1 and 3");
+    if (T < PQB_BOYSROW_TMAX) {
+        const int k = __double2int_rn(T * PQB_BOYSROW_STEP_INV);
+        const double d = k * (1.0 / PQB_BOYSROW_STEP_INV) - T;   // -(T - T_k)
+        const double *row = (M == 1 ? pqb_boys_row1 : pqb_boys_row3) + 8 * k;
+        double r[8];
+        ld4(row, r[0], r[1], r[2], r[3]);
+        ld4(row + 4, r[4], r[5], r[6], r[7]);
+        double f = r[6];
+#pragma unroll
+        for (int j = 5; j >= 0; --j) f = fma(f, d * (1.0 / (j + 1)), r[j]);
+        F[M] = f;
+        double ed = 1.0;
+#pragma unroll
+        for (int j = 8; j >= 1; --j) ed = fma(ed, d * (1.0 / j), 1.0);
+        const double e = r[7] * ed, t2 = 2.0 * T;
+#pragma unroll
+        for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * (1.0 / (2 * m + 1));
+    } else {
+        const double it = rcp_nr(T);
+        F[0] = 0.88622692545275801365 * rsqrt_nr(T);   // sqrt(pi)/2 / sqrt(T)
+        const double e = exp(-T), h = 0.5 * it;
+#pragma unroll
+        for (int m = 0; m < M; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+    }
+}
+
 // ------------------------------------------------------------------- Rys --
 __device__ __forceinline__ double clenshaw14(const double *c, double x)
 {
@@ -170,7 +215,7 @@ __device__ __forceinline__ void rys_roots(double T, double *u, double *w)
 }
 
 // All NR roots at T for the integral kernels.  NR = 1 and NR = 2 come from
-// one Boys-table row: the n-point rule is the Gauss rule of the moments
+// one compact Boys row (boys_row): the n-point rule is the Gauss rule of the moments
 // F_0..F_(2n-1)(T) (sum_r w_r u_r^k = F_k), so
 //   n = 1:  u = F1/F0, w = F0;
 //   n = 2:  the monic orthogonal polynomial u^2 + a1 u + a0 solves
@@ -185,12 +230,12 @@ __device__ __forceinline__ void rys_roots_fast(double T, double *u, double *w)
 {
     if constexpr (NR == 1) {
         double F[2];
-        boys<1>(T, F);
+        boys_row<1>(T, F);
         w[0] = F[0];
         u[0] = F[1] * rcp_nr(F[0]);
     } else if constexpr (NR == 2) {
         double F[4];
-        boys<3>(T, F);
+        boys_row<3>(T, F);
         const double id = rcp_nr(fma(F[0], F[2], -F[1] * F[1]));
         const double a1 = fma(F[1], F[2], -F[0] * F[3]) * id;
         const double a0 = fma(F[1], F[3], -F[2] * F[2]) * id;
@@ -309,20 +354,17 @@ __device__ __forceinline__ void rys2d(double u, double zeta, double eta, double 
     rys2d_c<LA, LB, LC, LD, R>(k, PA, QC, PQ, AB, CD, scale, out);
 }
 
-// The Fock-build fields of a PrimPair (zeta, 1/zeta, P, K) in three 128-bit loads.
+// The Fock-build fields of a PrimPair (zeta, 1/zeta, P, K): one 256-bit and
+// one 128-bit load.
 struct PrimJK {
     double zeta, izeta, P[3], K;
 };
 
 __device__ __forceinline__ PrimJK load_prim_jk(const PrimPair *p)
 {
-    const double2 *v = reinterpret_cast<const double2 *>(p);
-    const double2 a = __ldg(v), b = __ldg(v + 1), c = __ldg(v + 2);
     PrimJK r;
-    r.zeta = a.x;
-    r.izeta = a.y;
-    r.P[0] = b.x;
-    r.P[1] = b.y;
+    ld4(reinterpret_cast<const double *>(p), r.zeta, r.izeta, r.P[0], r.P[1]);
+    const double2 c = __ldg(reinterpret_cast<const double2 *>(p) + 2);
     r.P[2] = c.x;
     r.K = c.y;
     return r;

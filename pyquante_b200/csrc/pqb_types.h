@@ -27,8 +27,9 @@ struct PairInfo {
                        // (global function indices; 0 for a single molecule)
 };
 
-// 64 bytes, 16-byte aligned: the kernels fetch one with four 128-bit loads.
-struct __align__(16) PrimPair {
+// 64 bytes, 32-byte aligned: the kernels fetch the Fock-build fields with one
+// 256-bit and one 128-bit load.
+struct __align__(32) PrimPair {
     double zeta;       // alpha_a + alpha_b
     double izeta;      // 1 / zeta (the recurrences multiply; no division per quartet)
     double P[3];       // Gaussian product centre
