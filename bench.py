@@ -205,8 +205,11 @@ def run_stored(a):
     n = len(bs)
     eng = BasisEngine(bs.bfs)
     ints = eng.eri_packed()
-    S, h = Ints.get1ints(bs, mol)
-    D = torch.eye(n, dtype=torch.float64, device="cuda") * 0.05
+    # a dense symmetric density of the cluster's rank (seeded), so every
+    # J/K contribution is nonzero and takes its atomics
+    nocc = mol.get_nel() // 2
+    C = np.linalg.qr(np.random.default_rng(0).standard_normal((n, nocc)))[0]
+    D = torch.as_tensor(C @ C.T, device="cuda")
     for _ in range(a.warmup):
         jk_packed(ints, D, eng.ctx)
     torch.cuda.synchronize()

@@ -96,8 +96,11 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
  * qclass (0..20, or -1 for all; effective at the next pqb_plan);
  * PQB_PARAM_STREAMS = streams the class launches are spread over (1..16);
  * PQB_PARAM_ORDER = class launch order (0 by estimated cost, 1 highest
- * angular momentum first, the default). */
-enum { PQB_PARAM_CHUNK = 0, PQB_PARAM_STREAMS = 1, PQB_PARAM_ORDER = 2 };
+ * angular momentum first, the default); PQB_PARAM_PACKED_KERNEL = the
+ * stored-integral J/K kernel of pqb_jk_packed (0 automatic: the register
+ * form for nbf <= 512, one block per packed row above; 1 always the latter,
+ * so tests can compare the two). */
+enum { PQB_PARAM_CHUNK = 0, PQB_PARAM_STREAMS = 1, PQB_PARAM_ORDER = 2, PQB_PARAM_PACKED_KERNEL = 3 };
 int pqb_set_param(pqb_ctx *ctx, int param, int qclass, int value);
 
 /* Per-class statistics of the current plan, arrays of 2*21 int64 indexed

@@ -27,7 +27,8 @@ Rys roots and weights
     for T < RYS_TASYM[n]; above that the large-T limit is used:
     u_i = s_i/T, w_i = W_i/sqrt(T) with (s_i, 2 W_i) the generalised
     Gauss--Laguerre (alpha = -1/2) nodes and weights.  RYS_TASYM[n] is where
-    that limit is exact to < 2e-15 relative.
+    that limit is exact to < 2e-15 relative.  The table stores, per (n,
+    interval, root), the 14 coefficient pairs (root_k, weight_k) interleaved.
 
 This replaces the GAMESS piecewise fits in the reference's Src/crys.c:99-1438
 (Roots/Root123/Root4/Root5) with tables of this project's own construction.
@@ -185,11 +186,14 @@ def main():
     for n in range(1, RYS_NMAX + 1):
         lines.append("  {" + ", ".join("%.17e" % float(w) for w in asym[n][1]) + "},")
     lines.append("};")
-    lines.append("PQB_TABQ double pqb_rys_coef[PQB_RYS_TABLE_SIZE] = {")
+    # per (n, interval, root): the 14 (root, weight) coefficient pairs
+    # interleaved, 224 bytes, so a lane reads both series with 256-bit loads
+    lines.append("PQB_TABQ __align__(64) double pqb_rys_coef[PQB_RYS_TABLE_SIZE] = {")
     for n in range(1, RYS_NMAX + 1):
         for iv, funcs in enumerate(rys[n]):
-            for fc in funcs:
-                lines.append("  " + ", ".join("%.17e" % c for c in fc) + ",")
+            for r in range(n):
+                cu, cw = funcs[2 * r], funcs[2 * r + 1]
+                lines.append("  " + ", ".join("%.17e, %.17e" % (a, b) for a, b in zip(cu, cw)) + ",")
     lines.append("};")
     lines.append("PQB_TABQ double pqb_boys_tab[PQB_BOYS_NGRID * PQB_BOYS_NORD] = {")
     for row in boys_tab:

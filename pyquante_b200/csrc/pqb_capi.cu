@@ -61,6 +61,7 @@ struct pqb_ctx {
     int *d_shell_atom = nullptr;     // atom index of every shell (gradients)
     int2 *d_pk_tiles = nullptr;      // (i, j0) tiles of the stored-integral J/K kernel
     int pk_tiles_n = 0, pk_tiles_nbf = -1;
+    bool packed_simple = false;      // force the one-block-per-row stored J/K kernel (tests)
     // batched bases: molecules own consecutive shells/functions; D/J/K hold
     // one dense nm x nm block per molecule, back to back
     int nmol = 1;
@@ -643,132 +644,179 @@ __global__ void jk_packed_kernel(const double *__restrict__ ints, const double *
     }
 }
 
-// ---- tiled stored-integral J/K (the HBM-bound path).  A CTA owns the
-// packed rows IJ = (i, j) for j in [j0, j0+32) of one i and streams them once
-// (coalesced, 32 consecutive KL per warp instruction).  With v' the
-// degeneracy-weighted integral, the EpiJK updates become:
-//   Jacc[i,j] += 2 v' D_kl   row sums, one atomic per row
-//   Jacc[k,l] += 2 v' D_ij   summed over the CTA's rows per 32-column chunk
-//   Kacc[i,k], Kacc[i,l]     into a shared row Ki (same i for the whole CTA)
-//   Kacc[j,k], Kacc[j,l]     into shared rows Kj[j - j0]
-// Lanes of a chunk that share k form contiguous runs; k-indexed sums are
-// reduced over each run with shuffles before one shared add.  (A variant
-// with one warp per column range and per-element shared adds of Kacc[j,l]
-// measured slower: FP64 shared-memory atomics dominate it.)
-constexpr int kPkRows = 32, kPkWarps = 8;
+// ---- stored-integral J/K, register form (the HBM-bound path for
+// nbf <= 32 * MAXM).  A CTA owns the packed rows IJ = (i, j), j in
+// [j0, j0 + 16), of one i; warp w owns rows j0 + w and j0 + w + 8.  The
+// warps walk the columns KL = (k, l) segment by segment (k fixed, lane
+// owns l = lane + 32 m), reading every integral once with coalesced loads.
+// With v' the degeneracy-weighted integral:
+//   Jacc[i,j] += 2 v' D_kl   per-row register sums
+//   Jacc[k,l] += 2 v' D_ij   per-warp partials in shared memory, summed
+//                            over the CTA's rows once per segment
+//   Kacc[i,l] += v' D_jk     register row accI[m] (lane-owned columns)
+//   Kacc[i,k] += v' D_jl     warp sum per segment, added to column k of accI
+//   Kacc[j,l] += v' D_ik     register rows accJ[q][m]
+//   Kacc[j,k] += v' D_il     warp sum per segment, added to column k of accJ
+// The register rows go to Kacc once per CTA (accI summed over the warps).
+constexpr int kRgWarps = 8, kRgRPW = 2, kRgRows = kRgWarps * kRgRPW, kRgPrefetch = 2;
 
-__device__ __forceinline__ double run_sum(double x, int key, int lane)
+__device__ __forceinline__ double warp_sum(double x)
 {
-    // inclusive segmented scan over runs of equal `key` (contiguous lanes)
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const double y = __shfl_up_sync(0xffffffffu, x, o);
-        const int ky = __shfl_up_sync(0xffffffffu, key, o);
-        if (lane >= o && ky == key) x += y;
-    }
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     return x;
 }
 
-__global__ void __launch_bounds__(kPkWarps * 32) jk_packed_tiled_kernel(const double *__restrict__ ints,
-                                                                        const double *__restrict__ D, double *Jacc,
-                                                                        double *Kacc, int n,
-                                                                        const int2 *__restrict__ tiles, int ntiles)
+// L2 prefetch of the 16-byte aligned interior of [p, p + len) (a hint: no
+// data returns to the SM; the range lies inside the packed array).
+__device__ __forceinline__ void prefetch_l2(const double *p, int len)
 {
-    extern __shared__ double smem[];
-    double *Ki = smem;                          // [n]
-    double *Kj = smem + n;                      // [kPkRows][n]
-    double *jc = smem + n + kPkRows * n;        // [kPkWarps][32]
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uintptr_t a = ((uintptr_t)p + 15) & ~(uintptr_t)15, b = ((uintptr_t)(p + len)) & ~(uintptr_t)15;
+    if (b > a)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(__cvta_generic_to_global((const void *)a)),
+                     "r"((unsigned)(b - a))
+                     : "memory");
+}
+
+template <int MAXM>
+__global__ void __launch_bounds__(kRgWarps * 32) jk_packed_reg_kernel(const double *__restrict__ ints,
+                                                                      const double *__restrict__ D, double *Jacc,
+                                                                      double *Kacc, int n,
+                                                                      const int2 *__restrict__ tiles, int ntiles)
+{
+    // column partials of a segment, double-buffered: jc[2][kRgWarps][MAXM * 32];
+    // per-warp rows i, summed at the end: kis[kRgWarps][MAXM * 32]
+    extern __shared__ double rg_smem[];
+    double(*jc)[kRgWarps][MAXM * 32] = reinterpret_cast<double(*)[kRgWarps][MAXM * 32]>(rg_smem);
+    double(*kis)[MAXM * 32] = reinterpret_cast<double(*)[MAXM * 32]>(rg_smem + 2 * kRgWarps * MAXM * 32);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int i = tiles[t].x, j0 = tiles[t].y;
-        const int nrows = min(kPkRows, i + 1 - j0);
-        for (int x = tid; x < n + kPkRows * n; x += blockDim.x) smem[x] = 0.0;
-        __syncthreads();
         const int64_t I0 = (int64_t)i * (i + 1) / 2;
-        const int64_t KLmax = I0 + j0 + nrows - 1;
         const double *Di = D + (int64_t)i * n;
-        double jrow[kPkRows / kPkWarps], vnext[kPkRows / kPkWarps];
+        const double *rowp[kRgRPW], *Djp[kRgRPW];
+        int jq[kRgRPW];
+        bool okq[kRgRPW];
+        double Dij2[kRgRPW], wq[kRgRPW], jrow[kRgRPW], accJ[kRgRPW][MAXM], accI[MAXM];
 #pragma unroll
-        for (int q = 0; q < kPkRows / kPkWarps; ++q) jrow[q] = 0.0;
-        // the integrals of the next chunk are loaded while this one is digested
-        auto load_chunk = [&](int64_t c, double *v) {
-            const int64_t kl = c + lane;
+        for (int q = 0; q < kRgRPW; ++q) {
+            const int j = j0 + warp + kRgWarps * q;
+            okq[q] = j <= i;
+            jq[q] = okq[q] ? j : i;
+            const int64_t IJ = I0 + jq[q];
+            rowp[q] = ints + IJ * (IJ + 1) / 2;
+            Djp[q] = D + (int64_t)jq[q] * n;
+            Dij2[q] = okq[q] ? 2.0 * __ldg(Di + jq[q]) : 0.0;
+            wq[q] = okq[q] ? (i == jq[q] ? 0.5 : 1.0) : 0.0;   // rows past i contribute nothing
+            jrow[q] = 0.0;
 #pragma unroll
-            for (int q = 0; q < kPkRows / kPkWarps; ++q) {
-                const int r = warp + kPkWarps * q;
-                const int64_t IJ = I0 + j0 + r;
-                v[q] = (r < nrows && kl <= KLmax && kl <= IJ) ? __ldg(ints + IJ * (IJ + 1) / 2 + kl) : 0.0;
+            for (int m = 0; m < MAXM; ++m) accJ[q][m] = 0.0;
+        }
+#pragma unroll
+        for (int m = 0; m < MAXM; ++m) accI[m] = 0.0;
+        int buf = 0;
+        // the first kRgPrefetch segments of the warp's rows are requested from L2 up front
+        if (lane < kRgRPW) {
+            const double *rp = lane == 0 ? rowp[0] : rowp[kRgRPW - 1];
+            const bool okr = lane == 0 ? okq[0] : okq[kRgRPW - 1];
+            const int jr = lane == 0 ? jq[0] : jq[kRgRPW - 1];
+            for (int kk = 0; kk < kRgPrefetch && kk <= i && okr; ++kk)
+                prefetch_l2(rp + kk * (kk + 1) / 2, kk < i ? kk + 1 : jr + 1);
+        }
+        for (int k = 0; k <= i; ++k) {
+            const int KL0 = k * (k + 1) / 2;
+            const double *Dk = D + (int64_t)k * n;
+            const double Dik = __ldg(Di + k);
+            const bool last = k == i;   // row (i, j) holds kl <= (i, j): only l <= j in segment i
+            // segment k + kRgPrefetch of the warp's rows: one bulk L2 prefetch per row
+            if (lane < kRgRPW && k + kRgPrefetch <= i) {
+                const int kk = k + kRgPrefetch;
+                const double *rp = lane == 0 ? rowp[0] : rowp[kRgRPW - 1];
+                const bool okr = lane == 0 ? okq[0] : okq[kRgRPW - 1];
+                const int jr = lane == 0 ? jq[0] : jq[kRgRPW - 1];
+                if (okr) prefetch_l2(rp + kk * (kk + 1) / 2, kk < i ? kk + 1 : jr + 1);
             }
-        };
-        load_chunk(0, vnext);
-        for (int64_t c0 = 0; c0 <= KLmax; c0 += 32) {
-            double vcur[kPkRows / kPkWarps];
+            double Djk[kRgRPW], kjk[kRgRPW];
+            int lmax[kRgRPW];
 #pragma unroll
-            for (int q = 0; q < kPkRows / kPkWarps; ++q) vcur[q] = vnext[q];
-            if (c0 + 32 <= KLmax) load_chunk(c0 + 32, vnext);
-            const int64_t KL = c0 + lane;
-            const bool colok = KL <= KLmax;
-            int k = (int)((sqrt(8.0 * (double)KL + 1.0) - 1.0) * 0.5);
-            while ((int64_t)k * (k + 1) / 2 > KL) --k;
-            while ((int64_t)(k + 1) * (k + 2) / 2 <= KL) ++k;
-            const int l = (int)(KL - (int64_t)k * (k + 1) / 2);
-            const int kk = colok ? k : -1;
-            const double Dkl = colok ? __ldg(D + (int64_t)k * n + l) : 0.0;
-            const double Dil = colok ? __ldg(Di + l) : 0.0, Dik = colok ? __ldg(Di + k) : 0.0;
-            const double skl = (k == l ? 0.5 : 1.0);
-            double kik = 0.0, kil = 0.0, jcol = 0.0;
+            for (int q = 0; q < kRgRPW; ++q) {
+                Djk[q] = __ldg(Djp[q] + k);
+                kjk[q] = 0.0;
+                lmax[q] = !okq[q] ? -1 : (last ? jq[q] : k);   // rows past i load nothing
+            }
+            double kik = 0.0;
 #pragma unroll
-            for (int q = 0; q < kPkRows / kPkWarps; ++q) {
-                const int r = warp + kPkWarps * q;
-                const int j = j0 + r;
-                const int64_t IJ = I0 + j;
-                double kjk = 0.0;
-                if (r < nrows && colok && KL <= IJ) {
-                    const double v = vcur[q] * (i == j ? 0.5 : 1.0) * skl * (IJ == KL ? 0.5 : 1.0);
-                    const double *Dj = D + (int64_t)j * n;
-                    jrow[q] += v * Dkl;
-                    jcol += 2.0 * v * __ldg(Di + j);
-                    kik += v * __ldg(Dj + l);
-                    kil += v * __ldg(Dj + k);
-                    kjk = v * Dil;
-                    atomicAdd(Kj + r * n + l, v * Dik);
+            for (int m = 0; m < MAXM; ++m) {
+                if (32 * m > k) continue;   // warp-uniform: chunks past the segment are skipped
+                const int l = 32 * m + lane;
+                const bool inseg = l <= k;
+                const double Dkl = inseg ? __ldg(Dk + l) : 0.0;
+                const double Dil = inseg ? __ldg(Di + l) : 0.0;
+                const double wkl = l == k ? 0.5 : 1.0;
+                double jcol = 0.0;
+#pragma unroll
+                for (int q = 0; q < kRgRPW; ++q) {
+                    const bool ok = l <= lmax[q];
+                    double v = ok ? __ldg(rowp[q] + KL0 + l) : 0.0;
+                    const double Djl = ok ? __ldg(Djp[q] + l) : 0.0;
+                    v *= wq[q] * wkl * ((last && l == jq[q]) ? 0.5 : 1.0);
+                    jrow[q] = fma(v, Dkl, jrow[q]);
+                    jcol = fma(v, Dij2[q], jcol);
+                    kik = fma(v, Djl, kik);
+                    accI[m] = fma(v, Djk[q], accI[m]);
+                    kjk[q] = fma(v, Dil, kjk[q]);
+                    accJ[q][m] = fma(v, Dik, accJ[q][m]);
                 }
-                // Kacc[j,k] += v' D_il: reduce over the run of lanes with this k
-                if (r < nrows) {
-                    const double sum = run_sum(kjk, kk, lane);
-                    const int knext = __shfl_down_sync(0xffffffffu, kk, 1);
-                    if (kk >= 0 && (lane == 31 || knext != kk) && sum != 0.0) atomicAdd(Kj + r * n + kk, sum);
-                }
+                jc[buf][warp][l] = jcol;
             }
-            {
-                const double sum = run_sum(kik, kk, lane);
-                const int knext = __shfl_down_sync(0xffffffffu, kk, 1);
-                if (kk >= 0 && (lane == 31 || knext != kk) && sum != 0.0) atomicAdd(Ki + kk, sum);
+            // segment sums Kacc[i,k], Kacc[j,k] go to column k (lane k % 32, slot k / 32)
+            const double sk = warp_sum(kik);
+            double sj[kRgRPW];
+#pragma unroll
+            for (int q = 0; q < kRgRPW; ++q) sj[q] = warp_sum(kjk[q]);
+            // (as multiply-adds by a 0/1 factor: a conditional add here would
+            // let the compiler turn the unrolled slots back into an indexed,
+            // memory-resident array)
+            const int kslot = lane == (k & 31) ? (k >> 5) : -1;
+#pragma unroll
+            for (int m = 0; m < MAXM; ++m) {
+                const double f = m == kslot ? 1.0 : 0.0;
+                accI[m] = fma(f, sk, accI[m]);
+#pragma unroll
+                for (int q = 0; q < kRgRPW; ++q) accJ[q][m] = fma(f, sj[q], accJ[q][m]);
             }
-            if (kil != 0.0) atomicAdd(Ki + l, kil);
-            jc[warp * 32 + lane] = jcol;
             __syncthreads();
-            if (warp == 0) {
+            // Jacc[k, l] for l <= k: warps split the columns
+            for (int l = threadIdx.x; l <= k; l += kRgWarps * 32) {
                 double s = 0.0;
 #pragma unroll
-                for (int w = 0; w < kPkWarps; ++w) s += jc[w * 32 + lane];
-                if (colok && s != 0.0) atomicAdd(Jacc + (int64_t)k * n + l, s);
+                for (int w = 0; w < kRgWarps; ++w) s += jc[buf][w][l];
+                if (s != 0.0) atomicAdd(Jacc + (int64_t)k * n + l, s);
             }
-            __syncthreads();
+            buf ^= 1;
         }
 #pragma unroll
-        for (int q = 0; q < kPkRows / kPkWarps; ++q) {
-            double x = jrow[q];
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            const int r = warp + kPkWarps * q;
-            if (lane == 0 && r < nrows && x != 0.0) atomicAdd(Jacc + (int64_t)i * n + j0 + r, 2.0 * x);
+        for (int q = 0; q < kRgRPW; ++q) {
+            const double x = warp_sum(jrow[q]);
+            if (lane == 0 && okq[q] && x != 0.0) atomicAdd(Jacc + (int64_t)i * n + jq[q], 2.0 * x);
+        }
+        // rows j of Kacc from registers; row i summed over the warps
+#pragma unroll
+        for (int m = 0; m < MAXM; ++m) {
+            const int c = 32 * m + lane;
+            kis[warp][c] = accI[m];
+            if (c <= i) {
+#pragma unroll
+                for (int q = 0; q < kRgRPW; ++q)
+                    if (okq[q] && accJ[q][m] != 0.0) atomicAdd(Kacc + (int64_t)jq[q] * n + c, accJ[q][m]);
+            }
         }
         __syncthreads();
-        for (int x = tid; x <= i; x += blockDim.x)
-            if (Ki[x] != 0.0) atomicAdd(Kacc + (int64_t)i * n + x, Ki[x]);
-        for (int x = tid; x < nrows * n; x += blockDim.x) {
-            const int r = x / n, c = x - r * n;
-            if (c <= i && Kj[x] != 0.0) atomicAdd(Kacc + (int64_t)(j0 + r) * n + c, Kj[x]);
+        for (int c = threadIdx.x; c <= i; c += kRgWarps * 32) {
+            double s = 0.0;
+#pragma unroll
+            for (int w = 0; w < kRgWarps; ++w) s += kis[w][c];
+            if (s != 0.0) atomicAdd(Kacc + (int64_t)i * n + c, s);
         }
         __syncthreads();
     }
@@ -1205,6 +1253,10 @@ int pqb_set_param(pqb_ctx *ctx, int param, int qclass, int value)
         if (value < 0 || value > 1) return fail(ctx, PQB_E_ARG, "order %d out of range", value);
         ctx->order = value;
         return PQB_OK;
+    case PQB_PARAM_PACKED_KERNEL:
+        if (value < 0 || value > 1) return fail(ctx, PQB_E_ARG, "packed kernel %d out of range", value);
+        ctx->packed_simple = value == 1;
+        return PQB_OK;
     }
     return fail(ctx, PQB_E_ARG, "unknown parameter %d", param);
 }
@@ -1418,27 +1470,34 @@ int pqb_jk_packed(pqb_ctx *ctx, const double *ints, int64_t len, const double *D
     cudaStream_t st = (cudaStream_t)stream;
     PQB_CK(ctx, cudaMemsetAsync(J, 0, sizeof(double) * nbf * nbf, st));
     PQB_CK(ctx, cudaMemsetAsync(K, 0, sizeof(double) * nbf * nbf, st));
-    const size_t smem = sizeof(double) * ((size_t)(1 + kPkRows) * nbf + kPkWarps * 32);
-    if (smem <= 200 * 1024) {
+    if (nbf <= 512 && !ctx->packed_simple) {
+        // register form: tiles (i, j0) of 16 rows, heaviest (largest i) first
         if (ctx->pk_tiles_nbf != nbf) {
-            // tiles (i, j0), heaviest (largest i) first
             std::vector<int2> tiles;
             for (int i = nbf - 1; i >= 0; --i)
-                for (int j0 = 0; j0 <= i; j0 += kPkRows) tiles.push_back(make_int2(i, j0));
+                for (int j0 = 0; j0 <= i; j0 += kRgRows) tiles.push_back(make_int2(i, j0));
             free_dev(ctx->d_pk_tiles);
             ctx->d_pk_tiles = nullptr;
             PQB_CK(ctx, cudaMalloc(&ctx->d_pk_tiles, sizeof(int2) * tiles.size()));
             PQB_CK(ctx, cudaMemcpy(ctx->d_pk_tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
             ctx->pk_tiles_n = (int)tiles.size();
             ctx->pk_tiles_nbf = nbf;
-            PQB_CK(ctx, cudaFuncSetAttribute(jk_packed_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             200 * 1024));
         }
         int grid = ctx->pk_tiles_n;
-        if (grid > ctx->nsm * 8) grid = ctx->nsm * 8;
-        jk_packed_tiled_kernel<<<grid, kPkWarps * 32, smem, st>>>(ints, D, J, K, nbf, ctx->d_pk_tiles,
-                                                                  ctx->pk_tiles_n);
+        if (grid > ctx->nsm * 16) grid = ctx->nsm * 16;
+        const int maxm = nbf <= 256 ? 8 : 16;
+        const size_t rsm = sizeof(double) * 3 * kRgWarps * maxm * 32;
+        if (maxm == 8) {
+            PQB_CK(ctx, cudaFuncSetAttribute(jk_packed_reg_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm));
+            jk_packed_reg_kernel<8><<<grid, kRgWarps * 32, rsm, st>>>(ints, D, J, K, nbf, ctx->d_pk_tiles,
+                                                                      ctx->pk_tiles_n);
+        } else {
+            PQB_CK(ctx, cudaFuncSetAttribute(jk_packed_reg_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm));
+            jk_packed_reg_kernel<16><<<grid, kRgWarps * 32, rsm, st>>>(ints, D, J, K, nbf, ctx->d_pk_tiles,
+                                                                       ctx->pk_tiles_n);
+        }
     } else {
+        // one block per packed row (nbf > 512: the packed array alone is then over 69 GB)
         jk_packed_kernel<<<(unsigned)P, 256, 0, st>>>(ints, D, J, K, nbf);
     }
     symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, nbf, nullptr);

@@ -169,30 +169,35 @@ __device__ __forceinline__ void boys_row(double T, double *F)
 }
 
 // ------------------------------------------------------------------- Rys --
-__device__ __forceinline__ double clenshaw14(const double *c, double x)
-{
-    double b1 = 0.0, b2 = 0.0, x2 = 2.0 * x;
-#pragma unroll
-    for (int k = PQB_RYS_NCOEF - 1; k >= 1; --k) {
-        double t = fma(x2, b1, __ldg(c + k) - b2);
-        b2 = b1;
-        b1 = t;
-    }
-    return fma(x, b1, __ldg(c) - b2);
-}
-
 // Root r (0-based, ascending) of the n-point Rys rule at T, as u = t^2 in
-// (0,1), and its weight (sum_r w_r = F_0(T)).
+// (0,1), and its weight (sum_r w_r = F_0(T)).  Below the large-T limit both
+// come from degree-13 Chebyshev series on the unit interval of T holding it;
+// the table row of (n, interval, root) holds the 14 coefficient pairs
+// (root_k, weight_k) interleaved, read with seven 256-bit loads, and the two
+// Clenshaw recurrences run side by side.
 __device__ __forceinline__ void rys_root(int n, int r, double T, double &u, double &w)
 {
+    static_assert(PQB_RYS_NCOEF == 14, "seven 256-bit loads per root");
     if (T < pqb_rys_tasym[n]) {
-        int iv = (int)T;
-        double x = 2.0 * (T - iv) - 1.0;
-        const double *c = pqb_rys_coef + pqb_rys_offset[n] + (iv * 2 * n + 2 * r) * PQB_RYS_NCOEF;
-        u = clenshaw14(c, x);
-        w = clenshaw14(c + PQB_RYS_NCOEF, x);
+        const int iv = (int)T;
+        const double x = 2.0 * (T - iv) - 1.0, x2 = 2.0 * x;
+        const double *c = pqb_rys_coef + pqb_rys_offset[n] + (iv * n + r) * (2 * PQB_RYS_NCOEF);
+        double cu[PQB_RYS_NCOEF], cw[PQB_RYS_NCOEF];
+#pragma unroll
+        for (int j = 0; j < PQB_RYS_NCOEF / 2; ++j) ld4(c + 4 * j, cu[2 * j], cw[2 * j], cu[2 * j + 1], cw[2 * j + 1]);
+        double bu1 = 0.0, bu2 = 0.0, bw1 = 0.0, bw2 = 0.0;
+#pragma unroll
+        for (int k = PQB_RYS_NCOEF - 1; k >= 1; --k) {
+            const double tu = fma(x2, bu1, cu[k] - bu2), tw = fma(x2, bw1, cw[k] - bw2);
+            bu2 = bu1;
+            bu1 = tu;
+            bw2 = bw1;
+            bw1 = tw;
+        }
+        u = fma(x, bu1, cu[0] - bu2);
+        w = fma(x, bw1, cw[0] - bw2);
     } else {
-        double it = 1.0 / T;
+        const double it = 1.0 / T;
         u = pqb_rys_asym_root[n][r] * it;
         w = pqb_rys_asym_weight[n][r] * sqrt(it);
     }

@@ -211,6 +211,40 @@ def test_jk_stored_and_direct_vs_oracle():
     assert np.abs(Gt.cpu().numpy() - (2 * Jo - Ko)).max() < 2 * ERI_TOL
 
 
+def test_stored_jk_kernels_agree_with_oracle_and_direct():
+    """pqb_jk_packed: the register-form kernel (nbf <= 256 and 257..512
+    variants) and the one-block-per-row kernel give the same J and K; small
+    case against the oracle, (H2O)11 / 6-31G** (N = 275) against the direct
+    FP64 build."""
+    from pyquante_b200.engine import jk_packed
+    mol = geometries.water_cluster(2, seed=4)
+    bs = BasisSet(mol, "6-31g**")
+    D = _rand_density(len(bs))
+    Jo, Ko = O.getJK(O.orc_get2ints(oracle_bfs(bs)), D)
+    ints = Ints.get2ints(bs).tensor
+    Dt = torch.as_tensor(D, device="cuda")
+    ctx = _lib.Context(torch.cuda.current_device())
+    for simple in (0, 1):
+        ctx.check(ctx.lib.pqb_set_param(ctx.h, _lib.PQB_PARAM_PACKED_KERNEL, 0, simple))
+        J, K = jk_packed(ints, Dt, ctx)
+        assert np.abs(J.cpu().numpy() - Jo).max() < ERI_TOL, simple
+        assert np.abs(K.cpu().numpy() - Ko).max() < ERI_TOL, simple
+    mol = geometries.water_cluster(11, seed=1, box_ang=10.1)
+    bs = BasisSet(mol, "6-31g**")
+    n = len(bs)
+    assert 256 < n <= 512
+    D = _rand_density(n, 3)
+    Dt = torch.as_tensor(D, device="cuda")
+    eng = BasisEngine(bs.bfs)
+    Jd, Kd = eng.jk(Dt, "fp64", 0.0)
+    ints = eng.eri_packed()
+    ctx.check(ctx.lib.pqb_set_param(ctx.h, _lib.PQB_PARAM_PACKED_KERNEL, 0, 0))
+    J, K = jk_packed(ints, Dt, ctx)
+    assert float((J - Jd).abs().max()) < 1e-9 and float((K - Kd).abs().max()) < 1e-9
+    del ints
+    torch.cuda.empty_cache()
+
+
 def test_jk_mixed_precision_error_is_small():
     mol = geometries.water_cluster(3, seed=2)
     bs = BasisSet(mol, "6-31g**")
