@@ -1,5 +1,5 @@
 """Autotuner for the direct J/K plan: per angular-momentum class, the
-primitive-quartet chunk of a work item (1 .. 64), and the number of
+primitive-quartet chunk of a work item (2 .. 128), and the number of
 streams the class launches share.
 
     python -m pyquante_b200.autotune            # tunes (H2O)8 / 6-31G** on cuda:0
@@ -19,7 +19,7 @@ import os
 import numpy as np
 
 TUNED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned.json")
-CHUNKS = (2, 4, 8, 16, 32, 64)
+CHUNKS = (2, 4, 8, 16, 32, 64, 128)
 
 
 def load():
