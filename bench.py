@@ -34,6 +34,11 @@ WORKLOAD = "(H2O)8 cluster, 6-31G** cartesian, N=200, seed 0, 9 A cube"
 SCHWARZ = 1e-12
 FP32_THRESH = 1e-5
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on these workloads:
+# one stored-integral J/K launch (profiles/jk_packed_reg_h2o8_631gss.md) and the 34 class
+# launches of one FP64 direct build captured there (profiles/eri_jk_direct_h2o8_631gss.md, section 2)
+STORED_TRAFFIC_BYTES = 1620087000 + 4919296
+DIRECT_TRAFFIC_BYTES = 46173184
 
 
 def parse():
@@ -47,6 +52,8 @@ def parse():
     p.add_argument("--no-graph", action="store_true", help="launch the timed builds eagerly instead of replaying "
                                                              "a captured CUDA graph")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--soak", type=int, default=3000, help="untimed builds run under the clock sampler before the "
+                                                           "timed ones")
     p.add_argument("--workload", default="h2o8", choices=["h2o8", "stored", "c16h34", "h2o4-grad", "batch"],
                    help="h2o8: the headline Fock build; the others are the secondary workloads "
                         "(C16H34 threshold sweep, (H2O)4 gradient, batched SCF)")
@@ -233,8 +240,10 @@ def run_stored(a):
                       "config": {"workload": WORKLOAD, "packed_integrals": Q, "bytes_per_build": nbytes,
                                  "l2": "packed array 1.6 GB > L2, no flush"},
                       "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
-                                   "frac": gbs / peak, "traffic": None, "peak_source": src,
-                                   "kernel": "jk_packed_tiled_kernel"}}))
+                                   "frac": gbs / peak, "traffic": STORED_TRAFFIC_BYTES, "peak_source": src,
+                                   "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                                                     "profiles/jk_packed_reg_h2o8_631gss.md",
+                                   "kernel": "jk_packed_reg_kernel<8>"}}))
 
 def run_c16h34(a):
     """C16H34 / 6-31G* (N = 308): FP64 vs mixed Fock build and SCF energy for
@@ -481,6 +490,12 @@ def main():
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(torch.cuda.current_device()) as clk:
+        # the same builds (a fixed count, identical on every rank) for about
+        # 1.5 s before the timed ones, so the clock record (nvidia-smi every
+        # 0.2 s) covers the GPU under this load
+        for _ in range(a.soak):
+            run_build(a.precision)
+        torch.cuda.synchronize()
         ms = timed(a.precision, a.steps)
         torch.cuda.synchronize()
         barrier()
@@ -577,7 +592,9 @@ def main():
                     "h2d_bytes_per_step": int(D.numel() * 8), "d2h_bytes_per_step": int(D.numel() * 8),
                     "api": "pyquante_b200.Ints.DirectInts.jk (the get2JmK path) from pinned host D"},
             "roofline": {"bound": "fp64", "achieved": build_tflops, "peak": peak_tf, "unit": "TFLOP/s",
-                         "frac": build_tflops / peak_tf, "traffic": None,
+                         "frac": build_tflops / peak_tf, "traffic": DIRECT_TRAFFIC_BYTES,
+                         "traffic_note": "DRAM bytes of 34 of the 42 class launches of one FP64 build (ncu); the "
+                                         "build is L2-resident, so the FP64 pipe, not HBM, is the roofline",
                          "kernel": "eri_thread_kernel/eri_block_kernel<class, EpiJK>: all class instantiations "
                                    "of one FP64 Fock build, launched together by pqb_jk_direct",
                          "flops_per_build": tot_fl, "fp64_build_ms": ms_fp64,
