@@ -20,6 +20,7 @@
 // component pair (ia, ib) for all ket components, so the same engine
 // writes packed integrals, digests into J/K, or forms Schwarz bounds.
 #pragma once
+#include <type_traits>
 #include "pqb_device.cuh"
 #include "pqb_types.h"
 
@@ -379,6 +380,54 @@ struct EpiSchwarz {
 // small classes are latency bound, so they trade registers for occupancy.
 __host__ __device__ constexpr int thread_min_blocks(int nabcd) { return nabcd == 1 ? 8 : (nabcd <= 9 ? 4 : 2); }
 
+// Single-precision counterpart of add_prim_quartet for the FP32 lists of
+// the mixed mode: geometry, roots (rys_roots_f32), 2-D tables and assembly
+// all in FP32; only large-T root forms are evaluated in FP64.
+struct QuartetGeomF {
+    float A[3], C[3], AB[3], CD[3];
+};
+
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void add_prim_quartet_f32(const QuartetGeomF &g, const float *P, const float *Q, float *acc)
+{
+    constexpr int NB = ncart(LB), ND = ncart(LD);
+    constexpr int NAB = ncart(LA) * NB, NCD = ncart(LC) * ND;
+    constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
+    constexpr int G2D = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
+    // P, Q: zeta, 1/zeta, P[3], K
+    const float zeta = P[0], eta = Q[0];
+    const float PQ[3] = {P[2] - Q[2], P[3] - Q[3], P[4] - Q[4]};
+    const float rs = rsqrtf(zeta + eta), izpe = rs * rs;
+    const float T = zeta * eta * izpe * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+    const float pre = P[5] * Q[5] * rs;
+    float uu[NR], ww[NR];
+    rys_roots_f32<NR>(T, uu, ww);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const float ue = uu[r] * izpe, ce = eta * ue, cz = zeta * ue;
+        const float b00 = 0.5f * ue, b10 = 0.5f * P[1] * (1.0f - ce), b01 = 0.5f * Q[1] * (1.0f - cz);
+        float gx[G2D], gy[G2D], gz[G2D];
+        float *gt[3] = {gx, gy, gz};
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+            rys2d_f<LA, LB, LC, LD>(b00, b10, b01, fmaf(-ce, PQ[x], P[2 + x] - g.A[x]), fmaf(cz, PQ[x], Q[2 + x] - g.C[x]),
+                                    g.AB[x], g.CD[x], x == 0 ? ww[r] * pre : 1.0f, gt[x]);
+#pragma unroll
+        for (int ab = 0; ab < NAB; ++ab)
+#pragma unroll
+            for (int cd = 0; cd < NCD; ++cd) {
+                const int ia = ab / NB, ib = ab % NB, ic = cd / ND, id = cd % ND;
+                const int ox = ((cart_lx(LA, ia) * (LB + 1) + cart_lx(LB, ib)) * (LC + 1) + cart_lx(LC, ic)) * (LD + 1) +
+                               cart_lx(LD, id);
+                const int oy = ((cart_ly(LA, ia) * (LB + 1) + cart_ly(LB, ib)) * (LC + 1) + cart_ly(LC, ic)) * (LD + 1) +
+                               cart_ly(LD, id);
+                const int oz = ((cart_lz(LA, ia) * (LB + 1) + cart_lz(LB, ib)) * (LC + 1) + cart_lz(LC, ic)) * (LD + 1) +
+                               cart_lz(LD, id);
+                acc[ab * NCD + cd] = fmaf(gx[ox] * gy[oy], gz[oz], acc[ab * NCD + cd]);
+            }
+    }
+}
+
 template <int LA, int LB, int LC, int LD, typename R, class Epi>
 __global__ void __launch_bounds__(128, thread_min_blocks(ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)))
 eri_thread_kernel(const int4 *__restrict__ list, int nq,
@@ -403,6 +452,38 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
         const int npk = pk.nprim;
         const PrimPair *pbp = prims + pb.prim_off, *pkp = prims + pk.prim_off;
         int ib = e.z / npk, ik = e.z - (e.z / npk) * npk;
+        if constexpr (std::is_same_v<R, float>) {
+            // FP32 list of the mixed mode: single-precision primitive data
+            QuartetGeomF gf;
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+                gf.A[x] = (float)pb.A[x];
+                gf.C[x] = (float)pk.A[x];
+                gf.AB[x] = (float)pb.AB[x];
+                gf.CD[x] = (float)pk.AB[x];
+            }
+            float P[8], Qn[8];
+            ld8f(pbp[ib].f, P);
+            ld8f(pkp[ik].f, Qn);
+            for (int t = 0; t < e.w; ++t) {
+                float Q[8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) Q[c] = Qn[c];
+                int ik2 = ik + 1, ib2 = ib;
+                if (ik2 == npk) {
+                    ik2 = 0;
+                    ++ib2;
+                }
+                if (t + 1 < e.w) ld8f(pkp[ik2].f, Qn);
+                add_prim_quartet_f32<LA, LB, LC, LD>(gf, P, Q, reinterpret_cast<float *>(acc));
+                if (ib2 != ib && t + 1 < e.w) ld8f(pbp[ib2].f, P);
+                ib = ib2;
+                ik = ik2;
+            }
+            const QCtx q = make_qctx(pb, pk, e.x, e.y);
+            epi.template thread_quartet<LA, LB, LC, LD, R>(q, acc);
+            continue;
+        }
         PrimJK P = load_prim_jk(pbp + ib);
         PrimJK Qn = load_prim_jk(pkp + ik);
         for (int t = 0; t < e.w; ++t) {

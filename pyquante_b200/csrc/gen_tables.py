@@ -195,6 +195,18 @@ def main():
                 cu, cw = funcs[2 * r], funcs[2 * r + 1]
                 lines.append("  " + ", ".join("%.17e, %.17e" % (a, b) for a, b in zip(cu, cw)) + ",")
     lines.append("};")
+    # FP32 copy for the mixed-precision kernels: per (n, interval, root) the
+    # first 7 coefficient pairs (the rest sum to < 1.1e-8 relative) and a zero
+    # pair, 64 bytes: two 256-bit loads
+    lines.append("#define PQB_RYS_NCOEF_F32 7")
+    lines.append("PQB_TABQ __align__(64) float pqb_rys_coef_f32[PQB_RYS_TABLE_SIZE / 14 * 16 / 2] = {")
+    for n in range(1, RYS_NMAX + 1):
+        for iv, funcs in enumerate(rys[n]):
+            for r in range(n):
+                cu, cw = funcs[2 * r], funcs[2 * r + 1]
+                pairs = [(cu[k], cw[k]) for k in range(7)] + [(0.0, 0.0)]
+                lines.append("  " + ", ".join("%.9ef, %.9ef" % (a, b) for a, b in pairs) + ",")
+    lines.append("};")
     lines.append("PQB_TABQ double pqb_boys_tab[PQB_BOYS_NGRID * PQB_BOYS_NORD] = {")
     for row in boys_tab:
         lines.append("  " + ", ".join("%.17e" % v for v in row) + ",")
@@ -223,12 +235,24 @@ def main_boys_rows():
              "#define PQB_BOYSROW_STEP_INV %d" % BOYSROW_STEP_INV,
              "#define PQB_BOYSROW_NGRID %d" % BOYSROW_NGRID,
              "#define PQB_BOYSROW_TMAX %.1f" % BOYS_TMAX]
+    rows = {}
     for M in BOYSROW_ORDERS:
         lines.append("PQB_TABQ __align__(64) double pqb_boys_row%d[PQB_BOYSROW_NGRID * 8] = {" % M)
+        rows[M] = []
         for k in range(BOYSROW_NGRID):
             T = mp.mpf(k) / BOYSROW_STEP_INV
             row = [boys(M + j, T) for j in range(7)] + [mp.exp(-T)]
+            rows[M].append(row)
             lines.append("  " + ", ".join("%.17e" % float(v) for v in row) + ",")
+        lines.append("};")
+    # FP32 rows for the mixed-precision kernels: F_M .. F_(M+3)(T_k), exp(-T_k),
+    # three zeros (32 bytes: one 256-bit load; a 4-term Taylor series is
+    # accurate to 3e-9 relative for |T - T_k| <= 1/64)
+    for M in BOYSROW_ORDERS:
+        lines.append("PQB_TABQ __align__(64) float pqb_boys_row%d_f32[PQB_BOYSROW_NGRID * 8] = {" % M)
+        for row in rows[M]:
+            vals = [row[0], row[1], row[2], row[3], row[7], 0, 0, 0]
+            lines.append("  " + ", ".join("%.9ef" % float(v) for v in vals) + ",")
         lines.append("};")
     with open(os.path.join(here, "boys_rows.inc"), "w") as f:
         f.write("\n".join(lines) + "\n")

@@ -1086,6 +1086,10 @@ int pqb_shells_upload_batch(pqb_ctx *ctx, int nmol, const int *mol_shell_off, in
                     for (int x = 0; x < 3; ++x) pp.P[x] = (al * A[x] + be * B[x]) / z;
                     pp.K = prim_coef[p] * prim_coef[q] * kPairPre / z * e;
                     pp.alpha_a = al;
+                    pp.f[0] = (float)pp.zeta;
+                    pp.f[1] = (float)pp.izeta;
+                    for (int x = 0; x < 3; ++x) pp.f[2 + x] = (float)pp.P[x];
+                    pp.f[5] = (float)pp.K;
                     prims.push_back(pp);
                 }
             pi.nprim = (int)prims.size() - pi.prim_off;

@@ -168,6 +168,130 @@ __device__ __forceinline__ void boys_row(double T, double *F)
     }
 }
 
+// ------------------------------------------------ single precision (mixed) --
+// The FP32 kernels of the mixed mode evaluate the Boys function and the Rys
+// rules in single precision for T < PQB_BOYSROW_TMAX; larger arguments use
+// the FP64 asymptotic forms, rounded to single precision afterwards.
+
+// Eight floats from 32-byte aligned global memory with one 256-bit load.
+__device__ __forceinline__ void ld8f(const float *p, float *r)
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]), "=f"(r[7])
+        : "l"(__cvta_generic_to_global(p)));
+}
+
+// F_m(T), m = 0..M for M = 1 or 3, T < PQB_BOYSROW_TMAX, from one 32-byte row
+// of pqb_boys_rowM_f32 (F_M .. F_(M+3), exp(-T_k) at T_k = k/32): 4-term
+// Taylor series (remainder < 3e-9 F_M), exp(-T) = exp(-T_k) exp(-(T - T_k))
+// (4-term series), downward recursion.
+template <int M>
+__device__ __forceinline__ void boys_row_f32(float T, float *F)
+{
+    static_assert(M == 1 || M == 3, "rows exist for M = 1 and 3");
+    const int k = __float2int_rn(T * PQB_BOYSROW_STEP_INV);
+    const float d = k * (1.0f / PQB_BOYSROW_STEP_INV) - T;   // -(T - T_k)
+    float r[8];
+    ld8f((M == 1 ? pqb_boys_row1_f32 : pqb_boys_row3_f32) + 8 * k, r);
+    float f = r[3];
+    f = fmaf(f, d * (1.0f / 3.0f), r[2]);
+    f = fmaf(f, d * 0.5f, r[1]);
+    f = fmaf(f, d, r[0]);
+    F[M] = f;
+    float ed = fmaf(d, 1.0f / 4.0f, 1.0f);
+    ed = fmaf(d * (1.0f / 3.0f), ed, 1.0f);
+    ed = fmaf(d * 0.5f, ed, 1.0f);
+    ed = fmaf(d, ed, 1.0f);
+    const float e = r[4] * ed, t2 = 2.0f * T;
+#pragma unroll
+    for (int m = M - 1; m >= 0; --m) F[m] = fmaf(t2, F[m + 1], e) * (1.0f / (2 * m + 1));
+}
+
+// Root r of the n-point rule at T < pqb_rys_tasym[n] from the single-precision
+// Chebyshev table (7 coefficient pairs, interleaved, per (n, interval, root):
+// two 256-bit loads).
+__device__ __forceinline__ void rys_root_f32(int n, int r, float T, float &u, float &w)
+{
+    const int iv = (int)T;
+    const float x = 2.0f * (T - iv) - 1.0f, x2 = 2.0f * x;
+    const float *c = pqb_rys_coef_f32 + (pqb_rys_offset[n] / (2 * PQB_RYS_NCOEF) + iv * n + r) * 16;
+    float cc[16];
+    ld8f(c, cc);
+    ld8f(c + 8, cc + 8);
+    float bu1 = 0.0f, bu2 = 0.0f, bw1 = 0.0f, bw2 = 0.0f;
+#pragma unroll
+    for (int k = PQB_RYS_NCOEF_F32 - 1; k >= 1; --k) {
+        const float tu = fmaf(x2, bu1, cc[2 * k] - bu2), tw = fmaf(x2, bw1, cc[2 * k + 1] - bw2);
+        bu2 = bu1;
+        bu1 = tu;
+        bw2 = bw1;
+        bw1 = tw;
+    }
+    u = fmaf(x, bu1, cc[0] - bu2);
+    w = fmaf(x, bw1, cc[1] - bw2);
+}
+
+// All NR roots at T (single precision): moments of a Boys row for NR <= 2,
+// the truncated Chebyshev table for NR >= 3; FP64 large-T forms above the
+// tables (PQB_BOYSROW_TMAX for the Boys rows, pqb_rys_tasym[NR] otherwise).
+template <int NR>
+__device__ __forceinline__ void rys_roots_f32(float T, float *u, float *w)
+{
+    const bool large = NR <= 2 ? T >= (float)PQB_BOYSROW_TMAX : T >= (float)pqb_rys_tasym[NR];
+    if (large) {
+        const double Td = (double)T, it = rcp_nr(Td), rit = rsqrt_nr(Td);
+        if constexpr (NR <= 2) {
+            // F_m for the moments, exact large-T forms in FP64
+            double F[4];
+            F[0] = 0.88622692545275801365 * rit;
+            const double e = exp(-Td), h = 0.5 * it;
+#pragma unroll
+            for (int m = 0; m < 2 * NR - 1; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+            if constexpr (NR == 1) {
+                w[0] = (float)F[0];
+                u[0] = (float)(F[1] * rcp_nr(F[0]));
+            } else {
+                const double id = rcp_nr(fma(F[0], F[2], -F[1] * F[1]));
+                const double a1 = fma(F[1], F[2], -F[0] * F[3]) * id, a0 = fma(F[1], F[3], -F[2] * F[2]) * id;
+                const double disc = fma(a1, a1, -4.0 * a0), rs = rsqrt_nr(disc);
+                const double ub = 0.5 * fma(disc, rs, -a1);
+                u[0] = (float)(a0 * rcp_nr(ub));
+                u[1] = (float)ub;
+                const double w0 = fma(ub, F[0], -F[1]) * rs;
+                w[0] = (float)w0;
+                w[1] = (float)(F[0] - w0);
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                u[r] = (float)(pqb_rys_asym_root[NR][r] * it);
+                w[r] = (float)(pqb_rys_asym_weight[NR][r] * rit);
+            }
+        }
+        return;
+    }
+    if constexpr (NR == 1) {
+        float F[2];
+        boys_row_f32<1>(T, F);
+        w[0] = F[0];
+        u[0] = __fdividef(F[1], F[0]);
+    } else if constexpr (NR == 2) {
+        float F[4];
+        boys_row_f32<3>(T, F);
+        const float id = __fdividef(1.0f, fmaf(F[0], F[2], -F[1] * F[1]));
+        const float a1 = fmaf(F[1], F[2], -F[0] * F[3]) * id, a0 = fmaf(F[1], F[3], -F[2] * F[2]) * id;
+        const float disc = fmaf(a1, a1, -4.0f * a0), rs = rsqrtf(disc);
+        const float ub = 0.5f * fmaf(disc, rs, -a1);
+        u[0] = __fdividef(a0, ub);
+        u[1] = ub;
+        w[0] = fmaf(ub, F[0], -F[1]) * rs;
+        w[1] = F[0] - w[0];
+    } else {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) rys_root_f32(NR, r, T, u[r], w[r]);
+    }
+}
+
 // ------------------------------------------------------------------- Rys --
 // Root r (0-based, ascending) of the n-point Rys rule at T, as u = t^2 in
 // (0,1), and its weight (sum_r w_r = F_0(T)).  Below the large-T limit both
@@ -336,6 +460,58 @@ __device__ __forceinline__ void rys2d_c(const RysCoef &k, double PA, double QC, 
             for (int b = 1; b <= LB; ++b)
 #pragma unroll
                 for (int n = 0; n + b <= NB; ++n) t[n][b] = t[n + 1][b - 1] + (R)AB * t[n][b - 1];
+#pragma unroll
+            for (int a = 0; a <= LA; ++a)
+#pragma unroll
+                for (int b = 0; b <= LB; ++b) out[((a * (LB + 1) + b) * (LC + 1) + c) * (LD + 1) + d] = t[a][b];
+        }
+}
+
+// The 2-D tables in single precision from single-precision inputs (mixed
+// mode): the same recurrence and transfers as rys2d_c.
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void rys2d_f(float b00, float b10, float b01, float c00, float c01, float AB, float CD,
+                                        float scale, float *out)
+{
+    constexpr int NB = LA + LB, MK = LC + LD;
+    float g[NB + 1][MK + 1];
+    g[0][0] = scale;
+    if (NB > 0) g[1][0] = c00 * scale;
+#pragma unroll
+    for (int n = 1; n < NB; ++n) g[n + 1][0] = (n * b10) * g[n - 1][0] + c00 * g[n][0];
+#pragma unroll
+    for (int n = 0; n <= NB; ++n) {
+        if (MK > 0) g[n][1] = c01 * g[n][0] + (n > 0 ? (n * b00) * g[n - 1][0] : 0.0f);
+#pragma unroll
+        for (int m = 1; m < MK; ++m)
+            g[n][m + 1] = (m * b01) * g[n][m - 1] + c01 * g[n][m] + (n > 0 ? (n * b00) * g[n - 1][m] : 0.0f);
+    }
+    float h[NB + 1][LC + 1][LD + 1];
+#pragma unroll
+    for (int n = 0; n <= NB; ++n) {
+        float t[MK + 1][LD + 1];
+#pragma unroll
+        for (int m = 0; m <= MK; ++m) t[m][0] = g[n][m];
+#pragma unroll
+        for (int d = 1; d <= LD; ++d)
+#pragma unroll
+            for (int m = 0; m + d <= MK; ++m) t[m][d] = t[m + 1][d - 1] + CD * t[m][d - 1];
+#pragma unroll
+        for (int c = 0; c <= LC; ++c)
+#pragma unroll
+            for (int d = 0; d <= LD; ++d) h[n][c][d] = t[c][d];
+    }
+#pragma unroll
+    for (int c = 0; c <= LC; ++c)
+#pragma unroll
+        for (int d = 0; d <= LD; ++d) {
+            float t[NB + 1][LB + 1];
+#pragma unroll
+            for (int n = 0; n <= NB; ++n) t[n][0] = h[n][c][d];
+#pragma unroll
+            for (int b = 1; b <= LB; ++b)
+#pragma unroll
+                for (int n = 0; n + b <= NB; ++n) t[n][b] = t[n + 1][b - 1] + AB * t[n][b - 1];
 #pragma unroll
             for (int a = 0; a <= LA; ++a)
 #pragma unroll

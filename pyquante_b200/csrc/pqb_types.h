@@ -27,8 +27,9 @@ struct PairInfo {
                        // (global function indices; 0 for a single molecule)
 };
 
-// 64 bytes, 32-byte aligned: the kernels fetch the Fock-build fields with one
-// 256-bit and one 128-bit load.
+// 96 bytes, 32-byte aligned.  The FP64 kernels fetch the Fock-build fields
+// with one 256-bit and one 128-bit load; the FP32 kernels (mixed precision)
+// fetch their single-precision copy, f[], with one 256-bit load.
 struct __align__(32) PrimPair {
     double zeta;       // alpha_a + alpha_b
     double izeta;      // 1 / zeta (the recurrences multiply; no division per quartet)
@@ -36,6 +37,7 @@ struct __align__(32) PrimPair {
     double K;          // c_a c_b sqrt(2) pi^(5/4)/zeta exp(-alpha_a alpha_b/zeta |AB|^2)
     double alpha_a;    // exponent of the first shell's primitive (alpha_b = zeta - alpha_a)
     double pad_;
+    float f[8];        // zeta, 1/zeta, P[3], K rounded to single precision, 0, 0
 };
 
 __host__ __device__ inline int pair_class(int la, int lb)   // la >= lb
