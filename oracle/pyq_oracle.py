@@ -360,3 +360,92 @@ def rhf(atoms, S, h, ints, nclosed, conv=1e-10, maxiter=100, diis=False):
             break
         eold = energy
     return energy, orbe, orbs
+
+
+# --------------------------------------------------------------- gradient --
+def _deriv_parts(bf, x):
+    """d phi / dA_x of a contracted function on centre A as up to two
+    functions: raising, sum_p c_p N_p(l) 2 alpha_p x^(l+1) e^(-alpha_p r^2),
+    and lowering, -l sum_p c_p N_p(l) x^(l-1) e^(-alpha_p r^2).  (The
+    reference builds the same derivative from normalised primitives,
+    PyQuante/AnalyticDerivatives.py:457-674.)  BF renormalises per
+    primitive, so the coefficients divide that norm back out."""
+    parts = []
+    up = list(bf.powers)
+    up[x] += 1
+    c_up = [c * n * 2.0 * a / prim_norm(a, up) for a, c, n in zip(bf.pexps, bf.pcoefs, bf.pnorms)]
+    parts.append(BF(bf.origin, up, list(zip(bf.pexps, c_up))))
+    if bf.powers[x] > 0:
+        dn = list(bf.powers)
+        dn[x] -= 1
+        l = bf.powers[x]
+        c_dn = [-l * c * n / prim_norm(a, dn) for a, c, n in zip(bf.pexps, bf.pcoefs, bf.pnorms)]
+        parts.append(BF(bf.origin, dn, list(zip(bf.pexps, c_dn))))
+    return parts
+
+
+def rhf_gradient(atoms, basis_data, D, Q):
+    """dE/dR for closed-shell RHF, the formula of PyQuante/force.py:48-70
+    (Szabo eq. C.12) with D = C_occ C_occ^T and Q = C_occ e_occ C_occ^T
+    (Wavefunction.py:143-149):
+      dE/dR_a = 2 tr(D dH/dR_a) + tr(D dG[D]/dR_a) - 2 tr(Q dS/dR_a) + dE_nuc/dR_a,
+    dG[D]_ij = sum_kl D_kl [2 d(ij|kl) - (d(ik|jl) + d(il|kj))/2]
+    (force.py:310-357).  With D symmetric, every derivative of a product of
+    functions reduces to four times the derivative of the first one, and the
+    operator derivative of the nuclear attraction follows from translational
+    invariance.  Integrals come from this oracle's C restatement over the
+    basis extended by the derivative functions; meant for small bases."""
+    bfs = build_basis(atoms, basis_data)
+    n = len(bfs)
+    atid = []
+    for ia, (z, _) in enumerate(atoms):
+        for sym, _ in basis_data[z]:
+            atid += [ia] * len(SYM2POWERS[sym])
+    ext = list(bfs)
+    dparts = {}
+    for i, bf in enumerate(bfs):
+        for x in range(3):
+            ps = _deriv_parts(bf, x)
+            dparts[i, x] = list(range(len(ext), len(ext) + len(ps)))
+            ext += ps
+    m = len(ext)
+    _, h = orc_get1ints(ext, atoms)
+    S, T = orc_get1ints(ext, [])
+    Va = [orc_get1ints(ext, [at])[1] - T for at in atoms]
+    # (p j | k l) for p in ext, j, k, l in the original basis, one contracted
+    # integral at a time (p over the derivative functions only)
+    lib = oracle_lib()
+    arr = [(len(f.pexps), _carr(f.pexps), _carr(f.pcoefs), _carr(f.pnorms), _carr(f.origin),
+            (ctypes.c_int * 3)(*f.powers)) for f in ext]
+    base = orc_get2ints(bfs)
+    I = np.empty((m, n, n, n))
+    for j in range(n):
+        for k in range(n):
+            for l in range(n):
+                for p in range(n):
+                    I[p, j, k, l] = base[ijkl2intindex(p, j, k, l)]
+    for p in range(n, m):
+        for j in range(n):
+            for k in range(n):
+                for l in range(k + 1):
+                    I[p, j, k, l] = I[p, j, l, k] = lib.orc_contr_eri(*arr[p], *arr[j], *arr[k], *arr[l])
+    Jp = np.einsum("pjkl,kl->pj", I, D)
+    Kp = np.einsum("pkjl,kl->pj", I, D)
+    grad = np.zeros((len(atoms), 3))
+    for a, (za, ra) in enumerate(atoms):
+        for x in range(3):
+            g = 0.0
+            for i in range(n):
+                dsum = lambda M: sum(M[p, :n] for p in dparts[i, x])  # noqa: E731
+                if atid[i] == a:
+                    g += 4.0 * D[i] @ dsum(h)
+                    g += 4.0 * D[i] @ (2.0 * sum(Jp[p] for p in dparts[i, x]) - sum(Kp[p] for p in dparts[i, x]))
+                    g -= 4.0 * Q[i] @ dsum(S)
+                # operator part of the attraction to nucleus a
+                g -= 4.0 * D[i] @ sum(Va[a][p, :n] for p in dparts[i, x])
+            for b, (zb, rb) in enumerate(atoms):
+                if b != a:
+                    d = np.subtract(rb, ra)
+                    g += za * zb * d[x] / np.linalg.norm(d) ** 3
+            grad[a, x] = g
+    return grad

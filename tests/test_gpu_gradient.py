@@ -92,3 +92,31 @@ def test_gradient_h2o4_631gs_config():
     assert np.abs(g - fd).max() < TOL
     em, gm, _, _ = rhf_with_gradient(mol, "6-31g*", precision="mixed", **OPTS)
     assert np.abs(gm - fd).max() < TOL
+
+
+@pytest.mark.parametrize("basis", ["sto-3g", "6-31g*"])
+def test_adjoint_kernels_vs_restated_reference_gradient(basis):
+    """pqb_grad_2e + pqb_grad_1e against the oracle's restatement of the
+    reference's analytic gradient (PyQuante/force.py:48-70,
+    AnalyticDerivatives.py): the same D and W (the oracle's converged RHF) go
+    into both, so only the integral arithmetic differs."""
+    from pyquante_b200.Basis.basis import BasisSet
+    from pyquante_b200.Basis.Tools import get_basis_data
+    from pyquante_b200.force import rhf_gradient_from_density
+    mol = geometries.perturbed(geometries.water(), 0.05, seed=1)
+    atoms = [(a.atno, tuple(a.r)) for a in mol.atoms]
+    data = get_basis_data(basis)
+    bfs = O.build_basis(atoms, data)
+    S, h = O.orc_get1ints(bfs, atoms)
+    _, orbe, orbs = O.rhf(atoms, S, h, O.orc_get2ints(bfs), 5, conv=1e-13, maxiter=300, diis=True)
+    C = orbs[:, :5]
+    D = C @ C.T
+    W = C @ np.diag(orbe[:5]) @ C.T
+    go = O.rhf_gradient(atoms, data, D, W)
+    bs = BasisSet(mol, basis)
+    eng = bs._pqb_engine if hasattr(bs, "_pqb_engine") else None
+    if eng is None:
+        from pyquante_b200.engine import BasisEngine
+        eng = BasisEngine(bs.bfs)
+    g = rhf_gradient_from_density(mol, eng, D, W, "fp64", 0.0)
+    assert np.abs(g - go).max() < 1e-9, np.abs(g - go).max()

@@ -104,3 +104,31 @@ def test_getjk_restatement_symmetry():
     D = D + D.T
     J, K = O.getJK(ints, D)
     assert np.allclose(J, J.T) and np.allclose(K, K.T)
+
+
+def test_restated_reference_gradient_matches_oracle_finite_differences():
+    """The oracle's restatement of PyQuante/force.py:48-70 (Szabo C.12,
+    derivative integrals by raising/lowering) against central differences of
+    the oracle's own RHF energy: water / STO-3G, perturbed geometry."""
+    from pyquante_b200 import geometries
+    from pyquante_b200.Basis.sto3g import basis_data as STO3G
+    mol = geometries.perturbed(geometries.water(), 0.05, seed=1)
+    atoms = [(a.atno, tuple(a.r)) for a in mol.atoms]
+
+    def scf(at):
+        bfs = O.build_basis(at, STO3G)
+        S, h = O.orc_get1ints(bfs, at)
+        return O.rhf(at, S, h, O.orc_get2ints(bfs), 5, conv=1e-13, maxiter=300, diis=True)
+
+    E, orbe, orbs = scf(atoms)
+    C = orbs[:, :5]
+    g = O.rhf_gradient(atoms, STO3G, C @ C.T, C @ np.diag(orbe[:5]) @ C.T)
+    assert np.abs(g.sum(axis=0)).max() < 1e-10        # translational invariance
+    hstep = 1e-4
+    for a, x in [(0, 0), (0, 2), (1, 1), (2, 0), (2, 2)]:
+        p = [list(r) for _, r in atoms]
+        p[a][x] += hstep
+        ep = scf([(z, tuple(r)) for (z, _), r in zip(atoms, p)])[0]
+        p[a][x] -= 2 * hstep
+        em = scf([(z, tuple(r)) for (z, _), r in zip(atoms, p)])[0]
+        assert abs(g[a, x] - (ep - em) / (2 * hstep)) < 1e-7
