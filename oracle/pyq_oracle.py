@@ -333,7 +333,10 @@ def enuke(atoms):
 
 
 def rhf(atoms, S, h, ints, nclosed, conv=1e-10, maxiter=100, diis=False):
-    """PyQuante/hartree_fock.py:66-149 (DIIS per Convergence.py:73-136)."""
+    """PyQuante/hartree_fock.py:66-149 (DIIS per Convergence.py:73-136, with a
+    subspace of the last 8 Fock matrices and no extrapolation once the
+    commutator error is at rounding level: the reference's unbounded DIIS can
+    drift off the SCF solution near convergence)."""
     en = enuke(atoms)
     orbe, orbs = geigh(h, S)
     eold = 0.0
@@ -342,10 +345,11 @@ def rhf(atoms, S, h, ints, nclosed, conv=1e-10, maxiter=100, diis=False):
     for _ in range(maxiter):
         D = orbs[:, :nclosed] @ orbs[:, :nclosed].T
         F = h + get2JmK(ints, D)
-        if diis:
-            err = (F @ D @ S - S @ D @ F).ravel()
+        err = (F @ D @ S - S @ D @ F).ravel()
+        if diis and abs(err).max() >= 1e-13:
             Fs.append(F)
             Es.append(err)
+            del Fs[:-8], Es[:-8]
             m = len(Es)
             a = np.zeros((m + 1, m + 1))
             a[:m, :m] = np.array(Es) @ np.array(Es).T

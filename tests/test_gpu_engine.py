@@ -269,6 +269,50 @@ def test_rhf_water_sto3g_energy():
     assert abs(E2 - e["water_sto3g"]) < E_TOL
 
 
+def test_rhf_reference_unit_test_energies():
+    """The reference's own SCF unit tests: He and Ne / 6-31G** (Tests/he.py:16
+    to 1e-7, Tests/ne.py:13 to 1e-4, rhf defaults) and H2 / STO-3G, 6-31G**
+    at the TestMolecules geometry (Tests/UnitSweet.py:108-126, 4 decimals).
+    He also with DIIS on, which must land on the same energy."""
+    from pyquante_b200.Molecule import Molecule
+    he = Molecule("He", [(2, (0.0, 0.0, 0.0))])
+    e, _, _ = rhf(he, ConvCriteria=1e-10, MaxIter=100)
+    assert abs(e - (-2.85516040352)) < 1e-7
+    e, _, _ = rhf(he, ConvCriteria=1e-10, MaxIter=100, DoAveraging=True)
+    assert abs(e - (-2.85516040352)) < 1e-7
+    ne = Molecule("Ne", [(10, (0.0, 0.0, 0.0))])
+    e, _, _ = rhf(ne, ConvCriteria=1e-10, MaxIter=100)
+    assert abs(e - (-128.474406)) < 1e-4
+    h2 = Molecule("H2", [(1, (0.0, 0.0, 0.36628549)), (1, (0.0, 0.0, -0.36628549))], units="Angstrom")
+    e, _, _ = rhf(h2, basis_data="sto-3g", ConvCriteria=1e-10, MaxIter=100)
+    assert round(e - (-1.117099), 4) == 0
+    e, _, _ = rhf(h2, basis_data="6-31g**", ConvCriteria=1e-10, MaxIter=100)
+    assert round(e - (-1.131334), 4) == 0
+
+
+def test_single_function_and_zero_density_edge_cases():
+    """He / STO-3G has one function and one unique integral: packed, direct
+    and stored J/K against the oracle; a zero density gives J = K = 0."""
+    from pyquante_b200.Molecule import Molecule
+    he = Molecule("He", [(2, (0.0, 0.0, 0.0))])
+    bs = BasisSet(he, "sto-3g")
+    assert len(bs) == 1
+    ints = Ints.get2ints(bs)
+    ref = O.orc_get2ints(oracle_bfs(bs))
+    assert len(ints) == 1 and abs(ints[0] - ref[0]) < ERI_TOL
+    D = np.array([[0.7]])
+    Jo, Ko = O.getJK(ref, D)
+    d = Ints.get2ints(bs, direct=True, schwarz=0.0)
+    for src in (ints, d):
+        assert abs(Ints.getJ(src, D) - Jo).max() < ERI_TOL and abs(Ints.getK(src, D) - Ko).max() < ERI_TOL
+    Z = np.zeros((1, 1))
+    assert np.all(Ints.get2JmK(d, Z) == 0.0) and np.all(Ints.get2JmK(ints, Z) == 0.0)
+    mol = geometries.water_cluster(2, seed=4)
+    d = Ints.get2ints(BasisSet(mol, "6-31g**"), direct=True)
+    Z = np.zeros((50, 50))
+    assert np.all(Ints.get2JmK(d, Z) == 0.0)
+
+
 def test_rhf_reference_test_geometries():
     """Tests/h2o.py and Tests/h2.py known answers, and the oracle to 1e-8 Eh."""
     from pyquante_b200.Molecule import Molecule
