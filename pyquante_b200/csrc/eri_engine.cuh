@@ -46,7 +46,9 @@ __device__ __forceinline__ int64_t fpair(int i, int j)
 
 // ------------------------------------------------------------ epilogues --
 // Every epilogue offers
-//   thread_quartet<LA,LB,LC,LD>(q, acc[NAB*NCD])   whole quartet, thread mode
+//   thread_quartet<LA,LB,LC,LD>(q, acc[NAB*NCD], lane, live)
+//                                                  whole quartet, thread mode (all lanes
+//                                                  of the warp call it; live = a real item)
 //   kTile                                          false: block mode calls
 //     block_ab<LA,LB,LC,LD>(q, ia, ib, acc[NCD])     per bra component pair;
 //                                                  true: block mode stores the
@@ -106,9 +108,11 @@ struct EpiPacked {
             }
     }
     template <int LA, int LB, int LC, int LD, typename R>
-    __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc) const
+    __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc, int lane, bool live) const
     {
         constexpr int NB = ncart(LB), NCD = ncart(LC) * ncart(LD);
+        (void)lane;
+        if (!live) return;
 #pragma unroll
         for (int ab = 0; ab < ncart(LA) * NB; ++ab) this->ab<LC, LD, R>(q, ab / NB, ab % NB, acc + ab * NCD);
     }
@@ -116,6 +120,44 @@ struct EpiPacked {
     __device__ __forceinline__ void block_ab(const QCtx &q, int ia, int ib, const R *acc) const
     {
         ab<LC, LD, R>(q, ia, ib, acc);
+    }
+};
+
+// Runs of equal keys over the lanes of a warp (the thread-mode item lists
+// are ordered so that neighbouring lanes often share a bra pair and a ket
+// shell): sum() is an inclusive segmented scan, so the last lane of a run
+// holds the run's total and issues one atomic for the whole run.  Every lane
+// of the warp must take part.
+struct WarpRuns {
+    unsigned f;   // bit s: lane - 2^s lies in this lane's run
+    bool last;    // last lane of its run
+    __device__ __forceinline__ WarpRuns(long long key, int lane)
+    {
+        // a run is a maximal block of consecutive lanes with one key (the
+        // same key may come back later in the warp as another run): first
+        // the lane where this lane's run starts (max-scan of run heads)
+        const long long kp = __shfl_up_sync(0xffffffffu, key, 1);
+        int start = (lane == 0 || kp != key) ? lane : 0;
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            const int o = __shfl_up_sync(0xffffffffu, start, 1 << s);
+            if (lane >= (1 << s) && o > start) start = o;
+        }
+        f = 0;
+#pragma unroll
+        for (int s = 0; s < 5; ++s)
+            if (lane - (1 << s) >= start) f |= 1u << s;
+        const long long kn = __shfl_down_sync(0xffffffffu, key, 1);
+        last = lane == 31 || kn != key;
+    }
+    __device__ __forceinline__ double sum(double x) const
+    {
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            const double y = __shfl_up_sync(0xffffffffu, x, 1 << s);
+            if ((f >> s) & 1u) x += y;
+        }
+        return x;
     }
 };
 
@@ -141,11 +183,17 @@ struct EpiJK {
     double *Jacc, *Kacc;
     static constexpr bool kTile = true;
 
+    // (called by every lane of the warp; a lane past the end of the item list
+    // passes its neighbour's quartet with zero integrals)
     template <int LA, int LB, int LC, int LD, typename R>
-    __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc) const
+    __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc, int lane, bool) const
     {
         constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NCD = NC * ND;
         const bool bd = q.sa == q.sb, kd = q.sc == q.sd, qd = q.bra == q.ket, af = q.fa > q.fb;
+        // Jacc[a,b] is shared by lanes with the same bra pair; Kacc[a,c] and
+        // Kacc[b,c] by lanes that also share the ket's first shell
+        const WarpRuns rb((long long)q.bra, lane);
+        const WarpRuns rbc(((long long)q.bra << 32) | (unsigned)q.sc, lane);
         const double *Db = D + q.bo;
         double *Jb = Jacc + q.bo, *Kb = Kacc + q.bo;
         const int64_t nm = q.nm;
@@ -178,7 +226,8 @@ struct EpiJK {
                             jab = fma(v, dcd[c][d], jab);
                             jcd[c][d] = fma(v, dab[a][b], jcd[c][d]);
                         }
-                    if (jab != 0.0) atomicAdd(Jb + (q.fa + a) * nm + q.fb + b, 2.0 * jab);
+                    const double js = rb.sum(jab);
+                    if (rb.last && js != 0.0) atomicAdd(Jb + (q.fa + a) * nm + q.fb + b, 2.0 * js);
                 }
 #pragma unroll
             for (int c = 0; c < NC; ++c)
@@ -215,8 +264,10 @@ struct EpiJK {
                             kad[d] = fma(v, dbc[b][c], kad[d]);
                         }
 #pragma unroll
-                for (int c = 0; c < NC; ++c)
-                    if (kac[c] != 0.0) atomicAdd(Kb + (q.fa + a) * nm + q.fc + c, kac[c]);
+                for (int c = 0; c < NC; ++c) {
+                    const double ks = rbc.sum(kac[c]);
+                    if (rbc.last && ks != 0.0) atomicAdd(Kb + (q.fa + a) * nm + q.fc + c, ks);
+                }
 #pragma unroll
                 for (int d = 0; d < ND; ++d)
                     if (kad[d] != 0.0) atomicAdd(Kb + (q.fa + a) * nm + q.fd + d, kad[d]);
@@ -251,8 +302,10 @@ struct EpiJK {
                             kbd[d] = fma(v, dac[a][c], kbd[d]);
                         }
 #pragma unroll
-                for (int c = 0; c < NC; ++c)
-                    if (kbc[c] != 0.0) atomicAdd(Kb + (q.fb + b) * nm + q.fc + c, kbc[c]);
+                for (int c = 0; c < NC; ++c) {
+                    const double ks = rbc.sum(kbc[c]);
+                    if (rbc.last && ks != 0.0) atomicAdd(Kb + (q.fb + b) * nm + q.fc + c, ks);
+                }
 #pragma unroll
                 for (int d = 0; d < ND; ++d)
                     if (kbd[d] != 0.0) atomicAdd(Kb + (q.fb + b) * nm + q.fd + d, kbd[d]);
@@ -362,9 +415,11 @@ struct EpiSchwarz {
         atomicMax(Q2bits + q.bra, (unsigned long long)__double_as_longlong(v));
     }
     template <int LA, int LB, int LC, int LD, typename R>
-    __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc) const
+    __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc, int lane, bool live) const
     {
         constexpr int NB = ncart(LB), NCD = ncart(LC) * ncart(LD);
+        (void)lane;
+        if (!live) return;
 #pragma unroll
         for (int ab = 0; ab < ncart(LA) * NB; ++ab) this->ab<LC, LD, R>(q, ab / NB, ab % NB, acc + ab * NCD);
     }
@@ -438,8 +493,15 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
     constexpr int NAB = NA * NB, NCD = NC * ND;
     constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
     constexpr int G2D = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
-    for (int qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += gridDim.x * blockDim.x) {
-        const int4 e = list[qi];   // bra pair, ket pair, first primitive quartet, count
+    // whole warps step through the list together (the J/K epilogue reduces
+    // over the lanes); a lane past the end repeats the last item with no
+    // primitive quartets
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * blockDim.x + threadIdx.x - lane; base < nq; base += gridDim.x * blockDim.x) {
+        const int qi = base + lane;
+        const bool live = qi < nq;
+        int4 e = list[live ? qi : nq - 1];   // bra pair, ket pair, first primitive quartet, count
+        if (!live) e.w = 0;
         const PairInfo &pb = pairs[e.x];
         const PairInfo &pk = pairs[e.y];
         const double Ax = pb.A[0], Ay = pb.A[1], Az = pb.A[2];
@@ -481,7 +543,7 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
                 ik = ik2;
             }
             const QCtx q = make_qctx(pb, pk, e.x, e.y);
-            epi.template thread_quartet<LA, LB, LC, LD, R>(q, acc);
+            epi.template thread_quartet<LA, LB, LC, LD, R>(q, acc, lane, live);
             continue;
         }
         PrimJK P = load_prim_jk(pbp + ib);
@@ -529,7 +591,7 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
             ik = ik2;
         }
         const QCtx q = make_qctx(pb, pk, e.x, e.y);
-        epi.template thread_quartet<LA, LB, LC, LD, R>(q, acc);
+        epi.template thread_quartet<LA, LB, LC, LD, R>(q, acc, lane, live);
     }
 }
 
