@@ -988,6 +988,14 @@ static void bucket_sorted(std::vector<std::vector<int4>> &cls, std::vector<int4>
         }
         std::vector<int4> sorted(v.size());
         for (auto &e : v) sorted[hist[maxp - e.w]++] = e;
+        // within one count, bra pair then ket pair: neighbouring lanes share the
+        // bra (and often the ket's first shell), so the J/K epilogue's warp
+        // runs are long
+        std::stable_sort(sorted.begin(), sorted.end(), [](const int4 &a, const int4 &b) {
+            if (a.w != b.w) return a.w > b.w;
+            if (a.x != b.x) return a.x < b.x;
+            return a.y < b.y;
+        });
         off[c] = (int64_t)flat.size();
         cnt[c] = (int64_t)sorted.size();
         flat.insert(flat.end(), sorted.begin(), sorted.end());
