@@ -181,26 +181,35 @@ struct WarpRuns {
 struct EpiJK {
     const double *D;        // pre-scaled density
     double *Jacc, *Kacc;
+    const float *Df;        // its single-precision copy (FP32 lists of the mixed mode), or null
     static constexpr bool kTile = true;
 
     // (called by every lane of the warp; a lane past the end of the item list
     // passes its neighbour's quartet with zero integrals)
+    // The per-quartet products and block sums run in the list's precision R
+    // (FP32 lists read the single-precision density); the sums over lanes and
+    // the accumulation into Jacc/Kacc are FP64.
     template <int LA, int LB, int LC, int LD, typename R>
     __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc, int lane, bool) const
     {
+        using T = R;
         constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NCD = NC * ND;
         const bool bd = q.sa == q.sb, kd = q.sc == q.sd, qd = q.bra == q.ket, af = q.fa > q.fb;
         // Jacc[a,b] is shared by lanes with the same bra pair; Kacc[a,c] and
         // Kacc[b,c] by lanes that also share the ket's first shell
         const WarpRuns rb((long long)q.bra, lane);
         const WarpRuns rbc(((long long)q.bra << 32) | (unsigned)q.sc, lane);
-        const double *Db = D + q.bo;
+        const T *Db;
+        if constexpr (std::is_same_v<T, float>)
+            Db = Df + q.bo;
+        else
+            Db = D + q.bo;
         double *Jb = Jacc + q.bo, *Kb = Kacc + q.bo;
         const int64_t nm = q.nm;
-        const double *Da = Db + q.fa * nm, *Dbr = Db + q.fb * nm, *Dc = Db + q.fc * nm;
+        const T *Da = Db + q.fa * nm, *Dbr = Db + q.fb * nm, *Dc = Db + q.fc * nm;
         // Coulomb: Jacc[a,b] and Jacc[c,d]
         {
-            double dab[NA][NB], dcd[NC][ND], jcd[NC][ND];
+            T dab[NA][NB], dcd[NC][ND], jcd[NC][ND];
 #pragma unroll
             for (int a = 0; a < NA; ++a)
 #pragma unroll
@@ -210,34 +219,34 @@ struct EpiJK {
 #pragma unroll
                 for (int d = 0; d < ND; ++d) {
                     dcd[c][d] = __ldg(Dc + c * nm + q.fd + d);
-                    jcd[c][d] = 0.0;
+                    jcd[c][d] = (T)0;
                 }
 #pragma unroll
             for (int a = 0; a < NA; ++a)
 #pragma unroll
                 for (int b = 0; b < NB; ++b) {
-                    double jab = 0.0;
+                    T jab = (T)0;
 #pragma unroll
                     for (int c = 0; c < NC; ++c)
 #pragma unroll
                         for (int d = 0; d < ND; ++d) {
-                            const double v = (double)acc[(a * NB + b) * NCD + c * ND + d] *
-                                             comp_weight(a, b, c, d, bd, kd, qd, af);
+                            const T v = (T)acc[(a * NB + b) * NCD + c * ND + d] *
+                                        (T)comp_weight(a, b, c, d, bd, kd, qd, af);
                             jab = fma(v, dcd[c][d], jab);
                             jcd[c][d] = fma(v, dab[a][b], jcd[c][d]);
                         }
-                    const double js = rb.sum(jab);
+                    const double js = rb.sum((double)jab);
                     if (rb.last && js != 0.0) atomicAdd(Jb + (q.fa + a) * nm + q.fb + b, 2.0 * js);
                 }
 #pragma unroll
             for (int c = 0; c < NC; ++c)
 #pragma unroll
                 for (int d = 0; d < ND; ++d)
-                    if (jcd[c][d] != 0.0) atomicAdd(Jb + (q.fc + c) * nm + q.fd + d, 2.0 * jcd[c][d]);
+                    if (jcd[c][d] != (T)0) atomicAdd(Jb + (q.fc + c) * nm + q.fd + d, 2.0 * (double)jcd[c][d]);
         }
         // exchange rows of the bra's first shell: Kacc[a,c] += v D_bd, Kacc[a,d] += v D_bc
         {
-            double dbd[NB][ND], dbc[NB][NC];
+            T dbd[NB][ND], dbc[NB][NC];
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
 #pragma unroll
@@ -247,35 +256,35 @@ struct EpiJK {
             }
 #pragma unroll
             for (int a = 0; a < NA; ++a) {
-                double kac[NC], kad[ND];
+                T kac[NC], kad[ND];
 #pragma unroll
-                for (int c = 0; c < NC; ++c) kac[c] = 0.0;
+                for (int c = 0; c < NC; ++c) kac[c] = (T)0;
 #pragma unroll
-                for (int d = 0; d < ND; ++d) kad[d] = 0.0;
+                for (int d = 0; d < ND; ++d) kad[d] = (T)0;
 #pragma unroll
                 for (int b = 0; b < NB; ++b)
 #pragma unroll
                     for (int c = 0; c < NC; ++c)
 #pragma unroll
                         for (int d = 0; d < ND; ++d) {
-                            const double v = (double)acc[(a * NB + b) * NCD + c * ND + d] *
-                                             comp_weight(a, b, c, d, bd, kd, qd, af);
+                            const T v = (T)acc[(a * NB + b) * NCD + c * ND + d] *
+                                        (T)comp_weight(a, b, c, d, bd, kd, qd, af);
                             kac[c] = fma(v, dbd[b][d], kac[c]);
                             kad[d] = fma(v, dbc[b][c], kad[d]);
                         }
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
-                    const double ks = rbc.sum(kac[c]);
+                    const double ks = rbc.sum((double)kac[c]);
                     if (rbc.last && ks != 0.0) atomicAdd(Kb + (q.fa + a) * nm + q.fc + c, ks);
                 }
 #pragma unroll
                 for (int d = 0; d < ND; ++d)
-                    if (kad[d] != 0.0) atomicAdd(Kb + (q.fa + a) * nm + q.fd + d, kad[d]);
+                    if (kad[d] != (T)0) atomicAdd(Kb + (q.fa + a) * nm + q.fd + d, (double)kad[d]);
             }
         }
         // exchange rows of the bra's second shell: Kacc[b,c] += v D_ad, Kacc[b,d] += v D_ac
         {
-            double dad[NA][ND], dac[NA][NC];
+            T dad[NA][ND], dac[NA][NC];
 #pragma unroll
             for (int a = 0; a < NA; ++a) {
 #pragma unroll
@@ -285,30 +294,30 @@ struct EpiJK {
             }
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
-                double kbc[NC], kbd[ND];
+                T kbc[NC], kbd[ND];
 #pragma unroll
-                for (int c = 0; c < NC; ++c) kbc[c] = 0.0;
+                for (int c = 0; c < NC; ++c) kbc[c] = (T)0;
 #pragma unroll
-                for (int d = 0; d < ND; ++d) kbd[d] = 0.0;
+                for (int d = 0; d < ND; ++d) kbd[d] = (T)0;
 #pragma unroll
                 for (int a = 0; a < NA; ++a)
 #pragma unroll
                     for (int c = 0; c < NC; ++c)
 #pragma unroll
                         for (int d = 0; d < ND; ++d) {
-                            const double v = (double)acc[(a * NB + b) * NCD + c * ND + d] *
-                                             comp_weight(a, b, c, d, bd, kd, qd, af);
+                            const T v = (T)acc[(a * NB + b) * NCD + c * ND + d] *
+                                        (T)comp_weight(a, b, c, d, bd, kd, qd, af);
                             kbc[c] = fma(v, dad[a][d], kbc[c]);
                             kbd[d] = fma(v, dac[a][c], kbd[d]);
                         }
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
-                    const double ks = rbc.sum(kbc[c]);
+                    const double ks = rbc.sum((double)kbc[c]);
                     if (rbc.last && ks != 0.0) atomicAdd(Kb + (q.fb + b) * nm + q.fc + c, ks);
                 }
 #pragma unroll
                 for (int d = 0; d < ND; ++d)
-                    if (kbd[d] != 0.0) atomicAdd(Kb + (q.fb + b) * nm + q.fd + d, kbd[d]);
+                    if (kbd[d] != (T)0) atomicAdd(Kb + (q.fb + b) * nm + q.fd + d, (double)kbd[d]);
             }
         }
     }

@@ -1,16 +1,17 @@
-// Direct J/K instantiations of the ERI engine with FP32 recurrences and
-// contraction (roots, weights and prefactors in FP64; digestion into J/K in
-// FP64).  Used only for quartets whose Schwarz bound is below the mixed-
-// precision threshold.
+// Direct J/K instantiations of the ERI engine for the FP32 lists of the mixed
+// mode (quartets whose Schwarz bound is below the threshold): integrals and
+// per-quartet digestion in single precision, large-T roots and the
+// accumulation into J/K in FP64.
 #include "eri_engine.cuh"
 #include "eri_launch.h"
 
 namespace pqb {
 cudaError_t launch_jk_f32(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
-                          const double *Dscaled, double *Jacc, double *Kacc, int n, cudaStream_t st, int nsm)
+                          const double *Dscaled, const float *Dscaled_f, double *Jacc, double *Kacc, int n,
+                          cudaStream_t st, int nsm)
 {
     (void)n;
-    EpiJK epi{Dscaled, Jacc, Kacc};
+    EpiJK epi{Dscaled, Jacc, Kacc, Dscaled_f};
     return launch_eri<float>(qc, list, nq, pairs, prims, epi, st, nsm);
 }
 }  // namespace pqb

@@ -20,7 +20,8 @@ cudaError_t launch_packed_f64(int qc, const int4 *list, int nq, const PairInfo *
 cudaError_t launch_jk_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                           const double *Dscaled, double *Jacc, double *Kacc, int n, cudaStream_t st, int nsm);
 cudaError_t launch_jk_f32(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
-                          const double *Dscaled, double *Jacc, double *Kacc, int n, cudaStream_t st, int nsm);
+                          const double *Dscaled, const float *Dscaled_f, double *Jacc, double *Kacc, int n,
+                          cudaStream_t st, int nsm);
 cudaError_t launch_schwarz_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                                unsigned long long *Q2bits, const double *fscale, cudaStream_t st, int nsm);
 cudaError_t launch_grad_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,

@@ -42,6 +42,7 @@ struct pqb_ctx {
     // is pre-scaled element-wise by escale[(i,j)] = r_i r_j (r = fscale) into
     // d_Dscaled, and J, K are scaled by the same factors when symmetrised
     double *d_escale = nullptr, *d_Dscaled = nullptr;
+    float *d_Dscaled_f = nullptr;    // single-precision copy for the FP32 lists
     unsigned long long *d_q2 = nullptr;
     std::vector<PairInfo> pairs;
     std::vector<double> Q;           // Schwarz factors (host)
@@ -143,12 +144,16 @@ __global__ void symmetrize_blocks_kernel(double *M, const long long *__restrict_
     }
 }
 
-// Y = X * S element-wise (the pre-scaled density of the direct J/K kernels).
+// Y = X * S element-wise (the pre-scaled density of the direct J/K kernels)
+// and its single-precision copy Yf.
 __global__ void scale_elements_kernel(const double *__restrict__ X, const double *__restrict__ S, double *__restrict__ Y,
-                                      int64_t len)
+                                      float *__restrict__ Yf, int64_t len)
 {
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < len; t += (int64_t)gridDim.x * blockDim.x)
-        Y[t] = X[t] * S[t];
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < len; t += (int64_t)gridDim.x * blockDim.x) {
+        const double y = X[t] * S[t];
+        Y[t] = y;
+        Yf[t] = (float)y;
+    }
 }
 
 __device__ __forceinline__ double binom_d(int n, int k)
@@ -923,8 +928,10 @@ static void release_basis(pqb_ctx *ctx)
     free_dev(ctx->d_fscale);
     free_dev(ctx->d_escale);
     free_dev(ctx->d_Dscaled);
+    free_dev(ctx->d_Dscaled_f);
     ctx->d_escale = nullptr;
     ctx->d_Dscaled = nullptr;
+    ctx->d_Dscaled_f = nullptr;
     free_dev(ctx->d_q2);
     free_dev(ctx->d_full);
     free_dev(ctx->d_diag);
@@ -1142,6 +1149,7 @@ int pqb_shells_upload_batch(pqb_ctx *ctx, int nmol, const int *mol_shell_off, in
         }
         PQB_CK(ctx, cudaMalloc(&ctx->d_escale, sizeof(double) * std::max<size_t>(es.size(), 1)));
         PQB_CK(ctx, cudaMalloc(&ctx->d_Dscaled, sizeof(double) * std::max<size_t>(es.size(), 1)));
+        PQB_CK(ctx, cudaMalloc(&ctx->d_Dscaled_f, sizeof(float) * std::max<size_t>(es.size(), 1)));
         PQB_CK(ctx, cudaMemcpy(ctx->d_escale, es.data(), sizeof(double) * es.size(), cudaMemcpyHostToDevice));
     }
     // unscreened quartet list (packed integrals) and diagonal list (Schwarz)
@@ -1399,7 +1407,8 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
     const int n = ctx->nbf;
     PQB_CK(ctx, cudaMemsetAsync(J, 0, sizeof(double) * ctx->dense_len, st));
     PQB_CK(ctx, cudaMemsetAsync(K, 0, sizeof(double) * ctx->dense_len, st));
-    scale_elements_kernel<<<ctx->nsm * 4, 256, 0, st>>>(D, ctx->d_escale, ctx->d_Dscaled, ctx->dense_len);
+    scale_elements_kernel<<<ctx->nsm * 4, 256, 0, st>>>(D, ctx->d_escale, ctx->d_Dscaled, ctx->d_Dscaled_f,
+                                                         ctx->dense_len);
     const double *Ds = ctx->d_Dscaled;
     PQB_CK(ctx, ensure_streams(ctx));
     // fork: class launches spread over the context's streams, heaviest first
@@ -1423,7 +1432,7 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
         cudaStream_t sk = ctx->streams[k++ % ctx->nstreams];
         const int4 *list = ctx->d_plan + ctx->plan_off[part][c];
         if (part == 1 && mode == PQB_MIXED)
-            PQB_CK(ctx, launch_jk_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, J, K, n, sk, ctx->nsm));
+            PQB_CK(ctx, launch_jk_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, ctx->d_Dscaled_f, J, K, n, sk, ctx->nsm));
         else
             PQB_CK(ctx, launch_jk_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, J, K, n, sk, ctx->nsm));
     }
@@ -1461,10 +1470,11 @@ int pqb_jk_direct_class(pqb_ctx *ctx, const double *D, double *Jacc, double *Kac
     cudaStream_t st = (cudaStream_t)stream;
     const int4 *list = ctx->d_plan + ctx->plan_off[part][qclass];
     const int nq = (int)ctx->plan_cnt[part][qclass];
-    scale_elements_kernel<<<ctx->nsm * 4, 256, 0, st>>>(D, ctx->d_escale, ctx->d_Dscaled, ctx->dense_len);
+    scale_elements_kernel<<<ctx->nsm * 4, 256, 0, st>>>(D, ctx->d_escale, ctx->d_Dscaled, ctx->d_Dscaled_f,
+                                                         ctx->dense_len);
     if (mode == PQB_MIXED && part == 1)
-        PQB_CK(ctx, launch_jk_f32(qclass, list, nq, ctx->d_pairs, ctx->d_prims, ctx->d_Dscaled, Jacc, Kacc, ctx->nbf,
-                                  st, ctx->nsm));
+        PQB_CK(ctx, launch_jk_f32(qclass, list, nq, ctx->d_pairs, ctx->d_prims, ctx->d_Dscaled, ctx->d_Dscaled_f, Jacc,
+                                  Kacc, ctx->nbf, st, ctx->nsm));
     else
         PQB_CK(ctx, launch_jk_f64(qclass, list, nq, ctx->d_pairs, ctx->d_prims, ctx->d_Dscaled, Jacc, Kacc, ctx->nbf,
                                   st, ctx->nsm));
