@@ -975,40 +975,45 @@ int pqb_last_error(const pqb_ctx *ctx, char *buf, size_t len)
 
 int pqb_num_pairs(const pqb_ctx *ctx) { return ctx ? (int)ctx->pairs.size() : 0; }
 
-// Bucket work items by class, each class sorted by descending primitive-
-// quartet count (block-mode kernels advance their items in lockstep over
-// primitive quartets; thread-mode warps then get similar trip counts).
+// Bucket work items by class.  Within a class the items go by descending
+// primitive-quartet count (block-mode kernels advance their items in lockstep
+// over primitive quartets; thread-mode warps get similar trip counts), then by
+// bra pair, then in generation order (ket pair ascending), so neighbouring
+// lanes share the bra and often the ket's first shell and the J/K epilogue's
+// warp runs are long.  Two stable counting sorts (bra pair, then count) keep
+// this linear in the number of items, which reaches 5e8 for batched bases.
 static void bucket_sorted(std::vector<std::vector<int4>> &cls, std::vector<int4> &flat, int64_t *off, int64_t *cnt)
 {
     flat.clear();
     for (int c = 0; c < kNumQuartetClass; ++c) {
         auto &v = cls[c];
-        int maxp = 1;
-        for (auto &e : v) maxp = std::max(maxp, e.w);
+        int maxp = 1, maxbra = 0;
+        for (auto &e : v) {
+            maxp = std::max(maxp, e.w);
+            maxbra = std::max(maxbra, e.x);
+        }
+        std::vector<int4> bybra(v.size());
+        {
+            std::vector<int64_t> hist((size_t)maxbra + 2, 0);
+            for (auto &e : v) hist[e.x + 1]++;
+            for (size_t k = 1; k < hist.size(); ++k) hist[k] += hist[k - 1];
+            for (auto &e : v) bybra[hist[e.x]++] = e;
+        }
         std::vector<int64_t> hist(maxp + 2, 0);
-        for (auto &e : v) hist[maxp - e.w]++;
+        for (auto &e : bybra) hist[maxp - e.w]++;
         int64_t s = 0;
         for (auto &h : hist) {
             int64_t t = h;
             h = s;
             s += t;
         }
-        std::vector<int4> sorted(v.size());
-        for (auto &e : v) sorted[hist[maxp - e.w]++] = e;
-        // within one count, bra pair then ket pair: neighbouring lanes share the
-        // bra (and often the ket's first shell), so the J/K epilogue's warp
-        // runs are long
-        std::stable_sort(sorted.begin(), sorted.end(), [](const int4 &a, const int4 &b) {
-            if (a.w != b.w) return a.w > b.w;
-            if (a.x != b.x) return a.x < b.x;
-            return a.y < b.y;
-        });
         off[c] = (int64_t)flat.size();
-        cnt[c] = (int64_t)sorted.size();
-        flat.insert(flat.end(), sorted.begin(), sorted.end());
+        cnt[c] = (int64_t)v.size();
+        flat.resize(flat.size() + v.size());
+        int4 *dst = flat.data() + off[c];
+        for (auto &e : bybra) dst[hist[maxp - e.w]++] = e;
     }
 }
-
 
 static inline int4 oriented_quartet(const std::vector<PairInfo> &pairs, int p, int q, int &qc)
 {
