@@ -9,6 +9,8 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #define PQB_TABQ static __device__ const
@@ -663,7 +665,7 @@ __global__ void jk_packed_kernel(const double *__restrict__ ints, const double *
 //   Kacc[j,l] += v' D_ik     register rows accJ[q][m]
 //   Kacc[j,k] += v' D_il     warp sum per segment, added to column k of accJ
 // The register rows go to Kacc once per CTA (accI summed over the warps).
-constexpr int kRgWarps = 8, kRgRPW = 2, kRgRows = kRgWarps * kRgRPW, kRgPrefetch = 2;
+constexpr int kRgWarps = 8, kRgRPW = 2, kRgRows = kRgWarps * kRgRPW, kRgPrefetch = 3;
 
 __device__ __forceinline__ double warp_sum(double x)
 {
@@ -683,6 +685,153 @@ __device__ __forceinline__ void prefetch_l2(const double *p, int len)
                      : "memory");
 }
 
+// Per-warp state of a tile: the warp's rows j (q = 0 .. kRgRPW-1), the row
+// weights wq (1/2 on the diagonal row j = i, 0 past i) and the register rows.
+// The weights wq are applied to the row constants and, for accJ and jrow,
+// once at the end, so the per-integral loop multiplies only the column
+// weights (1/2 at l = k, and at kl = ij in the last segment).
+template <int MAXM> struct RgRows {
+    const double *rowp[kRgRPW], *Djp[kRgRPW];
+    int jq[kRgRPW];
+    bool okq[kRgRPW];
+    double Dij2[kRgRPW], wq[kRgRPW], jrow[kRgRPW], accJ[kRgRPW][MAXM], accI[MAXM];
+};
+
+template <int... Is, class F>
+__device__ __forceinline__ void rg_static_for(std::integer_sequence<int, Is...>, F &&f)
+{
+    (f(std::integral_constant<int, Is>{}), ...);
+}
+
+// Jacc[k, l] for l <= k from the CTA's per-warp column partials of one
+// segment (one barrier per segment; the partials are double-buffered).
+__device__ __forceinline__ void rg_column_sums(const double *jcb, int stride, double *Jacc, int n, int k)
+{
+    __syncthreads();
+    for (int l = threadIdx.x; l <= k; l += kRgWarps * 32) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kRgWarps; ++w) s += jcb[w * stride + l];
+        if (s != 0.0) atomicAdd(Jacc + (int64_t)k * n + l, s);
+    }
+}
+
+// Segment k (< i) of the warp's rows, k in [32 KB, 32 KB + 31]: the chunk
+// count KB + 1 and the register slot KB of column k are compile-time, so the
+// register rows stay in registers and the segment sums are plain adds.
+template <int MAXM, int KB>
+__device__ __forceinline__ void rg_segment(RgRows<MAXM> &r, const double *__restrict__ D, const double *Di,
+                                           double *jcw, int n, int i, int k, int lane)
+{
+    const int KL0 = k * (k + 1) / 2;
+    const double *Dk = D + (int64_t)k * n;
+    const double Dik = __ldg(Di + k);
+    double Djk[kRgRPW], kik[kRgRPW], kjk[kRgRPW];
+#pragma unroll
+    for (int q = 0; q < kRgRPW; ++q) {
+        Djk[q] = r.wq[q] * __ldg(r.Djp[q] + k);
+        kik[q] = 0.0;
+        kjk[q] = 0.0;
+    }
+#pragma unroll
+    for (int m = 0; m <= KB; ++m) {
+        const int l = 32 * m + lane;
+        const bool inseg = m < KB || l <= k;
+        const double Dkl = inseg ? __ldg(Dk + l) : 0.0;
+        const double Dil = inseg ? __ldg(Di + l) : 0.0;
+        double jcol = 0.0;
+#pragma unroll
+        for (int q = 0; q < kRgRPW; ++q) {
+            const bool ok = r.okq[q] && inseg;
+            double v = ok ? __ldg(r.rowp[q] + KL0 + l) : 0.0;
+            const double Djl = ok ? __ldg(r.Djp[q] + l) : 0.0;
+            if (m == KB && l == k) v *= 0.5;
+            r.jrow[q] = fma(v, Dkl, r.jrow[q]);
+            jcol = fma(v, r.Dij2[q], jcol);
+            kik[q] = fma(v, Djl, kik[q]);
+            r.accI[m] = fma(v, Djk[q], r.accI[m]);
+            kjk[q] = fma(v, Dil, kjk[q]);
+            r.accJ[q][m] = fma(v, Dik, r.accJ[q][m]);
+        }
+        jcw[l] = jcol;
+    }
+    double ki = 0.0;
+#pragma unroll
+    for (int q = 0; q < kRgRPW; ++q) ki = fma(r.wq[q], kik[q], ki);
+    const double sk = warp_sum(ki);
+    double sj[kRgRPW];
+#pragma unroll
+    for (int q = 0; q < kRgRPW; ++q) sj[q] = warp_sum(kjk[q]);
+    if (lane == (k & 31)) {
+        r.accI[KB] += sk;
+#pragma unroll
+        for (int q = 0; q < kRgRPW; ++q) r.accJ[q][KB] += sj[q];
+    }
+}
+
+// The last segment k = i: row (i, j) holds kl <= (i, j), so only l <= j,
+// with weight 1/2 at kl = ij.  Runs once per tile; the slot of column k is
+// a run-time index here.
+template <int MAXM>
+__device__ __forceinline__ void rg_last_segment(RgRows<MAXM> &r, const double *__restrict__ D, const double *Di,
+                                                double *jcw, int n, int i, int lane)
+{
+    const int k = i, KL0 = k * (k + 1) / 2;
+    const double *Dk = D + (int64_t)k * n;
+    const double Dik = __ldg(Di + k);
+    double Djk[kRgRPW], kik[kRgRPW], kjk[kRgRPW];
+    int lmax[kRgRPW];
+#pragma unroll
+    for (int q = 0; q < kRgRPW; ++q) {
+        Djk[q] = r.wq[q] * __ldg(r.Djp[q] + k);
+        kik[q] = 0.0;
+        kjk[q] = 0.0;
+        lmax[q] = r.okq[q] ? r.jq[q] : -1;   // rows past i load nothing
+    }
+#pragma unroll
+    for (int m = 0; m < MAXM; ++m) {
+        if (32 * m > k) continue;   // warp-uniform: chunks past the segment are skipped
+        const int l = 32 * m + lane;
+        const bool inseg = l <= k;
+        const double Dkl = inseg ? __ldg(Dk + l) : 0.0;
+        const double Dil = inseg ? __ldg(Di + l) : 0.0;
+        const double wkl = l == k ? 0.5 : 1.0;
+        double jcol = 0.0;
+#pragma unroll
+        for (int q = 0; q < kRgRPW; ++q) {
+            const bool ok = l <= lmax[q];
+            double v = ok ? __ldg(r.rowp[q] + KL0 + l) : 0.0;
+            const double Djl = ok ? __ldg(r.Djp[q] + l) : 0.0;
+            v *= wkl * (l == r.jq[q] ? 0.5 : 1.0);
+            r.jrow[q] = fma(v, Dkl, r.jrow[q]);
+            jcol = fma(v, r.Dij2[q], jcol);
+            kik[q] = fma(v, Djl, kik[q]);
+            r.accI[m] = fma(v, Djk[q], r.accI[m]);
+            kjk[q] = fma(v, Dil, kjk[q]);
+            r.accJ[q][m] = fma(v, Dik, r.accJ[q][m]);
+        }
+        jcw[l] = jcol;
+    }
+    double ki = 0.0;
+#pragma unroll
+    for (int q = 0; q < kRgRPW; ++q) ki = fma(r.wq[q], kik[q], ki);
+    const double sk = warp_sum(ki);
+    double sj[kRgRPW];
+#pragma unroll
+    for (int q = 0; q < kRgRPW; ++q) sj[q] = warp_sum(kjk[q]);
+    // (as multiply-adds by a 0/1 factor: a conditional add with a run-time
+    // slot would let the compiler turn the unrolled rows into an indexed,
+    // memory-resident array)
+    const int kslot = lane == (k & 31) ? (k >> 5) : -1;
+#pragma unroll
+    for (int m = 0; m < MAXM; ++m) {
+        const double f = m == kslot ? 1.0 : 0.0;
+        r.accI[m] = fma(f, sk, r.accI[m]);
+#pragma unroll
+        for (int q = 0; q < kRgRPW; ++q) r.accJ[q][m] = fma(f, sj[q], r.accJ[q][m]);
+    }
+}
+
 template <int MAXM>
 __global__ void __launch_bounds__(kRgWarps * 32) jk_packed_reg_kernel(const double *__restrict__ ints,
                                                                       const double *__restrict__ D, double *Jacc,
@@ -692,128 +841,78 @@ __global__ void __launch_bounds__(kRgWarps * 32) jk_packed_reg_kernel(const doub
     // column partials of a segment, double-buffered: jc[2][kRgWarps][MAXM * 32];
     // per-warp rows i, summed at the end: kis[kRgWarps][MAXM * 32]
     extern __shared__ double rg_smem[];
-    double(*jc)[kRgWarps][MAXM * 32] = reinterpret_cast<double(*)[kRgWarps][MAXM * 32]>(rg_smem);
-    double(*kis)[MAXM * 32] = reinterpret_cast<double(*)[MAXM * 32]>(rg_smem + 2 * kRgWarps * MAXM * 32);
+    constexpr int kStride = MAXM * 32;
+    double *jc = rg_smem;
+    double(*kis)[kStride] = reinterpret_cast<double(*)[kStride]>(rg_smem + 2 * kRgWarps * kStride);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int i = tiles[t].x, j0 = tiles[t].y;
         const int64_t I0 = (int64_t)i * (i + 1) / 2;
         const double *Di = D + (int64_t)i * n;
-        const double *rowp[kRgRPW], *Djp[kRgRPW];
-        int jq[kRgRPW];
-        bool okq[kRgRPW];
-        double Dij2[kRgRPW], wq[kRgRPW], jrow[kRgRPW], accJ[kRgRPW][MAXM], accI[MAXM];
+        RgRows<MAXM> r;
 #pragma unroll
         for (int q = 0; q < kRgRPW; ++q) {
             const int j = j0 + warp + kRgWarps * q;
-            okq[q] = j <= i;
-            jq[q] = okq[q] ? j : i;
-            const int64_t IJ = I0 + jq[q];
-            rowp[q] = ints + IJ * (IJ + 1) / 2;
-            Djp[q] = D + (int64_t)jq[q] * n;
-            Dij2[q] = okq[q] ? 2.0 * __ldg(Di + jq[q]) : 0.0;
-            wq[q] = okq[q] ? (i == jq[q] ? 0.5 : 1.0) : 0.0;   // rows past i contribute nothing
-            jrow[q] = 0.0;
+            r.okq[q] = j <= i;
+            r.jq[q] = r.okq[q] ? j : i;
+            const int64_t IJ = I0 + r.jq[q];
+            r.rowp[q] = ints + IJ * (IJ + 1) / 2;
+            r.Djp[q] = D + (int64_t)r.jq[q] * n;
+            r.wq[q] = r.okq[q] ? (i == r.jq[q] ? 0.5 : 1.0) : 0.0;   // rows past i contribute nothing
+            r.Dij2[q] = 2.0 * r.wq[q] * __ldg(Di + r.jq[q]);
+            r.jrow[q] = 0.0;
 #pragma unroll
-            for (int m = 0; m < MAXM; ++m) accJ[q][m] = 0.0;
+            for (int m = 0; m < MAXM; ++m) r.accJ[q][m] = 0.0;
         }
 #pragma unroll
-        for (int m = 0; m < MAXM; ++m) accI[m] = 0.0;
+        for (int m = 0; m < MAXM; ++m) r.accI[m] = 0.0;
+        // lane q < kRgRPW prefetches row q: segment kk of it into L2
+        const double *pf_row = r.rowp[0];
+        bool pf_ok = r.okq[0];
+        int pf_j = r.jq[0];
+#pragma unroll
+        for (int q = 1; q < kRgRPW; ++q)
+            if (lane == q) pf_row = r.rowp[q], pf_ok = r.okq[q], pf_j = r.jq[q];
+        pf_ok = pf_ok && lane < kRgRPW;
+        if (pf_ok)
+            for (int kk = 0; kk < kRgPrefetch && kk <= i; ++kk)
+                prefetch_l2(pf_row + kk * (kk + 1) / 2, kk < i ? kk + 1 : pf_j + 1);
         int buf = 0;
-        // the first kRgPrefetch segments of the warp's rows are requested from L2 up front
-        if (lane < kRgRPW) {
-            const double *rp = lane == 0 ? rowp[0] : rowp[kRgRPW - 1];
-            const bool okr = lane == 0 ? okq[0] : okq[kRgRPW - 1];
-            const int jr = lane == 0 ? jq[0] : jq[kRgRPW - 1];
-            for (int kk = 0; kk < kRgPrefetch && kk <= i && okr; ++kk)
-                prefetch_l2(rp + kk * (kk + 1) / 2, kk < i ? kk + 1 : jr + 1);
-        }
-        for (int k = 0; k <= i; ++k) {
-            const int KL0 = k * (k + 1) / 2;
-            const double *Dk = D + (int64_t)k * n;
-            const double Dik = __ldg(Di + k);
-            const bool last = k == i;   // row (i, j) holds kl <= (i, j): only l <= j in segment i
-            // segment k + kRgPrefetch of the warp's rows: one bulk L2 prefetch per row
-            if (lane < kRgRPW && k + kRgPrefetch <= i) {
-                const int kk = k + kRgPrefetch;
-                const double *rp = lane == 0 ? rowp[0] : rowp[kRgRPW - 1];
-                const bool okr = lane == 0 ? okq[0] : okq[kRgRPW - 1];
-                const int jr = lane == 0 ? jq[0] : jq[kRgRPW - 1];
-                if (okr) prefetch_l2(rp + kk * (kk + 1) / 2, kk < i ? kk + 1 : jr + 1);
-            }
-            double Djk[kRgRPW], kjk[kRgRPW];
-            int lmax[kRgRPW];
-#pragma unroll
-            for (int q = 0; q < kRgRPW; ++q) {
-                Djk[q] = __ldg(Djp[q] + k);
-                kjk[q] = 0.0;
-                lmax[q] = !okq[q] ? -1 : (last ? jq[q] : k);   // rows past i load nothing
-            }
-            double kik = 0.0;
-#pragma unroll
-            for (int m = 0; m < MAXM; ++m) {
-                if (32 * m > k) continue;   // warp-uniform: chunks past the segment are skipped
-                const int l = 32 * m + lane;
-                const bool inseg = l <= k;
-                const double Dkl = inseg ? __ldg(Dk + l) : 0.0;
-                const double Dil = inseg ? __ldg(Di + l) : 0.0;
-                const double wkl = l == k ? 0.5 : 1.0;
-                double jcol = 0.0;
-#pragma unroll
-                for (int q = 0; q < kRgRPW; ++q) {
-                    const bool ok = l <= lmax[q];
-                    double v = ok ? __ldg(rowp[q] + KL0 + l) : 0.0;
-                    const double Djl = ok ? __ldg(Djp[q] + l) : 0.0;
-                    v *= wq[q] * wkl * ((last && l == jq[q]) ? 0.5 : 1.0);
-                    jrow[q] = fma(v, Dkl, jrow[q]);
-                    jcol = fma(v, Dij2[q], jcol);
-                    kik = fma(v, Djl, kik);
-                    accI[m] = fma(v, Djk[q], accI[m]);
-                    kjk[q] = fma(v, Dil, kjk[q]);
-                    accJ[q][m] = fma(v, Dik, accJ[q][m]);
+        rg_static_for(std::make_integer_sequence<int, MAXM>{}, [&](auto kbc) {
+            constexpr int KB = decltype(kbc)::value;
+            if (32 * KB >= i) return;
+            const int kend = min(32 * KB + 31, i - 1);
+            for (int k = 32 * KB; k <= kend; ++k) {
+                if (pf_ok && k + kRgPrefetch <= i) {
+                    const int kk = k + kRgPrefetch;
+                    prefetch_l2(pf_row + kk * (kk + 1) / 2, kk < i ? kk + 1 : pf_j + 1);
                 }
-                jc[buf][warp][l] = jcol;
+                double *jcb = jc + buf * kRgWarps * kStride;
+                rg_segment<MAXM, KB>(r, D, Di, jcb + warp * kStride, n, i, k, lane);
+                rg_column_sums(jcb, kStride, Jacc, n, k);
+                buf ^= 1;
             }
-            // segment sums Kacc[i,k], Kacc[j,k] go to column k (lane k % 32, slot k / 32)
-            const double sk = warp_sum(kik);
-            double sj[kRgRPW];
-#pragma unroll
-            for (int q = 0; q < kRgRPW; ++q) sj[q] = warp_sum(kjk[q]);
-            // (as multiply-adds by a 0/1 factor: a conditional add here would
-            // let the compiler turn the unrolled slots back into an indexed,
-            // memory-resident array)
-            const int kslot = lane == (k & 31) ? (k >> 5) : -1;
-#pragma unroll
-            for (int m = 0; m < MAXM; ++m) {
-                const double f = m == kslot ? 1.0 : 0.0;
-                accI[m] = fma(f, sk, accI[m]);
-#pragma unroll
-                for (int q = 0; q < kRgRPW; ++q) accJ[q][m] = fma(f, sj[q], accJ[q][m]);
-            }
-            __syncthreads();
-            // Jacc[k, l] for l <= k: warps split the columns
-            for (int l = threadIdx.x; l <= k; l += kRgWarps * 32) {
-                double s = 0.0;
-#pragma unroll
-                for (int w = 0; w < kRgWarps; ++w) s += jc[buf][w][l];
-                if (s != 0.0) atomicAdd(Jacc + (int64_t)k * n + l, s);
-            }
-            buf ^= 1;
+        });
+        {
+            double *jcb = jc + buf * kRgWarps * kStride;
+            rg_last_segment<MAXM>(r, D, Di, jcb + warp * kStride, n, i, lane);
+            rg_column_sums(jcb, kStride, Jacc, n, i);
         }
 #pragma unroll
         for (int q = 0; q < kRgRPW; ++q) {
-            const double x = warp_sum(jrow[q]);
-            if (lane == 0 && okq[q] && x != 0.0) atomicAdd(Jacc + (int64_t)i * n + jq[q], 2.0 * x);
+            const double x = warp_sum(r.jrow[q]);
+            if (lane == 0 && r.okq[q] && x != 0.0) atomicAdd(Jacc + (int64_t)i * n + r.jq[q], 2.0 * r.wq[q] * x);
         }
         // rows j of Kacc from registers; row i summed over the warps
 #pragma unroll
         for (int m = 0; m < MAXM; ++m) {
             const int c = 32 * m + lane;
-            kis[warp][c] = accI[m];
+            kis[warp][c] = r.accI[m];
             if (c <= i) {
 #pragma unroll
                 for (int q = 0; q < kRgRPW; ++q)
-                    if (okq[q] && accJ[q][m] != 0.0) atomicAdd(Kacc + (int64_t)jq[q] * n + c, accJ[q][m]);
+                    if (r.okq[q] && r.accJ[q][m] != 0.0)
+                        atomicAdd(Kacc + (int64_t)r.jq[q] * n + c, r.wq[q] * r.accJ[q][m]);
             }
         }
         __syncthreads();
@@ -825,6 +924,18 @@ __global__ void __launch_bounds__(kRgWarps * 32) jk_packed_reg_kernel(const doub
         }
         __syncthreads();
     }
+}
+
+template <int MAXM>
+static cudaError_t launch_packed_reg(const double *ints, const double *D, double *J, double *K, int nbf,
+                                     const int2 *tiles, int ntiles, int grid, cudaStream_t st)
+{
+    const size_t smem = sizeof(double) * 3 * kRgWarps * MAXM * 32;
+    cudaError_t e = cudaFuncSetAttribute(jk_packed_reg_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    jk_packed_reg_kernel<MAXM><<<grid, kRgWarps * 32, smem, st>>>(ints, D, J, K, nbf, tiles, ntiles);
+    return cudaGetLastError();
 }
 
 __global__ void boys_eval_kernel(int m, int count, const double *T, double *F)
@@ -1512,17 +1623,18 @@ int pqb_jk_packed(pqb_ctx *ctx, const double *ints, int64_t len, const double *D
         }
         int grid = ctx->pk_tiles_n;
         if (grid > ctx->nsm * 16) grid = ctx->nsm * 16;
-        const int maxm = nbf <= 256 ? 8 : 16;
-        const size_t rsm = sizeof(double) * 3 * kRgWarps * maxm * 32;
-        if (maxm == 8) {
-            PQB_CK(ctx, cudaFuncSetAttribute(jk_packed_reg_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm));
-            jk_packed_reg_kernel<8><<<grid, kRgWarps * 32, rsm, st>>>(ints, D, J, K, nbf, ctx->d_pk_tiles,
-                                                                      ctx->pk_tiles_n);
-        } else {
-            PQB_CK(ctx, cudaFuncSetAttribute(jk_packed_reg_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm));
-            jk_packed_reg_kernel<16><<<grid, kRgWarps * 32, rsm, st>>>(ints, D, J, K, nbf, ctx->d_pk_tiles,
-                                                                       ctx->pk_tiles_n);
-        }
+        // register rows sized to the column count: 32 * MAXM >= nbf
+        const int need = (nbf + 31) / 32;
+        const int2 *tl = ctx->d_pk_tiles;
+        const int nt = ctx->pk_tiles_n;
+        if (need <= 2) PQB_CK(ctx, launch_packed_reg<2>(ints, D, J, K, nbf, tl, nt, grid, st));
+        else if (need <= 4) PQB_CK(ctx, launch_packed_reg<4>(ints, D, J, K, nbf, tl, nt, grid, st));
+        else if (need <= 6) PQB_CK(ctx, launch_packed_reg<6>(ints, D, J, K, nbf, tl, nt, grid, st));
+        else if (need <= 7) PQB_CK(ctx, launch_packed_reg<7>(ints, D, J, K, nbf, tl, nt, grid, st));
+        else if (need <= 8) PQB_CK(ctx, launch_packed_reg<8>(ints, D, J, K, nbf, tl, nt, grid, st));
+        else if (need <= 10) PQB_CK(ctx, launch_packed_reg<10>(ints, D, J, K, nbf, tl, nt, grid, st));
+        else if (need <= 12) PQB_CK(ctx, launch_packed_reg<12>(ints, D, J, K, nbf, tl, nt, grid, st));
+        else PQB_CK(ctx, launch_packed_reg<16>(ints, D, J, K, nbf, tl, nt, grid, st));
     } else {
         // one block per packed row (nbf > 512: the packed array alone is then over 69 GB)
         jk_packed_kernel<<<(unsigned)P, 256, 0, st>>>(ints, D, J, K, nbf);

@@ -245,6 +245,31 @@ def test_stored_jk_kernels_agree_with_oracle_and_direct():
     torch.cuda.empty_cache()
 
 
+@pytest.mark.parametrize("n", [50, 100, 180, 210, 256, 300, 380, 420])
+def test_stored_register_kernel_every_row_width(n):
+    """pqb_jk_packed's register kernel is instantiated for 2, 4, 6, 7, 8, 10,
+    12 and 16 column chunks of 32 (the smallest that holds N); each width, on
+    seeded random packed values (any packed array is a valid 8-fold
+    symmetric tensor), against the one-block-per-row kernel."""
+    from pyquante_b200.engine import jk_packed
+    P = n * (n + 1) // 2
+    g = torch.Generator(device="cuda").manual_seed(n)
+    ints = torch.rand(P * (P + 1) // 2, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    Dt = torch.as_tensor(_rand_density(n, n), device="cuda")
+    ctx = _lib.Context(torch.cuda.current_device())
+    out = []
+    for simple in (1, 0):
+        ctx.check(ctx.lib.pqb_set_param(ctx.h, _lib.PQB_PARAM_PACKED_KERNEL, 0, simple))
+        out.append(jk_packed(ints, Dt, ctx))
+    (Js, Ks), (Jr, Kr) = out
+    scale = float(Dt.abs().sum())
+    assert float((Jr - Js).abs().max()) < 1e-12 * scale * n
+    assert float((Kr - Ks).abs().max()) < 1e-12 * scale * n
+    assert torch.equal(Jr, Jr.T) and torch.equal(Kr, Kr.T)
+    del ints
+    torch.cuda.empty_cache()
+
+
 def test_jk_mixed_precision_error_is_small():
     mol = geometries.water_cluster(3, seed=2)
     bs = BasisSet(mol, "6-31g**")
