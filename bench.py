@@ -243,7 +243,7 @@ def run_stored(a):
                                    "frac": gbs / peak, "traffic": STORED_TRAFFIC_BYTES, "peak_source": src,
                                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
                                                      "profiles/jk_packed_reg_h2o8_631gss.md",
-                                   "kernel": "jk_packed_reg_kernel<8>"}}))
+                                   "kernel": "jk_packed_reg_kernel<7>"}}))
 
 def run_c16h34(a):
     """C16H34 / 6-31G* (N = 308): FP64 vs mixed Fock build and SCF energy for

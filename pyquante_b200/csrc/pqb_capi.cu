@@ -661,11 +661,16 @@ __global__ void jk_packed_kernel(const double *__restrict__ ints, const double *
 //   Jacc[k,l] += 2 v' D_ij   per-warp partials in shared memory, summed
 //                            over the CTA's rows once per segment
 //   Kacc[i,l] += v' D_jk     register row accI[m] (lane-owned columns)
-//   Kacc[i,k] += v' D_jl     warp sum per segment, added to column k of accI
+//   Kacc[i,k] += v' D_jl     per-segment partials over 8 lane groups, parked
+//                            in a shared ring and folded into column k of
+//                            accI once per 32-segment block
 //   Kacc[j,l] += v' D_ik     register rows accJ[q][m]
-//   Kacc[j,k] += v' D_il     warp sum per segment, added to column k of accJ
+//   Kacc[j,k] += v' D_il     the same, into column k of accJ
 // The register rows go to Kacc once per CTA (accI summed over the warps).
 constexpr int kRgWarps = 8, kRgRPW = 2, kRgRows = kRgWarps * kRgRPW, kRgPrefetch = 3;
+// segment-sum ring: kRgNv values (row i, rows j_q) x 8 partials x 32 columns,
+// rows padded to 33 so that the eight writers hit distinct banks
+constexpr int kRgNv = 1 + kRgRPW, kRgRingPitch = 33, kRgRing = kRgNv * 8 * kRgRingPitch;
 
 __device__ __forceinline__ double warp_sum(double x)
 {
@@ -721,7 +726,7 @@ __device__ __forceinline__ void rg_column_sums(const double *jcb, int stride, do
 // register rows stay in registers and the segment sums are plain adds.
 template <int MAXM, int KB>
 __device__ __forceinline__ void rg_segment(RgRows<MAXM> &r, const double *__restrict__ D, const double *Di,
-                                           double *jcw, int n, int i, int k, int lane)
+                                           double *jcw, double *ring, int n, int i, int k, int lane)
 {
     const int KL0 = k * (k + 1) / 2;
     const double *Dk = D + (int64_t)k * n;
@@ -755,18 +760,46 @@ __device__ __forceinline__ void rg_segment(RgRows<MAXM> &r, const double *__rest
         }
         jcw[l] = jcol;
     }
-    double ki = 0.0;
+    // the segment sums Kacc[i,k] (value 0) and Kacc[j_q,k] (value 1 + q):
+    // two butterfly levels leave lane p < 8 with the sum over lanes p + 8 t,
+    // parked in the warp's ring until the 32-segment block is folded
+    double sv[kRgNv];
+    sv[0] = 0.0;
 #pragma unroll
-    for (int q = 0; q < kRgRPW; ++q) ki = fma(r.wq[q], kik[q], ki);
-    const double sk = warp_sum(ki);
-    double sj[kRgRPW];
-#pragma unroll
-    for (int q = 0; q < kRgRPW; ++q) sj[q] = warp_sum(kjk[q]);
-    if (lane == (k & 31)) {
-        r.accI[KB] += sk;
-#pragma unroll
-        for (int q = 0; q < kRgRPW; ++q) r.accJ[q][KB] += sj[q];
+    for (int q = 0; q < kRgRPW; ++q) {
+        sv[0] = fma(r.wq[q], kik[q], sv[0]);
+        sv[1 + q] = kjk[q];
     }
+#pragma unroll
+    for (int v = 0; v < kRgNv; ++v) {
+        sv[v] += __shfl_xor_sync(0xffffffffu, sv[v], 16);
+        sv[v] += __shfl_xor_sync(0xffffffffu, sv[v], 8);
+    }
+    if (lane < 8) {
+#pragma unroll
+        for (int v = 0; v < kRgNv; ++v) ring[(v * 8 + lane) * kRgRingPitch + (k & 31)] = sv[v];
+    }
+}
+
+// Fold a finished 32-segment block KB out of the ring: lane c adds the eight
+// partials of column 32 KB + c to its register slot KB (compile-time).
+template <int MAXM, int KB>
+__device__ __forceinline__ void rg_fold_block(RgRows<MAXM> &r, const double *ring, int kend, int lane)
+{
+    __syncwarp();
+    if (32 * KB + lane <= kend) {
+        double s[kRgNv];
+#pragma unroll
+        for (int v = 0; v < kRgNv; ++v) {
+            s[v] = 0.0;
+#pragma unroll
+            for (int p = 0; p < 8; ++p) s[v] += ring[(v * 8 + p) * kRgRingPitch + lane];
+        }
+        r.accI[KB] += s[0];
+#pragma unroll
+        for (int q = 0; q < kRgRPW; ++q) r.accJ[q][KB] += s[1 + q];
+    }
+    __syncwarp();
 }
 
 // The last segment k = i: row (i, j) holds kl <= (i, j), so only l <= j,
@@ -845,6 +878,8 @@ __global__ void __launch_bounds__(kRgWarps * 32) jk_packed_reg_kernel(const doub
     double *jc = rg_smem;
     double(*kis)[kStride] = reinterpret_cast<double(*)[kStride]>(rg_smem + 2 * kRgWarps * kStride);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // per-warp ring of segment-sum partials: [value][partial p][column k % 32]
+    double *ring = rg_smem + 3 * kRgWarps * kStride + warp * kRgRing;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int i = tiles[t].x, j0 = tiles[t].y;
         const int64_t I0 = (int64_t)i * (i + 1) / 2;
@@ -888,10 +923,11 @@ __global__ void __launch_bounds__(kRgWarps * 32) jk_packed_reg_kernel(const doub
                     prefetch_l2(pf_row + kk * (kk + 1) / 2, kk < i ? kk + 1 : pf_j + 1);
                 }
                 double *jcb = jc + buf * kRgWarps * kStride;
-                rg_segment<MAXM, KB>(r, D, Di, jcb + warp * kStride, n, i, k, lane);
+                rg_segment<MAXM, KB>(r, D, Di, jcb + warp * kStride, ring, n, i, k, lane);
                 rg_column_sums(jcb, kStride, Jacc, n, k);
                 buf ^= 1;
             }
+            rg_fold_block<MAXM, KB>(r, ring, kend, lane);
         });
         {
             double *jcb = jc + buf * kRgWarps * kStride;
@@ -930,7 +966,7 @@ template <int MAXM>
 static cudaError_t launch_packed_reg(const double *ints, const double *D, double *J, double *K, int nbf,
                                      const int2 *tiles, int ntiles, int grid, cudaStream_t st)
 {
-    const size_t smem = sizeof(double) * 3 * kRgWarps * MAXM * 32;
+    const size_t smem = sizeof(double) * (3 * kRgWarps * MAXM * 32 + kRgWarps * kRgRing);
     cudaError_t e = cudaFuncSetAttribute(jk_packed_reg_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
