@@ -99,8 +99,13 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
  * angular momentum first, the default); PQB_PARAM_PACKED_KERNEL = the
  * stored-integral J/K kernel of pqb_jk_packed (0 automatic: the register
  * form for nbf <= 512, one block per packed row above; 1 always the latter,
- * so tests can compare the two). */
-enum { PQB_PARAM_CHUNK = 0, PQB_PARAM_STREAMS = 1, PQB_PARAM_ORDER = 2, PQB_PARAM_PACKED_KERNEL = 3 };
+ * so tests can compare the two); PQB_PARAM_GRAPH = 1 (default) lets
+ * pqb_jk_direct replay a CUDA graph of its class launches, captured on the
+ * second call per mode into context-owned accumulators and rebuilt after any
+ * change of basis, plan or parameter (single-molecule bases, callers not
+ * capturing a graph themselves); 0 launches the classes one by one. */
+enum { PQB_PARAM_CHUNK = 0, PQB_PARAM_STREAMS = 1, PQB_PARAM_ORDER = 2, PQB_PARAM_PACKED_KERNEL = 3,
+       PQB_PARAM_GRAPH = 4 };
 int pqb_set_param(pqb_ctx *ctx, int param, int qclass, int value);
 
 /* Per-class statistics of the current plan, arrays of 2*21 int64 indexed

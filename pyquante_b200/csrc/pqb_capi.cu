@@ -81,6 +81,14 @@ struct pqb_ctx {
     cudaStream_t streams[kStreams] = {nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[kStreams] = {nullptr};
     bool have_plan = false;
+    // pqb_jk_direct replays a captured graph of the class launches (one per
+    // mode), accumulating into ctx-owned J/K; rebuilt after any change of
+    // basis, plan or launch parameters
+    bool use_graph = true;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    bool graph_warm[2] = {false, false};   // one eager build first (one-time launch setup stays out of the capture)
+    double *d_Jacc = nullptr, *d_Kacc = nullptr;
     // small scratch
     double *d_atoms = nullptr;
     size_t atoms_cap = 0;
@@ -124,6 +132,22 @@ __global__ void symmetrize_kernel(double *M, int n, const double *__restrict__ S
     while ((int64_t)(i + 1) * (i + 2) / 2 <= t) ++i;
     int j = (int)(t - (int64_t)i * (i + 1) / 2);
     double s = M[(int64_t)i * n + j] + M[(int64_t)j * n + i];
+    if (S) s *= S[(int64_t)i * n + j];
+    M[(int64_t)i * n + j] = s;
+    M[(int64_t)j * n + i] = s;
+}
+
+// symmetrize_kernel from the accumulator A into M (every element of M written)
+__global__ void symmetrize_into_kernel(const double *__restrict__ A, double *M, int n, const double *__restrict__ S)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t P = (int64_t)n * (n + 1) / 2;
+    if (t >= P) return;
+    int i = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((int64_t)i * (i + 1) / 2 > t) --i;
+    while ((int64_t)(i + 1) * (i + 2) / 2 <= t) ++i;
+    int j = (int)(t - (int64_t)i * (i + 1) / 2);
+    double s = A[(int64_t)i * n + j] + A[(int64_t)j * n + i];
     if (S) s *= S[(int64_t)i * n + j];
     M[(int64_t)i * n + j] = s;
     M[(int64_t)j * n + i] = s;
@@ -668,9 +692,10 @@ __global__ void jk_packed_kernel(const double *__restrict__ ints, const double *
 //   Kacc[j,k] += v' D_il     the same, into column k of accJ
 // The register rows go to Kacc once per CTA (accI summed over the warps).
 constexpr int kRgWarps = 8, kRgRPW = 2, kRgRows = kRgWarps * kRgRPW, kRgPrefetch = 3;
-// segment-sum ring: kRgNv values (row i, rows j_q) x 8 partials x 32 columns,
-// rows padded to 33 so that the eight writers hit distinct banks
-constexpr int kRgNv = 1 + kRgRPW, kRgRingPitch = 33, kRgRing = kRgNv * 8 * kRgRingPitch;
+// segment-sum ring: kRgNv values (row i, rows j_q) x kRgParts partials x 32
+// columns, rows padded to 33 so that the writers hit distinct banks
+constexpr int kRgParts = 8;
+constexpr int kRgNv = 1 + kRgRPW, kRgRingPitch = 33, kRgRing = kRgNv * kRgParts * kRgRingPitch;
 
 __device__ __forceinline__ double warp_sum(double x)
 {
@@ -761,8 +786,9 @@ __device__ __forceinline__ void rg_segment(RgRows<MAXM> &r, const double *__rest
         jcw[l] = jcol;
     }
     // the segment sums Kacc[i,k] (value 0) and Kacc[j_q,k] (value 1 + q):
-    // two butterfly levels leave lane p < 8 with the sum over lanes p + 8 t,
-    // parked in the warp's ring until the 32-segment block is folded
+    // butterfly levels down to kRgParts leave lane p < kRgParts with the sum
+    // over lanes p + kRgParts t, parked in the warp's ring until the
+    // 32-segment block is folded
     double sv[kRgNv];
     sv[0] = 0.0;
 #pragma unroll
@@ -771,17 +797,16 @@ __device__ __forceinline__ void rg_segment(RgRows<MAXM> &r, const double *__rest
         sv[1 + q] = kjk[q];
     }
 #pragma unroll
-    for (int v = 0; v < kRgNv; ++v) {
-        sv[v] += __shfl_xor_sync(0xffffffffu, sv[v], 16);
-        sv[v] += __shfl_xor_sync(0xffffffffu, sv[v], 8);
-    }
-    if (lane < 8) {
+    for (int v = 0; v < kRgNv; ++v)
 #pragma unroll
-        for (int v = 0; v < kRgNv; ++v) ring[(v * 8 + lane) * kRgRingPitch + (k & 31)] = sv[v];
+        for (int o = 16; o >= kRgParts; o >>= 1) sv[v] += __shfl_xor_sync(0xffffffffu, sv[v], o);
+    if (lane < kRgParts) {
+#pragma unroll
+        for (int v = 0; v < kRgNv; ++v) ring[(v * kRgParts + lane) * kRgRingPitch + (k & 31)] = sv[v];
     }
 }
 
-// Fold a finished 32-segment block KB out of the ring: lane c adds the eight
+// Fold a finished 32-segment block KB out of the ring: lane c adds the kRgParts
 // partials of column 32 KB + c to its register slot KB (compile-time).
 template <int MAXM, int KB>
 __device__ __forceinline__ void rg_fold_block(RgRows<MAXM> &r, const double *ring, int kend, int lane)
@@ -793,7 +818,7 @@ __device__ __forceinline__ void rg_fold_block(RgRows<MAXM> &r, const double *rin
         for (int v = 0; v < kRgNv; ++v) {
             s[v] = 0.0;
 #pragma unroll
-            for (int p = 0; p < 8; ++p) s[v] += ring[(v * 8 + p) * kRgRingPitch + lane];
+            for (int p = 0; p < kRgParts; ++p) s[v] += ring[(v * kRgParts + p) * kRgRingPitch + lane];
         }
         r.accI[KB] += s[0];
 #pragma unroll
@@ -1068,8 +1093,21 @@ static cudaError_t ensure_streams(pqb_ctx *ctx)
     return cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
 }
 
+static void drop_graphs(pqb_ctx *ctx)
+{
+    for (int gi = 0; gi < 2; ++gi) {
+        if (ctx->graph_exec[gi]) cudaGraphExecDestroy(ctx->graph_exec[gi]);
+        ctx->graph_exec[gi] = nullptr;
+        ctx->graph_warm[gi] = false;
+    }
+}
+
 static void release_basis(pqb_ctx *ctx)
 {
+    drop_graphs(ctx);
+    free_dev(ctx->d_Jacc);
+    free_dev(ctx->d_Kacc);
+    ctx->d_Jacc = ctx->d_Kacc = nullptr;
     free_dev(ctx->d_pairs);
     free_dev(ctx->d_prims);
     free_dev(ctx->d_fscale);
@@ -1110,6 +1148,7 @@ void pqb_destroy(pqb_ctx *ctx)
         if (ctx->ev_join[k]) cudaEventDestroy(ctx->ev_join[k]);
     }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     delete ctx;
 }
 
@@ -1369,6 +1408,7 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
             for (int s0 = 0; s0 < e.w; s0 += ch) dst.push_back(make_int4(e.x, e.y, s0, std::min(ch, e.w - s0)));
         }
     }
+    drop_graphs(ctx);
     std::vector<int4> f64, f32;
     bucket_sorted(c64, f64, ctx->plan_off[0], ctx->plan_cnt[0]);
     bucket_sorted(c32, f32, ctx->plan_off[1], ctx->plan_cnt[1]);
@@ -1405,6 +1445,7 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
 int pqb_set_param(pqb_ctx *ctx, int param, int qclass, int value)
 {
     if (!ctx) return PQB_E_ARG;
+    drop_graphs(ctx);
     switch (param) {
     case PQB_PARAM_CHUNK:
         if (value < 1 || value > 4096) return fail(ctx, PQB_E_ARG, "chunk %d out of range 1..4096", value);
@@ -1429,6 +1470,10 @@ int pqb_set_param(pqb_ctx *ctx, int param, int qclass, int value)
         if (value < 0 || value > 1) return fail(ctx, PQB_E_ARG, "packed kernel %d out of range", value);
         ctx->packed_simple = value == 1;
         return PQB_OK;
+    case PQB_PARAM_GRAPH:
+        if (value < 0 || value > 1) return fail(ctx, PQB_E_ARG, "graph %d out of range", value);
+        ctx->use_graph = value == 1;
+        return PQB_OK;
     }
     return fail(ctx, PQB_E_ARG, "unknown parameter %d", param);
 }
@@ -1451,6 +1496,7 @@ int pqb_plan_shard(pqb_ctx *ctx, int rank, int nranks)
     if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_plan_shard: call pqb_plan first");
     if (nranks == 1) return PQB_OK;
     PQB_CK(ctx, cudaSetDevice(ctx->device));
+    drop_graphs(ctx);
     const size_t total = ctx->plan_h.size();
     std::vector<int4> out;
     out.reserve(total / nranks + 64);
@@ -1549,20 +1595,15 @@ int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
     return PQB_OK;
 }
 
-int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode, void *stream)
+// The class launches of one build into the accumulators Jacc, Kacc (zeroed
+// here) on stream st, forked over the context's streams and joined back;
+// they read the scaled density in d_Dscaled / d_Dscaled_f.
+static int launch_build(pqb_ctx *ctx, double *Jacc, double *Kacc, int mode, cudaStream_t st)
 {
-    if (!ctx || !D || !J || !K) return fail(ctx, PQB_E_ARG, "pqb_jk_direct: bad arguments");
-    if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_jk_direct: call pqb_plan first");
-    if (mode != PQB_FP64 && mode != PQB_MIXED) return fail(ctx, PQB_E_ARG, "pqb_jk_direct: mode %d", mode);
-    PQB_CK(ctx, cudaSetDevice(ctx->device));
-    cudaStream_t st = (cudaStream_t)stream;
     const int n = ctx->nbf;
-    PQB_CK(ctx, cudaMemsetAsync(J, 0, sizeof(double) * ctx->dense_len, st));
-    PQB_CK(ctx, cudaMemsetAsync(K, 0, sizeof(double) * ctx->dense_len, st));
-    scale_elements_kernel<<<ctx->nsm * 4, 256, 0, st>>>(D, ctx->d_escale, ctx->d_Dscaled, ctx->d_Dscaled_f,
-                                                         ctx->dense_len);
+    PQB_CK(ctx, cudaMemsetAsync(Jacc, 0, sizeof(double) * ctx->dense_len, st));
+    PQB_CK(ctx, cudaMemsetAsync(Kacc, 0, sizeof(double) * ctx->dense_len, st));
     const double *Ds = ctx->d_Dscaled;
-    PQB_CK(ctx, ensure_streams(ctx));
     // fork: class launches spread over the context's streams, heaviest first
     PQB_CK(ctx, cudaEventRecord(ctx->ev_fork, st));
     for (int k = 0; k < pqb_ctx::kStreams; ++k) PQB_CK(ctx, cudaStreamWaitEvent(ctx->streams[k], ctx->ev_fork, 0));
@@ -1584,17 +1625,76 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
         cudaStream_t sk = ctx->streams[k++ % ctx->nstreams];
         const int4 *list = ctx->d_plan + ctx->plan_off[part][c];
         if (part == 1 && mode == PQB_MIXED)
-            PQB_CK(ctx, launch_jk_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, ctx->d_Dscaled_f, J, K, n, sk, ctx->nsm));
+            PQB_CK(ctx, launch_jk_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, ctx->d_Dscaled_f, Jacc, Kacc, n, sk,
+                                      ctx->nsm));
         else
-            PQB_CK(ctx, launch_jk_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, J, K, n, sk, ctx->nsm));
+            PQB_CK(ctx, launch_jk_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, Jacc, Kacc, n, sk, ctx->nsm));
     }
     // join
     for (int k = 0; k < pqb_ctx::kStreams; ++k) {
         PQB_CK(ctx, cudaEventRecord(ctx->ev_join[k], ctx->streams[k]));
         PQB_CK(ctx, cudaStreamWaitEvent(st, ctx->ev_join[k], 0));
     }
+    return PQB_OK;
+}
+
+// Capture launch_build into the ctx-owned accumulators as a graph for mode
+// (index gi), once; later builds replay it with one launch.
+static int ensure_build_graph(pqb_ctx *ctx, int mode, int gi)
+{
+    if (ctx->graph_exec[gi]) return PQB_OK;
+    if (!ctx->cap_stream) PQB_CK(ctx, cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+    if (!ctx->d_Jacc) {
+        PQB_CK(ctx, cudaMalloc(&ctx->d_Jacc, sizeof(double) * std::max<long long>(ctx->dense_len, 1)));
+        PQB_CK(ctx, cudaMalloc(&ctx->d_Kacc, sizeof(double) * std::max<long long>(ctx->dense_len, 1)));
+    }
+    PQB_CK(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = launch_build(ctx, ctx->d_Jacc, ctx->d_Kacc, mode, ctx->cap_stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->cap_stream, &g);   // always ends the capture
+    if (rc != PQB_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return rc != PQB_OK ? rc : fail(ctx, PQB_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&ctx->graph_exec[gi], g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        ctx->graph_exec[gi] = nullptr;
+        return fail(ctx, PQB_E_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
+    }
+    return PQB_OK;
+}
+
+int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode, void *stream)
+{
+    if (!ctx || !D || !J || !K) return fail(ctx, PQB_E_ARG, "pqb_jk_direct: bad arguments");
+    if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_jk_direct: call pqb_plan first");
+    if (mode != PQB_FP64 && mode != PQB_MIXED) return fail(ctx, PQB_E_ARG, "pqb_jk_direct: mode %d", mode);
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const int n = ctx->nbf;
+    PQB_CK(ctx, ensure_streams(ctx));
+    scale_elements_kernel<<<ctx->nsm * 4, 256, 0, st>>>(D, ctx->d_escale, ctx->d_Dscaled, ctx->d_Dscaled_f,
+                                                         ctx->dense_len);
+    const int64_t P = (int64_t)n * (n + 1) / 2;
+    // graph replay for a single molecule when the caller is not capturing
+    // (a caller's own capture records the launches themselves)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PQB_CK(ctx, cudaStreamIsCapturing(st, &cs));
+    const int gi = mode == PQB_MIXED ? 1 : 0;
+    if (ctx->use_graph && ctx->nmol == 1 && cs == cudaStreamCaptureStatusNone && ctx->graph_warm[gi]) {
+        const int rc = ensure_build_graph(ctx, mode, gi);
+        if (rc != PQB_OK) return rc;
+        PQB_CK(ctx, cudaGraphLaunch(ctx->graph_exec[gi], st));
+        symmetrize_into_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(ctx->d_Jacc, J, n, ctx->d_escale);
+        symmetrize_into_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(ctx->d_Kacc, K, n, ctx->d_escale);
+        PQB_CK(ctx, cudaGetLastError());
+        return PQB_OK;
+    }
+    const int rc = launch_build(ctx, J, K, mode, st);
+    if (rc != PQB_OK) return rc;
+    if (cs == cudaStreamCaptureStatusNone) ctx->graph_warm[gi] = true;
     if (ctx->nmol == 1) {
-        const int64_t P = (int64_t)n * (n + 1) / 2;
         symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, n, ctx->d_escale);
         symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K, n, ctx->d_escale);
     } else {

@@ -270,6 +270,38 @@ def test_stored_register_kernel_every_row_width(n):
     torch.cuda.empty_cache()
 
 
+def test_direct_build_graph_replay_matches_launches():
+    """pqb_jk_direct replays a captured CUDA graph of its class launches from
+    the second call per mode on; replays, one-by-one launches and a re-plan
+    (which drops and recaptures the graph) give the same J and K."""
+    mol = geometries.water_cluster(3, seed=2)
+    bs = BasisSet(mol, "6-31g**")
+    eng = BasisEngine(bs.bfs)
+    D = torch.as_tensor(_rand_density(len(bs), 5), device="cuda")
+    for mode in ("fp64", "mixed"):
+        runs = {}
+        for graph in (0, 1):
+            eng.ctx.check(eng.ctx.lib.pqb_set_param(eng.ctx.h, _lib.PQB_PARAM_GRAPH, 0, graph))
+            # first call launches one by one, the second captures and replays, the third replays
+            runs[graph] = [tuple(x.clone() for x in eng.jk(D, mode, 1e-12, 1e-5)) for _ in range(3)]
+        J0, K0 = runs[0][0]
+        scale = float(J0.abs().max())
+        for graph in (0, 1):
+            for J, K in runs[graph]:
+                assert float((J - J0).abs().max()) < 1e-13 * scale
+                assert float((K - K0).abs().max()) < 1e-13 * scale
+        # a different plan: the graph is rebuilt for it
+        eng.ctx.check(eng.ctx.lib.pqb_set_param(eng.ctx.h, _lib.PQB_PARAM_GRAPH, 0, 1))
+        Jl, Kl = eng.jk(D, mode, 1e-7, 1e-5)
+        Jr, Kr = eng.jk(D, mode, 1e-7, 1e-5)
+        eng.ctx.check(eng.ctx.lib.pqb_set_param(eng.ctx.h, _lib.PQB_PARAM_GRAPH, 0, 0))
+        Je, Ke = eng.jk(D, mode, 1e-7, 1e-5)
+        assert float((Jr - Je).abs().max()) < 1e-13 * scale and float((Kr - Ke).abs().max()) < 1e-13 * scale
+        assert float((Jl - Je).abs().max()) < 1e-13 * scale
+        assert float((Je - J0).abs().max()) > 0.0   # the looser plan really differs
+    eng.ctx.check(eng.ctx.lib.pqb_set_param(eng.ctx.h, _lib.PQB_PARAM_GRAPH, 0, 1))
+
+
 def test_jk_mixed_precision_error_is_small():
     mol = geometries.water_cluster(3, seed=2)
     bs = BasisSet(mol, "6-31g**")
