@@ -37,7 +37,7 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on these workloads:
 # one stored-integral J/K launch (profiles/jk_packed_reg_h2o8_631gss.md) and the 34 class
 # launches of one FP64 direct build captured there (profiles/eri_jk_direct_h2o8_631gss.md, section 2)
-STORED_TRAFFIC_BYTES = 1620087000 + 4919296
+STORED_TRAFFIC_BYTES = 1620658000 + 5230080
 DIRECT_TRAFFIC_BYTES = 46173184
 
 
