@@ -20,7 +20,8 @@ multi-stream J/K launches, F and E of every bucket) is captured once in a
 CUDA graph and replayed; DIIS and the eigensolves run eagerly per bucket.
 A molecule is converged when its energy changes by less than ``conv`` (its
 SCF time is the time of that iteration); converged molecules keep their
-last solution.
+last solution, and from the next iteration on their DIIS step and
+eigensolve (torch runs one eigensolve per molecule) are skipped.
 """
 import ctypes
 import time
@@ -138,9 +139,12 @@ class _Bucket:
         self.E = torch.zeros(B, **f64)
         self.Fs, self.Es = [], []
 
-    def solve(self, Fm):
-        e, V = torch.linalg.eigh(self.X.transpose(1, 2) @ Fm @ self.X + self.shift)
-        return self.X @ V
+    def solve(self, Fm, ia=None):
+        """Orbitals of the Fock matrices Fm (all molecules of the bucket, or
+        the positions ia)."""
+        X, shift = (self.X, self.shift) if ia is None else (self.X.index_select(0, ia), self.shift.index_select(0, ia))
+        e, V = torch.linalg.eigh(X.transpose(1, 2) @ Fm @ X + shift)
+        return X @ V
 
 
 def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, graph=True, schwarz=1e-12,
@@ -209,6 +213,11 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
             fock_build()
         for q, bk in enumerate(buckets):
             nb, Bb = bk.nb, len(bk.idx)
+            # molecules converged in earlier iterations keep their orbitals: the
+            # eigensolves (one per molecule) run for the others only
+            act = ~done[bk.idx]
+            if not act.any():
+                continue
             err = bk.F @ bk.D @ bk.S - bk.S @ bk.D @ bk.F
             err = torch.where(bk.padmask, torch.zeros_like(err), err)
             bk.Fs.append(bk.F.clone())
@@ -230,10 +239,13 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
             c = torch.where((info == 0)[:, None], c, torch.nn.functional.one_hot(
                 torch.full((Bb,), k - 1, device=dev), k + 1).to(torch.float64))
             Fd = (c[:, :k, None, None] * torch.stack(bk.Fs, dim=1)).sum(dim=1)
-            Cn = bk.solve(Fd)
+            if act.all():
+                bk.C.copy_(bk.solve(Fd))
+            else:
+                ia = torch.from_numpy(np.nonzero(act)[0]).to(dev)
+                bk.C.index_copy_(0, ia, bk.solve(Fd.index_select(0, ia), ia))
             energy = bk.E.clone()
             newly = (~bdone[q]) & ((energy - eold[q]).abs() < conv)
-            bk.C.copy_(torch.where(bdone[q][:, None, None], bk.C, Cn))
             eold[q] = torch.where(bdone[q], eold[q], energy)
             bdone[q] = bdone[q] | newly
         flags = [(bd.cpu().numpy(), e.cpu().numpy()) for bd, e in zip(bdone, eold)]
