@@ -103,9 +103,13 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
  * pqb_jk_direct replay a CUDA graph of its class launches, captured on the
  * second call per mode into context-owned accumulators and rebuilt after any
  * change of basis, plan or parameter (single-molecule bases, callers not
- * capturing a graph themselves); 0 launches the classes one by one. */
+ * capturing a graph themselves); 0 launches the classes one by one;
+ * PQB_PARAM_THREADS = host threads that pqb_plan enumerates and orders the
+ * quartets on (0, the default: all hardware threads up to 32 once a plan
+ * has 4M shell quartets or more, else 1); the plan is the same for any
+ * count. */
 enum { PQB_PARAM_CHUNK = 0, PQB_PARAM_STREAMS = 1, PQB_PARAM_ORDER = 2, PQB_PARAM_PACKED_KERNEL = 3,
-       PQB_PARAM_GRAPH = 4 };
+       PQB_PARAM_GRAPH = 4, PQB_PARAM_THREADS = 5 };
 int pqb_set_param(pqb_ctx *ctx, int param, int qclass, int value);
 
 /* Per-class statistics of the current plan, arrays of 2*21 int64 indexed

@@ -14,7 +14,8 @@ LIB_PATH = os.path.join(_HERE, "libpyquante_b200.so")
 PQB_OK, PQB_E_ARG, PQB_E_CLASS, PQB_E_NPRIM, PQB_E_SHAPE, PQB_E_CUDA, PQB_E_STATE, PQB_E_TIMEOUT, PQB_E_NOMEM = range(9)
 PQB_FP64, PQB_MIXED = 0, 1
 PQB_ENGINE_RYS, PQB_ENGINE_HGP = 0, 1
-PQB_PARAM_CHUNK, PQB_PARAM_STREAMS, PQB_PARAM_ORDER, PQB_PARAM_PACKED_KERNEL, PQB_PARAM_GRAPH = 0, 1, 2, 3, 4
+(PQB_PARAM_CHUNK, PQB_PARAM_STREAMS, PQB_PARAM_ORDER, PQB_PARAM_PACKED_KERNEL, PQB_PARAM_GRAPH,
+ PQB_PARAM_THREADS) = 0, 1, 2, 3, 4, 5
 
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _c_dbl_p = ctypes.POINTER(ctypes.c_double)

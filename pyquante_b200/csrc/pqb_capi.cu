@@ -3,12 +3,14 @@
 // class-templated (general-L scalar ERIs by Rys and by Head-Gordon--Pople,
 // one-electron integrals, stored-integral J/K, Boys/Rys probes).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <utility>
 #include <vector>
@@ -85,6 +87,7 @@ struct pqb_ctx {
     // mode), accumulating into ctx-owned J/K; rebuilt after any change of
     // basis, plan or launch parameters
     bool use_graph = true;
+    int plan_threads = 0;            // host threads of pqb_plan (0: automatic)
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
     bool graph_warm[2] = {false, false};   // one eager build first (one-time launch setup stays out of the capture)
@@ -1054,6 +1057,29 @@ __global__ void finalize_q_kernel(const unsigned long long *q2, double *Q, int n
 
 static inline int64_t pair_idx64(int64_t i, int64_t j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
 
+// Run f(0) .. f(n - 1) on up to nthreads threads (tasks handed out in order).
+template <class F> static void run_tasks(int n, int nthreads, F f)
+{
+    nthreads = std::max(1, std::min(nthreads, n));
+    if (nthreads == 1) {
+        for (int i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; ++t)
+        pool.emplace_back([&] {
+            for (int i = next++; i < n; i = next++) f(i);
+        });
+    for (auto &th : pool) th.join();
+}
+
+static int host_threads()
+{
+    const unsigned hw = std::thread::hardware_concurrency();
+    return (int)std::min(32u, std::max(1u, hw));
+}
+
 extern "C" {
 
 int pqb_version(void) { return 1; }
@@ -1168,36 +1194,48 @@ int pqb_num_pairs(const pqb_ctx *ctx) { return ctx ? (int)ctx->pairs.size() : 0;
 // lanes share the bra and often the ket's first shell and the J/K epilogue's
 // warp runs are long.  Two stable counting sorts (bra pair, then count) keep
 // this linear in the number of items, which reaches 5e8 for batched bases.
+// The items of one class, given as segments in generation order, into dst
+// ordered by descending count, then bra pair, then generation order.
+static void order_class_items(const std::vector<const std::vector<int4> *> &segs, int4 *dst)
+{
+    size_t n = 0;
+    int maxp = 1, maxbra = 0;
+    for (auto *v : segs) {
+        n += v->size();
+        for (auto &e : *v) {
+            maxp = std::max(maxp, e.w);
+            maxbra = std::max(maxbra, e.x);
+        }
+    }
+    if (n == 0) return;
+    std::vector<int4> bybra(n);
+    {
+        std::vector<int64_t> hist((size_t)maxbra + 2, 0);
+        for (auto *v : segs)
+            for (auto &e : *v) hist[e.x + 1]++;
+        for (size_t k = 1; k < hist.size(); ++k) hist[k] += hist[k - 1];
+        for (auto *v : segs)
+            for (auto &e : *v) bybra[hist[e.x]++] = e;
+    }
+    std::vector<int64_t> hist(maxp + 2, 0);
+    for (auto &e : bybra) hist[maxp - e.w]++;
+    int64_t s = 0;
+    for (auto &h : hist) {
+        int64_t t = h;
+        h = s;
+        s += t;
+    }
+    for (auto &e : bybra) dst[hist[maxp - e.w]++] = e;
+}
+
 static void bucket_sorted(std::vector<std::vector<int4>> &cls, std::vector<int4> &flat, int64_t *off, int64_t *cnt)
 {
     flat.clear();
     for (int c = 0; c < kNumQuartetClass; ++c) {
-        auto &v = cls[c];
-        int maxp = 1, maxbra = 0;
-        for (auto &e : v) {
-            maxp = std::max(maxp, e.w);
-            maxbra = std::max(maxbra, e.x);
-        }
-        std::vector<int4> bybra(v.size());
-        {
-            std::vector<int64_t> hist((size_t)maxbra + 2, 0);
-            for (auto &e : v) hist[e.x + 1]++;
-            for (size_t k = 1; k < hist.size(); ++k) hist[k] += hist[k - 1];
-            for (auto &e : v) bybra[hist[e.x]++] = e;
-        }
-        std::vector<int64_t> hist(maxp + 2, 0);
-        for (auto &e : bybra) hist[maxp - e.w]++;
-        int64_t s = 0;
-        for (auto &h : hist) {
-            int64_t t = h;
-            h = s;
-            s += t;
-        }
         off[c] = (int64_t)flat.size();
-        cnt[c] = (int64_t)v.size();
-        flat.resize(flat.size() + v.size());
-        int4 *dst = flat.data() + off[c];
-        for (auto &e : bybra) dst[hist[maxp - e.w]++] = e;
+        cnt[c] = (int64_t)cls[c].size();
+        flat.resize(flat.size() + cls[c].size());
+        order_class_items({&cls[c]}, flat.data() + off[c]);
     }
 }
 
@@ -1390,53 +1428,94 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
     const auto &pairs = ctx->pairs;
     const auto &Q = ctx->Q;
     const int np = (int)pairs.size();
-    std::vector<std::vector<int4>> c64(kNumQuartetClass), c32(kNumQuartetClass);
-    int64_t total = 0, dropped = 0;
-    for (int p = 0; p < np; ++p) {
-        const int q0 = ctx->pair_first[p];
-        total += p - q0 + 1;
-        for (int q = q0; q <= p; ++q) {
-            const double b = Q[p] * Q[q];
-            if (b < schwarz_thresh) {
-                ++dropped;
-                continue;
+    // Enumeration: the bra pairs split into ranges of about equal quartet
+    // counts, one per host thread; each range keeps its own per-class lists
+    // in generation order, so the ranges in order are the sequential lists.
+    std::vector<int64_t> cum(np + 1, 0);
+    for (int p = 0; p < np; ++p) cum[p + 1] = cum[p] + (p - ctx->pair_first[p] + 1);
+    const int64_t total = cum[np];
+    const int T = ctx->plan_threads > 0 ? (int)std::min<int64_t>(ctx->plan_threads, std::max<int64_t>(np, 1))
+                                        : (total < (int64_t)1 << 22 ? 1 : host_threads());
+    std::vector<int> pb(T + 1, np);
+    pb[0] = 0;
+    for (int t = 1; t < T; ++t)
+        pb[t] = std::max(pb[t - 1], (int)(std::lower_bound(cum.begin(), cum.end(), total * t / T) - cum.begin()));
+    struct Range {
+        std::vector<int4> items[2][kNumQuartetClass];
+        int64_t prims[2][kNumQuartetClass] = {{0}};
+        int64_t dropped = 0;
+    };
+    std::vector<Range> rg(T);
+    run_tasks(T, T, [&](int t) {
+        Range &r = rg[t];
+        for (int p = pb[t]; p < pb[t + 1]; ++p) {
+            const int q0 = ctx->pair_first[p];
+            for (int q = q0; q <= p; ++q) {
+                const double b = Q[p] * Q[q];
+                if (b < schwarz_thresh) {
+                    ++r.dropped;
+                    continue;
+                }
+                int qc;
+                int4 e = oriented_quartet(pairs, p, q, qc);
+                const int part = b < fp32_thresh ? 1 : 0;
+                auto &dst = r.items[part][qc];
+                const int ch = ctx->chunk[qc];
+                for (int s0 = 0; s0 < e.w; s0 += ch) dst.push_back(make_int4(e.x, e.y, s0, std::min(ch, e.w - s0)));
+                r.prims[part][qc] += e.w;
             }
-            int qc;
-            int4 e = oriented_quartet(pairs, p, q, qc);
-            auto &dst = (b < fp32_thresh ? c32 : c64)[qc];
-            const int ch = ctx->chunk[qc];
-            for (int s0 = 0; s0 < e.w; s0 += ch) dst.push_back(make_int4(e.x, e.y, s0, std::min(ch, e.w - s0)));
         }
-    }
+    });
     drop_graphs(ctx);
-    std::vector<int4> f64, f32;
-    bucket_sorted(c64, f64, ctx->plan_off[0], ctx->plan_cnt[0]);
-    bucket_sorted(c32, f32, ctx->plan_off[1], ctx->plan_cnt[1]);
-    for (int c = 0; c < kNumQuartetClass; ++c) ctx->plan_off[1][c] += (int64_t)f64.size();
-    const size_t need = f64.size() + f32.size();
+    int64_t dropped = 0, nitems[2] = {0, 0};
+    for (int t = 0; t < T; ++t) dropped += rg[t].dropped;
+    for (int part = 0; part < 2; ++part)
+        for (int c = 0; c < kNumQuartetClass; ++c) {
+            int64_t n = 0, pr = 0;
+            for (int t = 0; t < T; ++t) {
+                n += (int64_t)rg[t].items[part][c].size();
+                pr += rg[t].prims[part][c];
+            }
+            ctx->plan_cnt[part][c] = n;
+            ctx->plan_prims[part][c] = pr;
+            nitems[part] += n;
+        }
+    // the FP64 part, then the FP32 part; classes in order within each
+    int64_t o = 0;
+    for (int part = 0; part < 2; ++part)
+        for (int c = 0; c < kNumQuartetClass; ++c) {
+            ctx->plan_off[part][c] = o;
+            o += ctx->plan_cnt[part][c];
+        }
+    const size_t need = (size_t)o;
+    ctx->plan_h.clear();
+    ctx->plan_h.resize(need);
+    // Ordering: the (part, class) lists are independent; the largest go first
+    std::vector<int> task(2 * kNumQuartetClass);
+    for (int i = 0; i < 2 * kNumQuartetClass; ++i) task[i] = i;
+    std::sort(task.begin(), task.end(), [&](int x, int y) {
+        return ctx->plan_cnt[x / kNumQuartetClass][x % kNumQuartetClass] >
+               ctx->plan_cnt[y / kNumQuartetClass][y % kNumQuartetClass];
+    });
+    run_tasks(2 * kNumQuartetClass, T, [&](int i) {
+        const int part = task[i] / kNumQuartetClass, c = task[i] % kNumQuartetClass;
+        std::vector<const std::vector<int4> *> segs;
+        for (int t = 0; t < T; ++t) segs.push_back(&rg[t].items[part][c]);
+        order_class_items(segs, ctx->plan_h.data() + ctx->plan_off[part][c]);
+        for (int t = 0; t < T; ++t) std::vector<int4>().swap(rg[t].items[part][c]);
+    });
     if (need > ctx->plan_cap) {
         free_dev(ctx->d_plan);
         ctx->d_plan = nullptr;
         PQB_CK(ctx, cudaMalloc(&ctx->d_plan, sizeof(int4) * std::max<size_t>(need, 1)));
         ctx->plan_cap = need;
     }
-    if (!f64.empty())
-        PQB_CK(ctx, cudaMemcpy(ctx->d_plan, f64.data(), sizeof(int4) * f64.size(), cudaMemcpyHostToDevice));
-    if (!f32.empty())
-        PQB_CK(ctx, cudaMemcpy(ctx->d_plan + f64.size(), f32.data(), sizeof(int4) * f32.size(), cudaMemcpyHostToDevice));
-    ctx->plan_h = f64;
-    ctx->plan_h.insert(ctx->plan_h.end(), f32.begin(), f32.end());
-    for (int part = 0; part < 2; ++part)
-        for (int c = 0; c < kNumQuartetClass; ++c) {
-            int64_t s = 0;
-            for (int64_t q = 0; q < ctx->plan_cnt[part][c]; ++q) s += ctx->plan_h[ctx->plan_off[part][c] + q].w;
-            ctx->plan_prims[part][c] = s;
-        }
+    if (need) PQB_CK(ctx, cudaMemcpy(ctx->d_plan, ctx->plan_h.data(), sizeof(int4) * need, cudaMemcpyHostToDevice));
     ctx->have_plan = true;
     if (counts) {
         counts[0] = total;
-        counts[1] = (int64_t)f64.size();
-        counts[2] = (int64_t)f32.size();
+        counts[1] = nitems[0];
+        counts[2] = nitems[1];
         counts[3] = dropped;
     }
     return PQB_OK;
@@ -1473,6 +1552,11 @@ int pqb_set_param(pqb_ctx *ctx, int param, int qclass, int value)
     case PQB_PARAM_GRAPH:
         if (value < 0 || value > 1) return fail(ctx, PQB_E_ARG, "graph %d out of range", value);
         ctx->use_graph = value == 1;
+        return PQB_OK;
+    case PQB_PARAM_THREADS:
+        if (value < 0 || value > 256) return fail(ctx, PQB_E_ARG, "threads %d out of range 0..256", value);
+        ctx->plan_threads = value;
+        ctx->have_plan = false;   // takes effect at the next pqb_plan
         return PQB_OK;
     }
     return fail(ctx, PQB_E_ARG, "unknown parameter %d", param);

@@ -302,6 +302,35 @@ def test_direct_build_graph_replay_matches_launches():
     eng.ctx.check(eng.ctx.lib.pqb_set_param(eng.ctx.h, _lib.PQB_PARAM_GRAPH, 0, 1))
 
 
+def test_plan_is_the_same_on_any_number_of_host_threads():
+    """pqb_plan enumerates bra-pair ranges and orders the class lists on
+    several host threads: the plan (per-class item and primitive counts) and
+    J/K equal the one-thread plan's, for thread counts that split the pairs
+    unevenly."""
+    import ctypes
+    mol = geometries.water_cluster(3, seed=2)
+    bs = BasisSet(mol, "6-31g**")
+    eng = BasisEngine(bs.bfs)
+    D = torch.as_tensor(_rand_density(len(bs), 7), device="cuda")
+    out = {}
+    for threads in (1, 3, 8, 0):
+        eng.ctx.check(eng.ctx.lib.pqb_set_param(eng.ctx.h, _lib.PQB_PARAM_THREADS, 0, threads))
+        eng._plan_key = None
+        counts = dict(eng.plan(1e-10, 1e-5))
+        qa = (ctypes.c_int64 * 42)()
+        pa = (ctypes.c_int64 * 42)()
+        eng.ctx.check(eng.ctx.lib.pqb_plan_stats(eng.ctx.h, qa, pa))
+        J, K = eng.jk(D, "mixed", 1e-10, 1e-5)
+        out[threads] = (counts, list(qa), list(pa), J.clone(), K.clone())
+    c1, q1, p1, J1, K1 = out[1]
+    assert c1["fp64"] > 0 and c1["fp32"] > 0 and c1["dropped"] > 0
+    scale = float(J1.abs().max())
+    for threads in (3, 8, 0):
+        c, q, p, J, K = out[threads]
+        assert c == c1 and q == q1 and p == p1, threads
+        assert float((J - J1).abs().max()) < 1e-13 * scale and float((K - K1).abs().max()) < 1e-13 * scale
+
+
 def test_jk_mixed_precision_error_is_small():
     mol = geometries.water_cluster(3, seed=2)
     bs = BasisSet(mol, "6-31g**")
