@@ -20,6 +20,7 @@
 // component pair (ia, ib) for all ket components, so the same engine
 // writes packed integrals, digests into J/K, or forms Schwarz bounds.
 #pragma once
+#include <atomic>
 #include <type_traits>
 #include "pqb_device.cuh"
 #include "pqb_types.h"
@@ -801,11 +802,16 @@ inline cudaError_t launch_eri_class(const int4 *list, int nq, const PairInfo *pa
     } else {
         using Lay = BlockLayout<LA, LB, LC, LD, R, Epi>;
         auto kern = eri_block_kernel<LA, LB, LC, LD, R, Epi>;
-        static bool attr_set = false;   // per instantiation
-        if (!attr_set) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::bytes);
+        // the attribute is per device: set once per instantiation and device
+        static std::atomic<unsigned long long> attr_set{0};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+        if (!bit || !(attr_set.load() & bit)) {
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::bytes);
             if (e != cudaSuccess) return e;
-            attr_set = true;
+            attr_set.fetch_or(bit);
         }
         int grid = (nq + Lay::NSQ - 1) / Lay::NSQ;
         if (grid > nsm * 8) grid = nsm * 8;
