@@ -40,7 +40,7 @@ enum {
     PQB_E_CUDA = 5,     /* a CUDA runtime call failed                        */
     PQB_E_STATE = 6,    /* call order: e.g. no basis uploaded yet            */
     PQB_E_TIMEOUT = 7,  /* a bounded device wait gave up                     */
-    PQB_E_NOMEM = 8     /* device allocation failed                          */
+    PQB_E_NOMEM = 8     /* device (or, in pqb_plan, host) allocation failed  */
 };
 
 /* precision modes of pqb_jk_direct */

@@ -1057,21 +1057,35 @@ __global__ void finalize_q_kernel(const unsigned long long *q2, double *Q, int n
 
 static inline int64_t pair_idx64(int64_t i, int64_t j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
 
-// Run f(0) .. f(n - 1) on up to nthreads threads (tasks handed out in order).
-template <class F> static void run_tasks(int n, int nthreads, F f)
+// Run f(0) .. f(n - 1) on up to nthreads threads (tasks handed out in
+// order).  Returns false if a task threw (a host allocation failure): no
+// exception crosses the C ABI, and the remaining tasks are not started.
+template <class F> static bool run_tasks(int n, int nthreads, F f)
 {
     nthreads = std::max(1, std::min(nthreads, n));
-    if (nthreads == 1) {
-        for (int i = 0; i < n; ++i) f(i);
-        return;
-    }
+    std::atomic<bool> failed{false};
     std::atomic<int> next{0};
+    auto worker = [&] {
+        for (int i = next++; i < n && !failed.load(); i = next++) {
+            try {
+                f(i);
+            } catch (...) {
+                failed.store(true);
+            }
+        }
+    };
+    if (nthreads == 1) {
+        worker();
+        return !failed.load();
+    }
     std::vector<std::thread> pool;
-    for (int t = 0; t < nthreads; ++t)
-        pool.emplace_back([&] {
-            for (int i = next++; i < n; i = next++) f(i);
-        });
+    try {
+        for (int t = 0; t < nthreads; ++t) pool.emplace_back(worker);
+    } catch (...) {
+        failed.store(true);   // no thread could be started: the running ones stop early
+    }
     for (auto &th : pool) th.join();
+    return !failed.load();
 }
 
 static int host_threads()
@@ -1445,8 +1459,15 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
         int64_t prims[2][kNumQuartetClass] = {{0}};
         int64_t dropped = 0;
     };
-    std::vector<Range> rg(T);
-    run_tasks(T, T, [&](int t) {
+    drop_graphs(ctx);
+    ctx->have_plan = false;
+    std::vector<Range> rg;
+    try {
+        rg.resize(T);
+    } catch (...) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_plan: host allocation failed");
+    }
+    const bool enumerated = run_tasks(T, T, [&](int t) {
         Range &r = rg[t];
         for (int p = pb[t]; p < pb[t + 1]; ++p) {
             const int q0 = ctx->pair_first[p];
@@ -1466,7 +1487,7 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
             }
         }
     });
-    drop_graphs(ctx);
+    if (!enumerated) return fail(ctx, PQB_E_NOMEM, "pqb_plan: host allocation failed (quartet lists)");
     int64_t dropped = 0, nitems[2] = {0, 0};
     for (int t = 0; t < T; ++t) dropped += rg[t].dropped;
     for (int part = 0; part < 2; ++part)
@@ -1488,8 +1509,13 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
             o += ctx->plan_cnt[part][c];
         }
     const size_t need = (size_t)o;
-    ctx->plan_h.clear();
-    ctx->plan_h.resize(need);
+    try {
+        ctx->plan_h.clear();
+        ctx->plan_h.resize(need);
+    } catch (...) {
+        std::vector<int4>().swap(ctx->plan_h);
+        return fail(ctx, PQB_E_NOMEM, "pqb_plan: host allocation failed (%zu work items)", need);
+    }
     // Ordering: the (part, class) lists are independent; the largest go first
     std::vector<int> task(2 * kNumQuartetClass);
     for (int i = 0; i < 2 * kNumQuartetClass; ++i) task[i] = i;
@@ -1497,13 +1523,14 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
         return ctx->plan_cnt[x / kNumQuartetClass][x % kNumQuartetClass] >
                ctx->plan_cnt[y / kNumQuartetClass][y % kNumQuartetClass];
     });
-    run_tasks(2 * kNumQuartetClass, T, [&](int i) {
+    const bool ordered = run_tasks(2 * kNumQuartetClass, T, [&](int i) {
         const int part = task[i] / kNumQuartetClass, c = task[i] % kNumQuartetClass;
         std::vector<const std::vector<int4> *> segs;
         for (int t = 0; t < T; ++t) segs.push_back(&rg[t].items[part][c]);
         order_class_items(segs, ctx->plan_h.data() + ctx->plan_off[part][c]);
         for (int t = 0; t < T; ++t) std::vector<int4>().swap(rg[t].items[part][c]);
     });
+    if (!ordered) return fail(ctx, PQB_E_NOMEM, "pqb_plan: host allocation failed (ordering)");
     if (need > ctx->plan_cap) {
         free_dev(ctx->d_plan);
         ctx->d_plan = nullptr;
