@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <type_traits>
@@ -1108,7 +1109,8 @@ int pqb_create(pqb_ctx **out, int device)
 {
     if (!out) return PQB_E_ARG;
     *out = nullptr;
-    pqb_ctx *ctx = new pqb_ctx();
+    pqb_ctx *ctx = new (std::nothrow) pqb_ctx();
+    if (!ctx) return PQB_E_NOMEM;
     ctx->device = device;
     for (int c = 0; c < kNumQuartetClass; ++c) ctx->chunk[c] = kDefaultChunk;
     cudaError_t e = cudaSetDevice(device);
@@ -1273,9 +1275,9 @@ int pqb_shells_upload(pqb_ctx *ctx, int nshell, const int *shell_l, const int *s
                                    prim_exp, prim_coef, nbf, fscale);
 }
 
-int pqb_shells_upload_batch(pqb_ctx *ctx, int nmol, const int *mol_shell_off, int nshell, const int *shell_l,
-                            const int *shell_nprim, const int *prim_off, const int *shell_f0, const double *shell_xyz,
-                            const double *prim_exp, const double *prim_coef, int nbf, const double *fscale)
+static int shells_upload_batch_impl(pqb_ctx *ctx, int nmol, const int *mol_shell_off, int nshell, const int *shell_l,
+                                    const int *shell_nprim, const int *prim_off, const int *shell_f0, const double *shell_xyz,
+                                    const double *prim_exp, const double *prim_coef, int nbf, const double *fscale)
 {
     if (!ctx || nmol <= 0 || !mol_shell_off || nshell <= 0 || !shell_l || !shell_nprim || !prim_off || !shell_f0 ||
         !shell_xyz || !prim_exp || !prim_coef || !fscale || nbf <= 0)
@@ -1410,7 +1412,21 @@ int pqb_shells_upload_batch(pqb_ctx *ctx, int nmol, const int *mol_shell_off, in
     return PQB_OK;
 }
 
-int pqb_schwarz(pqb_ctx *ctx, double *Q_host, void *stream)
+int pqb_shells_upload_batch(pqb_ctx *ctx, int nmol, const int *mol_shell_off, int nshell, const int *shell_l,
+                            const int *shell_nprim, const int *prim_off, const int *shell_f0, const double *shell_xyz,
+                            const double *prim_exp, const double *prim_coef, int nbf, const double *fscale)
+{
+    try {
+        return shells_upload_batch_impl(ctx, nmol, mol_shell_off, nshell, shell_l, shell_nprim, prim_off, shell_f0,
+                                        shell_xyz, prim_exp, prim_coef, nbf, fscale);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_shells_upload_batch: host allocation failed");
+    } catch (...) {
+        return fail(ctx, PQB_E_STATE, "pqb_shells_upload_batch: unexpected host exception");
+    }
+}
+
+static int schwarz_impl(pqb_ctx *ctx, double *Q_host, void *stream)
 {
     if (!ctx) return PQB_E_ARG;
     if (!ctx->d_pairs) return fail(ctx, PQB_E_STATE, "pqb_schwarz: no basis uploaded");
@@ -1432,6 +1448,17 @@ int pqb_schwarz(pqb_ctx *ctx, double *Q_host, void *stream)
     ctx->have_q = true;
     if (Q_host) memcpy(Q_host, ctx->Q.data(), sizeof(double) * np);
     return PQB_OK;
+}
+
+int pqb_schwarz(pqb_ctx *ctx, double *Q_host, void *stream)
+{
+    try {
+        return schwarz_impl(ctx, Q_host, stream);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_schwarz: host allocation failed");
+    } catch (...) {
+        return fail(ctx, PQB_E_STATE, "pqb_schwarz: unexpected host exception");
+    }
 }
 
 int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *counts)
@@ -1601,7 +1628,7 @@ int pqb_plan_stats(const pqb_ctx *ctx, int64_t *quartets, int64_t *prim_quartets
     return PQB_OK;
 }
 
-int pqb_plan_shard(pqb_ctx *ctx, int rank, int nranks)
+static int plan_shard_impl(pqb_ctx *ctx, int rank, int nranks)
 {
     if (!ctx || nranks < 1 || rank < 0 || rank >= nranks) return fail(ctx, PQB_E_ARG, "pqb_plan_shard: bad rank");
     if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_plan_shard: call pqb_plan first");
@@ -1630,6 +1657,17 @@ int pqb_plan_shard(pqb_ctx *ctx, int rank, int nranks)
     memcpy(ctx->plan_prims, prims, sizeof prims);
     ctx->plan_h.swap(out);
     return PQB_OK;
+}
+
+int pqb_plan_shard(pqb_ctx *ctx, int rank, int nranks)
+{
+    try {
+        return plan_shard_impl(ctx, rank, nranks);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_plan_shard: host allocation failed");
+    } catch (...) {
+        return fail(ctx, PQB_E_STATE, "pqb_plan_shard: unexpected host exception");
+    }
 }
 
 int pqb_fp64_peak(pqb_ctx *ctx, int iters, double *flops)
@@ -1677,7 +1715,7 @@ static int ensure_full_list(pqb_ctx *ctx)
     return PQB_OK;
 }
 
-int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
+static int eri_packed_impl(pqb_ctx *ctx, double *out, int64_t len, void *stream)
 {
     if (!ctx || !out) return fail(ctx, PQB_E_ARG, "pqb_eri_packed: bad arguments");
     if (!ctx->d_pairs) return fail(ctx, PQB_E_STATE, "pqb_eri_packed: no basis uploaded");
@@ -1704,6 +1742,17 @@ int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
         PQB_CK(ctx, cudaStreamWaitEvent(st, ctx->ev_join[k], 0));
     }
     return PQB_OK;
+}
+
+int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
+{
+    try {
+        return eri_packed_impl(ctx, out, len, stream);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_eri_packed: host allocation failed");
+    } catch (...) {
+        return fail(ctx, PQB_E_STATE, "pqb_eri_packed: unexpected host exception");
+    }
 }
 
 // The class launches of one build into the accumulators Jacc, Kacc (zeroed
@@ -1844,8 +1893,8 @@ int pqb_jk_direct_class(pqb_ctx *ctx, const double *D, double *Jacc, double *Kac
     return PQB_OK;
 }
 
-int pqb_jk_packed(pqb_ctx *ctx, const double *ints, int64_t len, const double *D, double *J, double *K, int nbf,
-                  void *stream)
+static int jk_packed_impl(pqb_ctx *ctx, const double *ints, int64_t len, const double *D, double *J, double *K, int nbf,
+                          void *stream)
 {
     if (!ctx || !ints || !D || !J || !K || nbf <= 0) return fail(ctx, PQB_E_ARG, "pqb_jk_packed: bad arguments");
     const int64_t P = (int64_t)nbf * (nbf + 1) / 2;
@@ -1892,9 +1941,21 @@ int pqb_jk_packed(pqb_ctx *ctx, const double *ints, int64_t len, const double *D
     return PQB_OK;
 }
 
-int pqb_eri_functions(pqb_ctx *ctx, int engine, int aux_m, int nq, const int *quartets, int n, const double *origin,
-                      const int *powers, const int *prim_off, const double *exps, const double *cn,
-                      const double *norms, double *out, void *stream)
+int pqb_jk_packed(pqb_ctx *ctx, const double *ints, int64_t len, const double *D, double *J, double *K, int nbf,
+                  void *stream)
+{
+    try {
+        return jk_packed_impl(ctx, ints, len, D, J, K, nbf, stream);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_jk_packed: host allocation failed");
+    } catch (...) {
+        return fail(ctx, PQB_E_STATE, "pqb_jk_packed: unexpected host exception");
+    }
+}
+
+static int eri_functions_impl(pqb_ctx *ctx, int engine, int aux_m, int nq, const int *quartets, int n, const double *origin,
+                              const int *powers, const int *prim_off, const double *exps, const double *cn,
+                              const double *norms, double *out, void *stream)
 {
     if (!ctx || nq < 0 || !quartets || n <= 0 || !origin || !powers || !prim_off || !exps || !cn || !norms || !out)
         return fail(ctx, PQB_E_ARG, "pqb_eri_functions: bad arguments");
@@ -1914,9 +1975,23 @@ int pqb_eri_functions(pqb_ctx *ctx, int engine, int aux_m, int nq, const int *qu
     return PQB_OK;
 }
 
-int pqb_oneint(pqb_ctx *ctx, int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
-               const double *cn, const double *norms, int natoms, const double *atom_xyz, const double *atom_z,
-               double *S, double *T, double *V, void *stream)
+int pqb_eri_functions(pqb_ctx *ctx, int engine, int aux_m, int nq, const int *quartets, int n, const double *origin,
+                      const int *powers, const int *prim_off, const double *exps, const double *cn,
+                      const double *norms, double *out, void *stream)
+{
+    try {
+        return eri_functions_impl(ctx, engine, aux_m, nq, quartets, n, origin, powers, prim_off, exps, cn, norms, out,
+                                  stream);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_eri_functions: host allocation failed");
+    } catch (...) {
+        return fail(ctx, PQB_E_STATE, "pqb_eri_functions: unexpected host exception");
+    }
+}
+
+static int oneint_impl(pqb_ctx *ctx, int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
+                       const double *cn, const double *norms, int natoms, const double *atom_xyz, const double *atom_z,
+                       double *S, double *T, double *V, void *stream)
 {
     if (!ctx || n <= 0 || !origin || !powers || !prim_off || !exps || !cn || !norms || natoms < 0 ||
         (V && natoms > 0 && (!atom_xyz || !atom_z)))
@@ -1943,6 +2018,20 @@ int pqb_oneint(pqb_ctx *ctx, int n, const double *origin, const int *powers, con
     // the host staging buffer must outlive the async copy
     PQB_CK(ctx, cudaStreamSynchronize(st));
     return PQB_OK;
+}
+
+int pqb_oneint(pqb_ctx *ctx, int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
+               const double *cn, const double *norms, int natoms, const double *atom_xyz, const double *atom_z,
+               double *S, double *T, double *V, void *stream)
+{
+    try {
+        return oneint_impl(ctx, n, origin, powers, prim_off, exps, cn, norms, natoms, atom_xyz, atom_z, S, T, V,
+                           stream);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_oneint: host allocation failed");
+    } catch (...) {
+        return fail(ctx, PQB_E_STATE, "pqb_oneint: unexpected host exception");
+    }
 }
 
 // Host code may not use pqb_noalloc_atoms' name as a device address: its
@@ -1979,7 +2068,7 @@ int pqb_oneint_noalloc(int n, const double *origin, const int *powers, const int
     return cudaGetLastError() == cudaSuccess ? PQB_OK : PQB_E_CUDA;
 }
 
-int pqb_set_shell_atoms(pqb_ctx *ctx, const int *shell_atom)
+static int set_shell_atoms_impl(pqb_ctx *ctx, const int *shell_atom)
 {
     if (!ctx || !shell_atom) return fail(ctx, PQB_E_ARG, "pqb_set_shell_atoms: bad arguments");
     if (!ctx->d_pairs) return fail(ctx, PQB_E_STATE, "pqb_set_shell_atoms: no basis uploaded");
@@ -1989,7 +2078,18 @@ int pqb_set_shell_atoms(pqb_ctx *ctx, const int *shell_atom)
     return PQB_OK;
 }
 
-int pqb_grad_2e(pqb_ctx *ctx, const double *D, double *grad, int mode, void *stream)
+int pqb_set_shell_atoms(pqb_ctx *ctx, const int *shell_atom)
+{
+    try {
+        return set_shell_atoms_impl(ctx, shell_atom);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_set_shell_atoms: host allocation failed");
+    } catch (...) {
+        return fail(ctx, PQB_E_STATE, "pqb_set_shell_atoms: unexpected host exception");
+    }
+}
+
+static int grad_2e_impl(pqb_ctx *ctx, const double *D, double *grad, int mode, void *stream)
 {
     if (!ctx || !D || !grad) return fail(ctx, PQB_E_ARG, "pqb_grad_2e: bad arguments");
     if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_grad_2e: call pqb_plan first");
@@ -2011,9 +2111,20 @@ int pqb_grad_2e(pqb_ctx *ctx, const double *D, double *grad, int mode, void *str
     return PQB_OK;
 }
 
-int pqb_grad_1e(pqb_ctx *ctx, int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
-                const double *cn, const double *norms, const int *func_atom, int natoms, const double *atom_xyz,
-                const double *atom_z, const double *D, const double *W, double *grad, void *stream)
+int pqb_grad_2e(pqb_ctx *ctx, const double *D, double *grad, int mode, void *stream)
+{
+    try {
+        return grad_2e_impl(ctx, D, grad, mode, stream);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_grad_2e: host allocation failed");
+    } catch (...) {
+        return fail(ctx, PQB_E_STATE, "pqb_grad_2e: unexpected host exception");
+    }
+}
+
+static int grad_1e_impl(pqb_ctx *ctx, int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
+                        const double *cn, const double *norms, const int *func_atom, int natoms, const double *atom_xyz,
+                        const double *atom_z, const double *D, const double *W, double *grad, void *stream)
 {
     if (!ctx || n <= 0 || !origin || !powers || !prim_off || !exps || !cn || !norms || !func_atom || natoms <= 0 ||
         !atom_xyz || !atom_z || !D || !W || !grad)
@@ -2039,6 +2150,20 @@ int pqb_grad_1e(pqb_ctx *ctx, int n, const double *origin, const int *powers, co
     PQB_CK(ctx, cudaGetLastError());
     PQB_CK(ctx, cudaStreamSynchronize(st));
     return PQB_OK;
+}
+
+int pqb_grad_1e(pqb_ctx *ctx, int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
+                const double *cn, const double *norms, const int *func_atom, int natoms, const double *atom_xyz,
+                const double *atom_z, const double *D, const double *W, double *grad, void *stream)
+{
+    try {
+        return grad_1e_impl(ctx, n, origin, powers, prim_off, exps, cn, norms, func_atom, natoms, atom_xyz, atom_z, D,
+                            W, grad, stream);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_grad_1e: host allocation failed");
+    } catch (...) {
+        return fail(ctx, PQB_E_STATE, "pqb_grad_1e: unexpected host exception");
+    }
 }
 
 int pqb_boys_eval(pqb_ctx *ctx, int m, int count, const double *T, double *F, void *stream)
