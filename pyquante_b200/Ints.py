@@ -171,13 +171,33 @@ def _back(x, orig):
     return x.cpu().numpy()
 
 
+_JK_CACHE = 2   # densities remembered per integral object (uhf: alpha and beta)
+
+
 def _jk(Ints, D):
-    if isinstance(Ints, DirectInts):
-        Dd, _ = _as_device(D, Ints.engine.device)
-        return Ints.jk(Dd)
-    if isinstance(Ints, PackedInts):
-        t = Ints.tensor
-    elif isinstance(Ints, torch.Tensor):
+    """J and K of D.  One build gives both, and PyQuante's callers ask for
+    them one at a time: getJ(Ints, D) then getK(Ints, D), and uhf does
+    getJ(Da), getJ(Db), getK(Da), getK(Db).  So PackedInts and DirectInts
+    keep their last two densities with J and K, and serve a repeated density
+    without a second build.  The key is the density's values plus the
+    precision and thresholds (direct) or the integral tensor's identity and
+    in-place version (packed).  The cache holds copies and hands out copies,
+    so nothing a caller does to its arrays changes a later answer."""
+    if isinstance(Ints, (PackedInts, DirectInts)):
+        direct = isinstance(Ints, DirectInts)
+        Dd, _ = _as_device(D, Ints.engine.device if direct else Ints.tensor.device)
+        key = ((Ints.precision, Ints.schwarz, Ints.fp32_threshold) if direct
+               else (id(Ints.tensor), Ints.tensor._version))
+        cache = Ints.__dict__.setdefault("_jk_cache", [])
+        for i, (k, Dc, Jc, Kc) in enumerate(cache):
+            if k == key and Dc.shape == Dd.shape and torch.equal(Dc, Dd):
+                cache.insert(0, cache.pop(i))
+                return Jc.clone(), Kc.clone()
+        J, K = Ints.jk(Dd) if direct else jk_packed(Ints.tensor.contiguous(), Dd)
+        cache.insert(0, (key, Dd.clone(), J.clone(), K.clone()))
+        del cache[_JK_CACHE:]
+        return J, K
+    if isinstance(Ints, torch.Tensor):
         t = Ints.to(dtype=torch.float64)
         if not t.is_cuda:
             t = t.cuda()

@@ -45,3 +45,50 @@ def test_engine_raises_without_device(monkeypatch):
     monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
     with pytest.raises(_lib.EngineUnavailable):
         _lib.Context(0)
+
+
+def test_repeated_density_reuses_the_last_build(monkeypatch):
+    """getJ(Ints, D) then getK(Ints, D) (the reference's call pattern) runs
+    one J/K build, not two, and uhf's getJ(Da), getJ(Db), getK(Da), getK(Db)
+    runs two.  A new density,
+    an in-place change to the density or to the integrals, and changes a
+    caller makes to returned arrays all behave as without the cache.  Host
+    logic only: the build is replaced by a counting stand-in."""
+    import numpy as np
+    import torch
+    from pyquante_b200 import Ints as I
+    calls = []
+
+    def fake_jk_packed(t, D):
+        calls.append(1)
+        s = float(t.sum())
+        return D * 2.0 + s, D * 3.0 + s
+
+    monkeypatch.setattr(I, "jk_packed", fake_jk_packed)
+    ints = I.PackedInts(torch.ones(21, dtype=torch.float64), 5)
+    rng = np.random.default_rng(0)
+    Da = rng.standard_normal((5, 5))
+    Db = rng.standard_normal((5, 5))
+    J = I.getJ(ints, Da)
+    K = I.getK(ints, Da)
+    assert len(calls) == 1
+    assert np.allclose(J, 2 * Da + 21) and np.allclose(K, 3 * Da + 21)
+    J[:] = 0.0                                   # the caller's array, not the cache
+    assert np.allclose(I.getJ(ints, Da), 2 * Da + 21) and len(calls) == 1
+    assert np.allclose(I.get2JmK(ints, Da), 4 * Da + 42 - 3 * Da - 21) and len(calls) == 1
+    I.getJ(ints, Db)
+    I.getK(ints, Db)
+    assert len(calls) == 2
+    Db[0, 0] += 1.0                              # same array, new values
+    assert np.allclose(I.getK(ints, Db), 3 * Db + 21) and len(calls) == 3
+    ints.tensor.mul_(2.0)                        # the integrals changed in place
+    assert np.allclose(I.getK(ints, Db), 3 * Db + 42) and len(calls) == 4
+    Dt = torch.as_tensor(Da)
+    Jt = I.getJ(ints, Dt)
+    Jt.zero_()                                   # torch in, torch out: still a copy
+    assert torch.allclose(I.getJ(ints, Dt), 2 * Dt + 42) and len(calls) == 5
+    # uhf's order: J of alpha and beta, then K of alpha and beta -> two builds
+    Da2, Db2 = Da + 1.0, Db + 1.0
+    Ja, Jb, Ka, Kb = I.getJ(ints, Da2), I.getJ(ints, Db2), I.getK(ints, Da2), I.getK(ints, Db2)
+    assert len(calls) == 7
+    assert np.allclose(Ka, 3 * Da2 + 42) and np.allclose(Kb, 3 * Db2 + 42) and np.allclose(Jb, 2 * Db2 + 42)

@@ -376,6 +376,40 @@ def test_rhf_reference_unit_test_energies():
     assert round(e - (-1.131334), 4) == 0
 
 
+def test_uhf_reference_no_energy(monkeypatch):
+    """NO / 6-31G** UHF at 2.12955 bohr, the reference's Tests/no_uhf.py
+    (-129.247769 within 1e-4, uhf defaults).  The same uhf iterations on the
+    oracle's integrals (numpy J/K) must give the GPU energy to 1e-7, and each
+    iteration's getJ(Da), getJ(Db), getK(Da), getK(Db) runs two builds."""
+    from pyquante_b200 import hartree_fock as HF
+    from pyquante_b200.Molecule import Molecule
+    no = Molecule("NO", atomlist=[(7, (0.0, 0.0, 0.0)), (8, (2.12955, 0.0, 0.0))], multiplicity=2)
+    builds = []
+    real = Ints.jk_packed
+
+    def counted(t, D):
+        builds.append(1)
+        return real(t, D)
+
+    monkeypatch.setattr(Ints, "jk_packed", counted)
+    gets = []
+    for name in ("getJ", "getK"):
+        f = getattr(HF, name)
+        monkeypatch.setattr(HF, name, lambda I, D, f=f: (gets.append(1), f(I, D))[1])
+    e_gpu, _, _ = HF.uhf(no)
+    assert abs(e_gpu - (-129.247769)) < 1e-4
+    assert 0 < len(builds) <= len(gets) // 2
+    # the same driver on the oracle's integrals
+    bs = BasisSet(no, "6-31g**")
+    obfs = oracle_bfs(bs)
+    S, h = O.orc_get1ints(obfs, atoms_of(no))
+    ref = O.orc_get2ints(obfs)
+    monkeypatch.setattr(HF, "getJ", lambda I, D: O.getJK(I, D)[0])
+    monkeypatch.setattr(HF, "getK", lambda I, D: O.getJK(I, D)[1])
+    e_orc, _, _ = HF.uhf(no, bfs=bs.bfs, integrals=(S, h, ref))
+    assert abs(e_gpu - e_orc) < 1e-7
+
+
 def test_single_function_and_zero_density_edge_cases():
     """He / STO-3G has one function and one unique integral: packed, direct
     and stored J/K against the oracle; a zero density gives J = K = 0."""
