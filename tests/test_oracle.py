@@ -132,3 +132,36 @@ def test_restated_reference_gradient_matches_oracle_finite_differences():
         p[a][x] -= 2 * hstep
         em = scf([(z, tuple(r)) for (z, _), r in zip(atoms, p)])[0]
         assert abs(g[a, x] - (ep - em) / (2 * hstep)) < 1e-7
+
+
+def test_package_scf_drivers_on_oracle_integrals(monkeypatch):
+    """hartree_fock.rhf and uhf (geigh, mkdens, DIIS, density averaging: the
+    host side of the SCF) driven by the oracle's integrals instead of the GPU
+    reproduce the reference's known answers: H2O / 6-31G** (Tests/h2o.py:16)
+    with and without DIIS, and NO / 6-31G** UHF at 2.12955 bohr
+    (Tests/no_uhf.py, 1e-4)."""
+    from pyquante_b200 import hartree_fock as HF
+    from pyquante_b200.Basis.basis import BasisSet
+    from pyquante_b200.Molecule import Molecule
+    e = json.load(open(os.path.join(GOLDEN, "energies.json")))
+    monkeypatch.setattr(HF, "get2JmK", O.get2JmK)
+    monkeypatch.setattr(HF, "getJ", lambda I, D: O.getJK(I, D)[0])
+    monkeypatch.setattr(HF, "getK", lambda I, D: O.getJK(I, D)[1])
+
+    def oracle_integrals(mol, basis):
+        bs = BasisSet(mol, basis)
+        bfs = [O.BF(bf.origin, bf.powers, list(zip(bf.pexps, bf.pcoefs))) for bf in bs.bfs]
+        S, h = O.orc_get1ints(bfs, atoms_of(mol))
+        return bs.bfs, (S, h, O.orc_get2ints(bfs))
+
+    a2b = 1 / 0.529177249
+    h2o = Molecule("h2o", [(8, (0.0, 0.0, 0.0)), (1, (a2b, 0.0, 0.0)), (1, (0.0, a2b, 0.0))], units="bohr")
+    bfs, ints = oracle_integrals(h2o, "6-31g**")
+    for diis in (False, True):
+        E, _, _ = HF.rhf(h2o, bfs=bfs, integrals=ints, ConvCriteria=1e-10, MaxIter=100, DoAveraging=diis)
+        assert abs(E - e["h2o_test_literal"]) < e["h2o_test_tol"]
+        assert abs(E - e["h2o_test_geometry_631ss"]) < 1e-8
+    no = Molecule("NO", atomlist=[(7, (0.0, 0.0, 0.0)), (8, (2.12955, 0.0, 0.0))], multiplicity=2)
+    bfs, ints = oracle_integrals(no, "6-31g**")
+    E, _, _ = HF.uhf(no, bfs=bfs, integrals=ints)
+    assert abs(E - (-129.247769)) < 1e-4
