@@ -1,19 +1,22 @@
 """Benchmark: integral-direct 2J-K Fock build on (H2O)8 / 6-31G** (N = 200).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pqb|reference]
-                    [--precision mixed|fp64] [--no-cpu-baseline]
+                    [--no-cpu-baseline] [--workload h2o8|stored|c16h34|h2o4-grad|batch]
 
-One step = one full 2J-K Fock build G(D) = 2J(D) - K(D) for a fixed SCF
-density D of the seeded (H2O)8 cluster (Schwarz 1e-12; mixed precision puts
-quartets with Q_ab Q_cd < 1e-5 in FP32).  value = nominal unique quartets
-Q = P(P+1)/2 (P = N(N+1)/2, 202,015,050) per second of Fock build, i.e. the
-same count the reference's get2ints evaluates (PyQuante/Ints.py:146-167).
-Under torchrun the quartet lists are sharded over ranks and J/K summed
-with one NCCL all-reduce per build (strong scaling).
+One step = one full FP64 2J-K Fock build G(D) = 2J(D) - K(D) for a fixed SCF
+density D of the seeded (H2O)8 cluster (Schwarz 1e-12).  value = nominal
+unique quartets Q = P(P+1)/2 (P = N(N+1)/2, 202,015,050) per second of Fock
+build, the count the reference's get2ints evaluates (PyQuante/Ints.py:146-167);
+the line also gives the quartets computed after Schwarz screening per second.
+The mixed FP32/FP64 build (quartets with Q_ab Q_cd < 1e-5 in FP32) is timed
+beside it, with its SCF energy error against the FP64 path.  Under torchrun
+the quartet lists are sharded over ranks and J/K summed with one NCCL
+all-reduce per build (strong scaling).
 
 The reference arm (--impl reference) times the reference's own C Rys engine
-(oracle/_ref/ref_fock, compiled from the reference's Src/lib/utils/crys.c)
-over a bounded sample of the same quartets on all host cores.
+(oracle/_ref, compiled from the reference's Src/lib/utils/crys.c) over a
+bounded sample of the same quartets on all host cores and on one, plus full
+get2ints + get2JmK steps of small molecules.
 """
 import argparse
 import json
@@ -34,11 +37,11 @@ WORKLOAD = "(H2O)8 cluster, 6-31G** cartesian, N=200, seed 0, 9 A cube"
 SCHWARZ = 1e-12
 FP32_THRESH = 1e-5
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on these workloads:
-# one stored-integral J/K launch (profiles/jk_packed_reg_h2o8_631gss.md) and the 34 class
-# launches of one FP64 direct build captured there (profiles/eri_jk_direct_h2o8_631gss.md, section 2)
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one stored-integral J/K
+# launch on this workload, and of all class launches of one FP64 direct build (None: not
+# captured for the current kernels)
 STORED_TRAFFIC_BYTES = 1620658000 + 5230080
-DIRECT_TRAFFIC_BYTES = 46173184
+DIRECT_TRAFFIC_BYTES = None
 
 
 def parse():
@@ -47,7 +50,8 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="pqb", choices=["pqb", "reference"])
-    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    p.add_argument("--precision", default="fp64", choices=["mixed", "fp64"],
+                   help="precision of the --profile-builds builds")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-graph", action="store_true", help="launch the timed builds eagerly instead of replaying "
                                                              "a captured CUDA graph")
@@ -78,6 +82,8 @@ def nominal_quartets(n):
 def _oracle_table(bs):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyq_oracle as O
+    if bs is None:
+        return O, None
     return O, O.Table([O.BF(bf.origin, bf.powers, list(zip(bf.pexps, bf.pcoefs))) for bf in bs.bfs])
 
 
@@ -112,6 +118,51 @@ def reference_rate(bs, seconds, seed=0, nproc=None):
                 cores=nproc)
 
 
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def reference_full_steps(nproc):
+    """Full reference steps, timed: Ints.get2ints (every unique quartet) and
+    one get2JmK on the packed array, through the reference's compiled crys
+    (ref_fock.c), for water / STO-3G (406 quartets) and water clusters of
+    two and three molecules in 6-31G** (N = 50, 75)."""
+    O, _ = _oracle_table(None)
+    from pyquante_b200 import geometries
+    from pyquante_b200.Basis.p631ss import basis_data as P631SS
+    from pyquante_b200.Basis.sto3g import basis_data as STO3G
+    lib = O.ref_lib("fock")
+    out = []
+    for name, mol, basis in (("water / STO-3G", geometries.water(), STO3G),
+                             ("(H2O)2 / 6-31G**", geometries.water_cluster(2, seed=4), P631SS),
+                             ("(H2O)3 / 6-31G**", geometries.water_cluster(3, seed=2), P631SS)):
+        bfs = O.build_basis([(at.atno, tuple(at.r)) for at in mol.atoms], basis)
+        t = O.Table(bfs)
+        nq = O.nquartets(t.nbf)
+        ints = np.zeros(nq)
+        rng = np.random.default_rng(0)
+        C = rng.standard_normal((t.nbf, max(1, t.nbf // 5)))
+        D = np.ascontiguousarray(C @ C.T)
+        G = np.zeros_like(D)
+        t0 = time.perf_counter()
+        rc = lib.ref_get2ints(*t.args(), ints.ctypes.data_as(O._dp), nproc)
+        t1 = time.perf_counter()
+        lib.ref_get2JmK(t.nbf, ints.ctypes.data_as(O._dp), D.ctypes.data_as(O._dp), G.ctypes.data_as(O._dp))
+        t2 = time.perf_counter()
+        if rc != 0:
+            raise RuntimeError("ref_get2ints failed (%d)" % rc)
+        out.append({"molecule": name, "nbf": t.nbf, "quartets": nq, "get2ints_s": t1 - t0, "get2JmK_s": t2 - t1,
+                    "step_s": t2 - t0, "quartets_per_s": nq / (t1 - t0), "processes": nproc})
+    return out
+
+
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -122,21 +173,30 @@ def run_reference(a):
     per_step = max(2.0, min(20.0, 120.0 / max(a.steps + a.warmup, 1)))
     for i in range(a.warmup):
         reference_rate(bs, per_step / 2, seed=100 + i, nproc=cores)
-    rates, secs, counts = [], [], []
+    secs, counts = [], []
     for i in range(a.steps):
         r = reference_rate(bs, per_step, seed=i, nproc=cores)
-        rates.append(r["value"])
         secs.append(r["seconds"])
         counts.append(r["quartets"])
     value = sum(counts) / sum(secs)
+    one = reference_rate(bs, min(per_step, 10.0), seed=1000, nproc=1)
+    full = reference_full_steps(cores)
     Q = nominal_quartets(len(bs))
     line = {
-        "impl": "reference", "metric": "ERI quartets/s (2J-K Fock build, nominal unique (ij|kl))",
+        "impl": "reference", "metric": "ERI quartets/s (2J-K Fock build, FP64; nominal unique (ij|kl))",
         "value": value, "unit": "quartets/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": 1e3 * Q / value, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
+        "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "precision": "fp64", "nominal_quartets": Q,
-                   "sample": "random bra rows of Ints.get2ints, all kl >= ij per row, ~%.0f s per step" % per_step},
+                   "step": "one bounded sample of the workload: random bra rows of Ints.get2ints, every kl >= ij "
+                           "per row, ~%.0f s on all host cores (ms_per_step is that sample's time)" % per_step},
+        "full_build_s_extrapolated": Q / value, "extrapolated": True,
+        "extrapolation_note": "the reference computes every unique quartet unscreened; a full c1 build at the "
+                              "sampled rate would take full_build_s_extrapolated seconds",
+        "one_process": {"value": one["value"], "unit": "quartets/s", "quartets": one["quartets"],
+                        "seconds": one["seconds"]},
+        "full_steps": full,
+        "cpu_model": _cpu_model(),
         "cpu_baseline": {"value": value, "unit": "quartets/s", "cores": cores, "kind": "reference",
                          "sample": "%d quartets over %d steps" % (sum(counts), a.steps)},
         "e2e": {"value": value, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -241,8 +301,7 @@ def run_stored(a):
                                  "l2": "packed array 1.6 GB > L2, no flush"},
                       "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
                                    "frac": gbs / peak, "traffic": STORED_TRAFFIC_BYTES, "peak_source": src,
-                                   "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
-                                                     "profiles/jk_packed_reg_h2o8_631gss.md",
+                                   "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch",
                                    "kernel": "jk_packed_reg_kernel<7>"}}))
 
 def run_c16h34(a):
@@ -369,6 +428,46 @@ def run_batch(a):
                                          "max_abs_dE_vs_batched": float(max(s[1] for s in single))}}}))
 
 
+def _timed(fn, steps, stream, flush):
+    """Mean CUDA-event time (ms) of fn() on `stream`, L2 flushed before each."""
+    import torch
+    tot = 0.0
+    for _ in range(steps):
+        flush.zero_()          # L2 flush between timed builds, outside the timed window
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        tot += e0.elapsed_time(e1)
+    return tot / steps
+
+
+def _scf(mol, bs, precision):
+    """RHF to 1e-10 Eh (DIIS) on the integral-direct path; returns the energy,
+    the number of Fock builds and the wall time."""
+    from pyquante_b200 import Ints
+    from pyquante_b200.hartree_fock import rhf
+
+    class Counting(Ints.DirectInts):
+        builds = 0
+
+        def jk(self, D):
+            Counting.builds += 1
+            return super().jk(D)
+
+    from pyquante_b200.Ints import _engine_for, get1ints
+    eng = _engine_for(bs)
+    S, h = get1ints(bs, mol)
+    ints = Counting(eng, precision, SCHWARZ, FP32_THRESH)
+    rhf(mol, bfs=bs, integrals=(S, h, ints), ConvCriteria=1e-10, MaxIter=80, DoAveraging=True)   # warm-up
+    Counting.builds = 0
+    t0 = time.perf_counter()
+    e, _, _ = rhf(mol, bfs=bs, integrals=(S, h, ints), ConvCriteria=1e-10, MaxIter=80, DoAveraging=True)
+    return e, Counting.builds, time.perf_counter() - t0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -380,6 +479,8 @@ def main():
         {"stored": run_stored, "c16h34": run_c16h34, "h2o4-grad": run_h2o4_grad,
          "batch": run_batch}[a.workload](a)
         return
+    import ctypes
+
     import torch
     import torch.distributed as dist
 
@@ -413,6 +514,13 @@ def main():
     eng = BasisEngine(bs.bfs, device=local)
     counts = eng.plan(SCHWARZ, FP32_THRESH)
     shard_plan(eng, rank, world)
+    qa = (ctypes.c_int64 * 42)()
+    pa = (ctypes.c_int64 * 42)()
+    eng.ctx.check(eng.ctx.lib.pqb_plan_stats(eng.ctx.h, qa, pa))
+    qs = np.array(qa[:]).reshape(2, 21)
+    ps = np.array(pa[:]).reshape(2, 21)
+    kept_shell_quartets = counts["shell_quartets"] - counts["dropped"]
+    prim_quartets = int(ps.sum())
     # a realistic density: a few SCF iterations from the core guess
     S, h = Ints.get1ints(bs, mol)
     St = torch.as_tensor(S, device="cuda")
@@ -437,58 +545,44 @@ def main():
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
 
-    def build(mode):
-        eng.jk(D, mode, SCHWARZ, FP32_THRESH, J=J, K=K)
+    def build(mode, e=eng):
+        e.jk(D, mode, e._plan_key[0], e._plan_key[1], J=J, K=K)
         allreduce_jk(J, K)
         torch.sub(J.mul(2.0), K, out=G)
 
     use_graph = world == 1 and not a.no_graph
     graphs = {}
 
-    def capture(mode):
-        # one Fock build (memsets, 42 class launches over the context's
-        # streams, symmetrisation, G) captured once and replayed per step
+    def capture(key, fn):
+        # one Fock build (memsets, class launches over the context's streams,
+        # symmetrisation, G) captured once and replayed per step
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
-            build(mode)
+            fn()
         torch.cuda.current_stream().wait_stream(s)
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
-            build(mode)
+            fn()
         torch.cuda.synchronize()
-        return g
+        graphs[key] = g
 
-    def run_build(mode):
-        if use_graph:
-            graphs[mode].replay()
-        else:
-            build(mode)
+    def runner(key, fn):
+        return (lambda: graphs[key].replay()) if use_graph else fn
 
-    def timed(mode, steps):
-        tot = 0.0
-        for _ in range(steps):
-            flush.zero_()          # L2 flush between timed builds, outside the timed window
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            run_build(mode)
-            e1.record(stream)
-            e1.synchronize()
-            tot += e0.elapsed_time(e1)
-        return tot / steps
-
+    modes = {"fp64": lambda: build("fp64"), "mixed": lambda: build("mixed")}
     for _ in range(a.warmup):
-        build(a.precision)
-        build("fp64")
+        for fn in modes.values():
+            fn()
     torch.cuda.synchronize()
     if use_graph:
-        for mode in {a.precision, "fp64"}:
-            graphs[mode] = capture(mode)
-        for _ in range(a.warmup):
-            run_build(a.precision)
-            run_build("fp64")
+        for key, fn in modes.items():
+            capture(key, fn)
+    run = {key: runner(key, fn) for key, fn in modes.items()}
+    for _ in range(a.warmup):
+        for fn in run.values():
+            fn()
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -497,65 +591,68 @@ def main():
         # 1.5 s before the timed ones, so the clock record (nvidia-smi every
         # 0.2 s) covers the GPU under this load
         for _ in range(a.soak):
-            run_build(a.precision)
+            run["fp64"]()
         torch.cuda.synchronize()
-        ms = timed(a.precision, a.steps)
+        ms = _timed(run["fp64"], a.steps, stream, flush)
+        ms_mixed = _timed(run["mixed"], a.steps, stream, flush)
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
-    ms_fp64 = timed("fp64", a.steps)
     if world > 1:
-        t = torch.tensor([ms, ms_fp64], device="cuda")
+        t = torch.tensor([ms, ms_mixed], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_fp64 = t.tolist()
+        ms, ms_mixed = t.tolist()
+
+    # the mixed mode's FP64 list alone (quartets with Q_ab Q_cd >= the FP32
+    # threshold): the time the mixed build cannot go below however cheap the
+    # FP32 quartets become
+    ms_list64 = None
+    if world == 1:
+        eng64 = BasisEngine(bs.bfs, device=local)
+        eng64.plan(FP32_THRESH, FP32_THRESH)
+        fn = lambda: build("fp64", eng64)   # noqa: E731
+        for _ in range(a.warmup):
+            fn()
+        if use_graph:
+            capture("list64", fn)
+        ms_list64 = _timed(runner("list64", fn), a.steps, stream, flush)
+        del eng64
 
     # end to end through the public API: pinned host D in, host G out
     Dh = D.cpu().pin_memory()
-    direct = Ints.DirectInts(eng, a.precision, SCHWARZ, FP32_THRESH)
     Gh = torch.empty_like(Dh).pin_memory()
 
-    def e2e_step():
-        Dd = Dh.to("cuda", non_blocking=True)
-        Jd, Kd = direct.jk(Dd)
-        allreduce_jk(Jd, Kd)
-        Gh.copy_(2.0 * Jd - Kd, non_blocking=True)
+    def e2e(precision):
+        direct = Ints.DirectInts(eng, precision, SCHWARZ, FP32_THRESH)
 
-    for _ in range(a.warmup):
-        e2e_step()
-    torch.cuda.synchronize()
-    barrier()
-    e2e_ms = 0.0
-    for _ in range(a.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        e2e_step()
-        e1.record(stream)
-        e1.synchronize()
-        e2e_ms += e0.elapsed_time(e1)
-    e2e_ms /= a.steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t[0])
+        def step():
+            Dd = Dh.to("cuda", non_blocking=True)
+            Jd, Kd = direct.jk(Dd)
+            allreduce_jk(Jd, Kd)
+            Gh.copy_(2.0 * Jd - Kd, non_blocking=True)
+
+        for _ in range(a.warmup):
+            step()
+        torch.cuda.synchronize()
+        barrier()
+        t = _timed(step, a.steps, stream, flush)
+        if world > 1:
+            tt = torch.tensor([t], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt[0])
+        return t
+
+    e2e_ms = e2e("fp64")
+    e2e_mixed_ms = e2e("mixed")
 
     # roofline: per-class FP64 timing of the direct J/K kernels
-    qs = (torch.zeros(42, dtype=torch.int64)).numpy()
-    ps = qs.copy()
-    import ctypes
-    qa = (ctypes.c_int64 * 42)()
-    pa = (ctypes.c_int64 * 42)()
-    eng.ctx.check(eng.ctx.lib.pqb_plan_stats(eng.ctx.h, qa, pa))
-    qs = np.array(qa[:]).reshape(2, 21)
-    ps = np.array(pa[:]).reshape(2, 21)
     per_class = []
-    launches = 2   # two symmetrise kernels per build
+    nlaunch = 3   # density scaling and two symmetrise kernels per build
     for part in (0, 1):
         for qc in range(21):
             if qs[part, qc] == 0:
                 continue
-            launches += 1
+            nlaunch += 1
             tms = []
             for _ in range(3):
                 flush.zero_()
@@ -577,36 +674,66 @@ def main():
     peak_tf = peak.value / 1e12
     dom = max(per_class, key=lambda r: r["ms"])
     tot_fl = sum(r["flops"] for r in per_class)
-    build_tflops = tot_fl / (ms_fp64 * 1e-3) / 1e12
+    build_tflops = tot_fl / (ms * 1e-3) / 1e12
+
+    # accuracy of the mixed mode: RHF on each path from the same start
+    scf = None
+    if rank == 0:
+        e64, it64, s64 = _scf(mol, bs, "fp64")
+        emx, itmx, smx = _scf(mol, bs, "mixed")
+        scf = dict(e64=e64, emx=emx, it64=it64, itmx=itmx, s64=s64, smx=smx)
     if rank == 0:
         line = {
-            "metric": "ERI quartets/s (2J-K Fock build, nominal unique (ij|kl))",
+            "metric": "ERI quartets/s (2J-K Fock build, FP64; nominal unique (ij|kl))",
             "value": Q / (ms * 1e-3), "unit": "quartets/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-            "dtype": "f64+f32" if a.precision == "mixed" else "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "precision": a.precision, "schwarz": SCHWARZ,
-                       "fp32_threshold": FP32_THRESH, "nominal_quartets": Q,
-                       "shell_quartets": counts["shell_quartets"], "kept_fp64": counts["fp64"],
-                       "kept_fp32": counts["fp32"], "l2": "256 MiB buffer zeroed between timed builds",
-                       "cuda_graph": use_graph,
-                       "fp64_ms_per_step": ms_fp64, "mixed_speedup_vs_fp64": ms_fp64 / ms,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "fp64", "schwarz": SCHWARZ, "nominal_quartets": Q,
+                       "shell_quartets": counts["shell_quartets"],
+                       "computed_shell_quartets": kept_shell_quartets,
+                       "computed_primitive_quartets": prim_quartets,
+                       "work_items": counts["fp64"] + counts["fp32"],
+                       "l2": "256 MiB buffer zeroed between timed builds", "cuda_graph": use_graph,
                        "parallelism": "quartet shards x%d + NCCL all-reduce of J,K" % world if world > 1 else "1 GPU"},
+            "computed_shell_quartets_per_s": kept_shell_quartets / (ms * 1e-3),
+            "computed_primitive_quartets_per_s": prim_quartets / (ms * 1e-3),
+            "s_per_fock_build": ms * 1e-3,
             "e2e": {"value": Q / (e2e_ms * 1e-3), "unit": "quartets/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": int(D.numel() * 8), "d2h_bytes_per_step": int(D.numel() * 8),
-                    "api": "pyquante_b200.Ints.DirectInts.jk (the get2JmK path) from pinned host D"},
+                    "api": "pyquante_b200.Ints.DirectInts.jk (the get2JmK path), FP64, from pinned host D"},
+            "mixed": {"precision": "mixed", "fp32_threshold": FP32_THRESH, "dtype": "f64+f32",
+                      "ms_per_step": ms_mixed, "value": Q / (ms_mixed * 1e-3), "unit": "quartets/s",
+                      "speedup_vs_fp64": ms / ms_mixed,
+                      "fp64_list_alone_ms": ms_list64,
+                      "speedup_ceiling": (ms / ms_list64) if ms_list64 else None,
+                      "speedup_ceiling_note": "FP64 build time over the time of the mixed mode's FP64 list alone "
+                                              "(quartets with Q_ab Q_cd >= the FP32 threshold): the bound if the "
+                                              "FP32 quartets cost nothing",
+                      "kept_fp64_items": counts["fp64"], "kept_fp32_items": counts["fp32"],
+                      "e2e": {"value": Q / (e2e_mixed_ms * 1e-3), "unit": "quartets/s", "ms_per_step": e2e_mixed_ms}},
             "roofline": {"bound": "fp64", "achieved": build_tflops, "peak": peak_tf, "unit": "TFLOP/s",
                          "frac": build_tflops / peak_tf, "traffic": DIRECT_TRAFFIC_BYTES,
-                         "traffic_note": "DRAM bytes of 34 of the 42 class launches of one FP64 build (ncu); the "
-                                         "build is L2-resident, so the FP64 pipe, not HBM, is the roofline",
+                         "traffic_note": "DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) summed over "
+                                         "the class launches of one FP64 build of this workload; the build is "
+                                         "L2-resident, so the FP64 pipe, not HBM, is the roofline",
                          "kernel": "eri_thread_kernel/eri_block_kernel<class, EpiJK>: all class instantiations "
                                    "of one FP64 Fock build, launched together by pqb_jk_direct",
-                         "flops_per_build": tot_fl, "fp64_build_ms": ms_fp64,
+                         "flops_per_build": tot_fl, "flop_model": "pyquante_b200.flops (per-class counts of the "
+                                                                   "kernels' FP64 operations, FMA = 2)",
                          "peak_source": "measured DFMA probe (pqb_fp64_peak) on this GPU",
                          "slowest_class_alone": "(%d%d|%d%d)" % tuple(dom["cls"]),
                          "slowest_class_alone_tflops": dom["tflops"]},
-            "gpu_launches": launches * a.steps,
+            "gpu_launches": nlaunch * a.steps,
             "clocks": clk.summary(),
         }
+        if scf is not None:
+            line["scf"] = {"energy_fp64": scf["e64"], "energy_mixed": scf["emx"],
+                           "abs_dE_mixed_vs_fp64": abs(scf["emx"] - scf["e64"]),
+                           "fock_builds_fp64": scf["it64"], "fock_builds_mixed": scf["itmx"],
+                           "s_per_iteration_fp64": scf["s64"] / max(scf["it64"], 1),
+                           "s_per_iteration_mixed": scf["smx"] / max(scf["itmx"], 1),
+                           "convergence": "RHF, DIIS, |dE| < 1e-10 Eh, core guess; host eigensolver"}
+            line["mixed"]["abs_dE_vs_fp64"] = line["scf"]["abs_dE_mixed_vs_fp64"]
         if cpu is not None:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": "quartets/s", "cores": cpu["cores"],
                                     "kind": "reference",
@@ -617,6 +744,7 @@ def main():
                                   for r in sorted(per_class, key=lambda r: -r["ms"])]
         print(json.dumps(line))
     if world > 1:
+        graphs.clear()
         dist.destroy_process_group()
 
 

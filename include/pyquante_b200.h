@@ -174,12 +174,14 @@ int pqb_oneint(pqb_ctx *ctx, int n, const double *origin, const int *powers, con
  * arrays, and the packed atom table the kernel reads lives in a file-scope
  * device array of PQB_NOALLOC_MAX_ATOMS = 4096 atoms (128 KiB per GPU, held
  * until exit); natoms above that returns PQB_E_SHAPE.  It calls no
- * cudaMalloc/cudaFree.  The first call on each device looks the array's
- * address up (cudaGetSymbolAddress, that device current); make that first
- * call before any stream capture.  All calls share the array: calls that
- * overlap on the GPU (e.g. on two streams) race; each call rewrites the
- * entries it uses, so nothing needs clearing.  Status codes only (no
- * context, so no pqb_last_error message). */
+ * cudaMalloc/cudaFree.  The atoms are read only when V is requested (V may
+ * be NULL, as in pqb_oneint).  `stream` must belong to the current device
+ * (PQB_E_ARG otherwise).  The first call on each device that computes V
+ * looks the array's address up (cudaGetSymbolAddress, that device current);
+ * make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (e.g. on two streams) race; each call
+ * rewrites the entries it uses, so nothing needs clearing.  Status codes
+ * only (no context, so no pqb_last_error message). */
 int pqb_oneint_noalloc(int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
                        const double *cn, const double *norms, int natoms, const double *atom_xyz,
                        const double *atom_z, double *S, double *T, double *V, void *stream);

@@ -86,6 +86,16 @@ class PackedInts:
         self.nbf = nbf
         self.engine = engine
 
+    @property
+    def tensor(self):
+        return self._tensor
+
+    @tensor.setter
+    def tensor(self, t):
+        # a new integral array invalidates every J/K remembered for the old one
+        self._tensor = t
+        self.__dict__.pop("_jk_cache", None)
+
     def __len__(self):
         return self.tensor.numel()
 
@@ -180,14 +190,15 @@ def _jk(Ints, D):
     getJ(Da), getJ(Db), getK(Da), getK(Db).  So PackedInts and DirectInts
     keep their last two densities with J and K, and serve a repeated density
     without a second build.  The key is the density's values plus the
-    precision and thresholds (direct) or the integral tensor's identity and
-    in-place version (packed).  The cache holds copies and hands out copies,
+    precision and thresholds (direct) or the integral tensor's address, size
+    and in-place version (packed); assigning a new tensor to PackedInts.tensor
+    empties the cache.  The cache holds copies and hands out copies,
     so nothing a caller does to its arrays changes a later answer."""
     if isinstance(Ints, (PackedInts, DirectInts)):
         direct = isinstance(Ints, DirectInts)
         Dd, _ = _as_device(D, Ints.engine.device if direct else Ints.tensor.device)
         key = ((Ints.precision, Ints.schwarz, Ints.fp32_threshold) if direct
-               else (id(Ints.tensor), Ints.tensor._version))
+               else (Ints.tensor.data_ptr(), Ints.tensor.numel(), Ints.tensor._version))
         cache = Ints.__dict__.setdefault("_jk_cache", [])
         for i, (k, Dc, Jc, Kc) in enumerate(cache):
             if k == key and Dc.shape == Dd.shape and torch.equal(Dc, Dd):

@@ -1804,9 +1804,20 @@ static int ensure_build_graph(pqb_ctx *ctx, int mode, int gi)
 {
     if (ctx->graph_exec[gi]) return PQB_OK;
     if (!ctx->cap_stream) PQB_CK(ctx, cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
-    if (!ctx->d_Jacc) {
-        PQB_CK(ctx, cudaMalloc(&ctx->d_Jacc, sizeof(double) * std::max<long long>(ctx->dense_len, 1)));
-        PQB_CK(ctx, cudaMalloc(&ctx->d_Kacc, sizeof(double) * std::max<long long>(ctx->dense_len, 1)));
+    if (!ctx->d_Jacc || !ctx->d_Kacc) {
+        // both or neither: a failed second allocation leaves no half-made pair
+        free_dev(ctx->d_Jacc);
+        free_dev(ctx->d_Kacc);
+        ctx->d_Jacc = ctx->d_Kacc = nullptr;
+        const size_t bytes = sizeof(double) * std::max<long long>(ctx->dense_len, 1);
+        cudaError_t e = cudaMalloc(&ctx->d_Jacc, bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&ctx->d_Kacc, bytes);
+        if (e != cudaSuccess) {
+            free_dev(ctx->d_Jacc);
+            free_dev(ctx->d_Kacc);
+            ctx->d_Jacc = ctx->d_Kacc = nullptr;
+            return fail(ctx, PQB_E_CUDA, "graph accumulators: %s", cudaGetErrorString(e));
+        }
     }
     PQB_CK(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
     const int rc = launch_build(ctx, ctx->d_Jacc, ctx->d_Kacc, mode, ctx->cap_stream);
@@ -2044,14 +2055,25 @@ int pqb_oneint_noalloc(int n, const double *origin, const int *powers, const int
                        const double *cn, const double *norms, int natoms, const double *atom_xyz,
                        const double *atom_z, double *S, double *T, double *V, void *stream)
 {
+    // the same argument rules as pqb_oneint: atoms are read only for V
     if (n <= 0 || !origin || !powers || !prim_off || !exps || !cn || !norms || natoms < 0 ||
-        (natoms > 0 && (!atom_xyz || !atom_z)))
+        (V && natoms > 0 && (!atom_xyz || !atom_z)))
         return PQB_E_ARG;
     if (natoms > PQB_NOALLOC_MAX_ATOMS) return PQB_E_SHAPE;
+    // a non-sticky error left by an unrelated earlier call must not be read
+    // as this call's launch status below
+    (void)cudaGetLastError();
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= PQB_NOALLOC_MAX_DEVICES) return PQB_E_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    // the scratch address below is the current device's copy: a stream of
+    // another device would launch against the wrong one
+    int sdev = dev;
+    if (cudaStreamGetDevice(st, &sdev) != cudaSuccess) return PQB_E_CUDA;
+    if (sdev != dev) return PQB_E_ARG;
+    const int nat = V ? natoms : 0;
     double *atoms = nullptr;
-    {
+    if (nat > 0) {
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
         if (!g_noalloc_atoms[dev]) {
             void *p = nullptr;
@@ -2059,12 +2081,11 @@ int pqb_oneint_noalloc(int n, const double *origin, const int *powers, const int
             g_noalloc_atoms[dev] = static_cast<double *>(p);
         }
         atoms = g_noalloc_atoms[dev];
+        pack_atoms_kernel<<<(nat + 127) / 128, 128, 0, st>>>(nat, atom_xyz, atom_z, atoms);
     }
-    cudaStream_t st = (cudaStream_t)stream;
-    if (natoms > 0) pack_atoms_kernel<<<(natoms + 127) / 128, 128, 0, st>>>(natoms, atom_xyz, atom_z, atoms);
     FuncTable ft{origin, powers, prim_off, exps, cn, norms};
     const int64_t nn = (int64_t)n * n;
-    oneint_kernel<<<(unsigned)((nn + 127) / 128), 128, 0, st>>>(n, ft, natoms, atoms, S, T, V);
+    oneint_kernel<<<(unsigned)((nn + 127) / 128), 128, 0, st>>>(n, ft, nat, atoms, S, T, V);
     return cudaGetLastError() == cudaSuccess ? PQB_OK : PQB_E_CUDA;
 }
 

@@ -27,18 +27,22 @@ constexpr double kPi = 3.14159265358979323846;
 constexpr double kPairPre = 5.9149671727956128778;
 
 // ---------------------------------------------- reciprocal and 1/sqrt --
-// Newton--Raphson from the single-precision hardware estimates
-// (rcp.approx.ftz.f32 and rsqrt.approx.ftz.f32, relative error < 2^-22):
-// one third-order step each.  For 1/x with e = 1 - x r:
-//   r' = r (1 + e + e^2)                     (remaining error ~ e^3 ~ 2^-66);
-// for 1/sqrt(x) with e = 1 - x y^2:
-//   y' = y (1 + e/2 + 3 e^2/8)               (remaining error ~ 5 e^3/16).
-// Both end within a couple of ulps of the exact value.  x must be positive
-// and inside single-precision range (about 1e-37 .. 1e37); every caller here
-// passes exponent sums, Boys values or Rys discriminants, which are.
+// Refinement of the single-precision hardware estimates
+// (rcp.approx.ftz.f32 and rsqrt.approx.ftz.f32, relative error < 2^-22) by
+// one step of the third-order Householder iteration, i.e. the truncated
+// series of (1 - e)^(-1) and (1 - e)^(-1/2) in the residual e:
+//   1/x:       e = 1 - x r,    r' = r (1 + e + e^2)        (error ~ e^3 ~ 2^-66)
+//   1/sqrt(x): e = 1 - x y^2,  y' = y (1 + e/2 + 3 e^2/8)  (error ~ 5 e^3/16)
+// Both end within a couple of ulps of the exact value.  x must be positive;
+// outside the single-precision normal range (about 1e-36 .. 1e36, where the
+// estimate of the rounded x would be 0 or inf) the IEEE operation is used
+// instead.  The callers here pass exponent sums, Boys values and Rys
+// discriminants, which stay inside it, so that branch is never taken on the
+// Fock-build path.
 __device__ __forceinline__ double rcp_nr(double x)
 {
     const float xf = (float)x;
+    if (!(fabsf(xf) > 1e-36f && fabsf(xf) < 1e36f)) return 1.0 / x;
     float rf;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rf) : "f"(xf));
     const double r = (double)rf;
@@ -49,6 +53,7 @@ __device__ __forceinline__ double rcp_nr(double x)
 __device__ __forceinline__ double rsqrt_nr(double x)
 {
     const float xf = (float)x;
+    if (!(xf > 1e-36f && xf < 1e36f)) return 1.0 / sqrt(x);
     float yf;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
     const double y = (double)yf;

@@ -2,6 +2,8 @@
 
     make -C oracle ref && python tests/golden/make_golden.py
 
+    python tests/golden/make_golden.py --only-c16h34   # just the C16H34 sample
+
 Sources (nothing here is copied from the reference's files):
   * known answers quoted by the reference's own tests:
       Boys F_0(0)=1, F_0(1), F_{1/2}(6.8)   Src/lib/utils/tests/TestMath.c:18-20
@@ -111,5 +113,57 @@ def main():
     print(json.dumps(energies, indent=1))
 
 
+def c16h34_sample(count=3000):
+    """C16H34 / 6-31G* (N = 308, Q = 1,132,237,791): quartets straight from
+    the reference's compiled crys, drawn (i) where the packed index's
+    intermediate ij*(ij+1) no longer fits a 32-bit int (ij >= 46341, the
+    range where Src/cints.c:413-425 overflows) and (ii) uniformly over all
+    unique quartets.  Its own seeded generator, so regenerating it leaves
+    the other fixtures unchanged."""
+    from pyquante_b200.Basis.p631s import basis_data as P631S
+    bfs = O.build_basis(atoms_of(geometries.alkane(16)), P631S)
+    n = len(bfs)
+    assert n == 308
+    P = n * (n + 1) // 2
+    rng = np.random.default_rng(308)
+
+    def split(ij):
+        i = int((np.sqrt(8 * ij + 1) - 1) // 2)
+        while i * (i + 1) // 2 > ij:
+            i -= 1
+        while (i + 1) * (i + 2) // 2 <= ij:
+            i += 1
+        return i, ij - i * (i + 1) // 2
+
+    # functions 304..307 (the only i with ij >= 46341) sit on the last two H
+    # atoms; the last carbon (225..239) and the last H atoms are their
+    # neighbours, which gives integrals well above zero
+    near = np.r_[225:240, 290:308]
+    quart = []
+    for t in range(count):
+        if t < count // 3:
+            i = int(rng.integers(304, 308))
+            j, k, l = (int(x) for x in rng.choice(near, 3))
+            if k < l:
+                k, l = l, k
+            j = min(j, i)
+            if k * (k + 1) // 2 + l > i * (i + 1) // 2 + j:
+                k, l = i, j
+        else:
+            lo = 46341 if t < count * 2 // 3 else 0
+            ij = int(rng.integers(lo, P))
+            kl = int(rng.integers(0, ij + 1))
+            i, j = split(ij)
+            k, l = split(kl)
+        quart.append((i, j, k, l))
+    quart = np.array(quart, dtype=np.int64)
+    vals = np.array([O.ref_contr(bfs[i], bfs[j], bfs[k], bfs[l]) for i, j, k, l in quart])
+    idx = np.array([O.ijkl2intindex(*q) for q in quart], dtype=np.int64)
+    np.savez(os.path.join(HERE, "eri_631s_c16h34_sample.npz"), quartets=quart.astype(np.int32), index=idx,
+             value=vals)
+
+
 if __name__ == "__main__":
-    main()
+    if "--only-c16h34" not in sys.argv:
+        main()
+    c16h34_sample()

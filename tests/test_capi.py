@@ -50,9 +50,9 @@ def test_engine_raises_without_device(monkeypatch):
 def test_repeated_density_reuses_the_last_build(monkeypatch):
     """getJ(Ints, D) then getK(Ints, D) (the reference's call pattern) runs
     one J/K build, not two, and uhf's getJ(Da), getJ(Db), getK(Da), getK(Db)
-    runs two.  A new density,
-    an in-place change to the density or to the integrals, and changes a
-    caller makes to returned arrays all behave as without the cache.  Host
+    runs two.  A new density, an in-place change to the density or to the
+    integrals, a new integral array, and changes a caller makes to returned
+    arrays all behave as without the cache.  Host
     logic only: the build is replaced by a counting stand-in."""
     import numpy as np
     import torch
@@ -92,3 +92,6 @@ def test_repeated_density_reuses_the_last_build(monkeypatch):
     Ja, Jb, Ka, Kb = I.getJ(ints, Da2), I.getJ(ints, Db2), I.getK(ints, Da2), I.getK(ints, Db2)
     assert len(calls) == 7
     assert np.allclose(Ka, 3 * Da2 + 42) and np.allclose(Kb, 3 * Db2 + 42) and np.allclose(Jb, 2 * Db2 + 42)
+    # a new integral array assigned to the same object: nothing remembered for the old one is served
+    ints.tensor = torch.full((21,), 3.0, dtype=torch.float64)
+    assert np.allclose(I.getK(ints, Db2), 3 * Db2 + 63) and len(calls) == 8

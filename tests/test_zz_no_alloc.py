@@ -39,6 +39,26 @@ def test_oneint_noalloc_matches_oneint_on_two_calls():
             assert float((got - want).abs().max()) < 1e-12, call
 
 
+def test_oneint_noalloc_without_v_reads_no_atoms():
+    """As with pqb_oneint, the atoms are needed only for V: S and T alone
+    take null atom arrays."""
+    from pyquante_b200 import _lib, geometries
+    from pyquante_b200.Basis.basis import BasisSet
+    from pyquante_b200.engine import FunctionTable, oneint
+
+    ctx = _lib.context()
+    mol = geometries.water()
+    ft = FunctionTable(BasisSet(mol, "6-31g**").bfs, ctx.device)
+    S0, T0, _ = oneint(ft, mol.atoms, ctx)
+    S = torch.full_like(S0, float("nan"))
+    T = torch.full_like(S0, float("nan"))
+    rc = ctx.lib.pqb_oneint_noalloc(*ft.args(), len(mol.atoms), None, None, _lib.ptr(S), _lib.ptr(T), None,
+                                    _lib.stream_ptr())
+    assert rc == _lib.PQB_OK
+    torch.cuda.synchronize()
+    assert float((S - S0).abs().max()) < 1e-12 and float((T - T0).abs().max()) < 1e-12
+
+
 def test_oneint_noalloc_rejects_too_many_atoms():
     from pyquante_b200 import _lib
     lib = _lib.load()
