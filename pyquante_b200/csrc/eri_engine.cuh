@@ -1,11 +1,17 @@
 // Shell-quartet ERI engine: one kernel template per angular-momentum class
 // (LA LB | LC LD), fed a class-sorted list of (bra pair, ket pair) quartets.
 //
-// The integral is the Rys quadrature of the reference's Src/crys.c:56-97
-// (sum over roots of Ix*Iy*Iz*w, ABD eqs 5, 9), but organised per SHELL
-// quartet: roots and 2-D integrals are computed once per primitive quartet
-// and shared by every cartesian component, instead of once per component as
-// crys.contr_coulomb does (Src/crys.c:34-54).
+// Two integral schemes, chosen per class at compile time:
+//  * classes with LA+LB+LC+LD <= 4 (thread mode): the Obara--Saika vertical
+//    recurrence per primitive quartet and the Head-Gordon--Pople horizontal
+//    transfer once per contracted item (the scheme of the reference's
+//    Src/chgp.c:78-419), as straight-line code generated by gen_os.py
+//    (os_classes.inc);
+//  * the rest: the Rys quadrature of the reference's Src/crys.c:56-97 (sum
+//    over roots of Ix*Iy*Iz*w, ABD eqs 5, 9).
+// Both are organised per SHELL quartet: the recurrences run once per
+// primitive quartet and serve every cartesian component, instead of once per
+// component as crys.contr_coulomb does (Src/crys.c:34-54).
 //
 // Two execution modes:
 //  * thread mode (NAB*NCD <= 54 in FP64, <= 81 in FP32): one thread per quartet,
@@ -440,6 +446,30 @@ struct EpiSchwarz {
     }
 };
 
+// ------------------------------------------------- Obara--Saika classes --
+// Per-primitive-quartet coefficients of the Obara--Saika vertical recurrence
+// (PA = P - A, QC = Q - C, WP = -rho/zeta PQ, WQ = rho/eta PQ, PQ = P - Q,
+// rz = rho/zeta = eta/(zeta+eta), re = rho/eta = zeta/(zeta+eta),
+// oo2z = 1/(2 zeta), oo2e = 1/(2 eta), oo2ze = 1/(2 (zeta+eta))).
+template <typename R>
+struct OsGeom {
+    R PA[3], WP[3], QC[3], WQ[3];
+    R oo2z, rz, oo2e, re, oo2ze;
+};
+
+// Classes without generated routines keep the Rys quadrature.
+template <int LA, int LB, int LC, int LD>
+struct OsClass {
+    static constexpr bool kOn = false;
+    static constexpr int NV = 1;
+    template <typename R>
+    __device__ static void vrr(const OsGeom<R> &, const R *, R *) {}
+    template <typename R>
+    __device__ static void hrr(const R *, const R *, const R *, R *) {}
+};
+
+#include "os_classes.inc"
+
 // ---------------------------------------------------------- thread mode --
 // Register cap per class (via the minimum resident blocks of 128 threads):
 // small classes are latency bound, so they trade registers for occupancy.
@@ -493,6 +523,38 @@ __device__ __forceinline__ void add_prim_quartet_f32(const QuartetGeomF &g, cons
     }
 }
 
+// The same for the Obara--Saika classes: F_m(T) and the vertical
+// recurrence in single precision, accumulated into the contracted [e0|f0].
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void os_prim_quartet_f32(const QuartetGeomF &g, const float *P, const float *Q, float *v)
+{
+    constexpr int LT = LA + LB + LC + LD;
+    const float zeta = P[0], eta = Q[0];
+    const float PQ[3] = {P[2] - Q[2], P[3] - Q[3], P[4] - Q[4]};
+    const float rs = rsqrtf(zeta + eta), izpe = rs * rs;
+    const float T = zeta * eta * izpe * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
+    const float pre = P[5] * Q[5] * rs;
+    float F[LT + 1];
+    boys_os_f32<LT>(T, F);
+#pragma unroll
+    for (int m = 0; m <= LT; ++m) F[m] *= pre;
+    OsGeom<float> o;
+    const float rz = eta * izpe, re = zeta * izpe;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        o.PA[x] = P[2 + x] - g.A[x];
+        o.QC[x] = Q[2 + x] - g.C[x];
+        o.WP[x] = -rz * PQ[x];
+        o.WQ[x] = re * PQ[x];
+    }
+    o.rz = rz;
+    o.re = re;
+    o.oo2z = 0.5f * P[1];
+    o.oo2e = 0.5f * Q[1];
+    o.oo2ze = 0.5f * izpe;
+    OsClass<LA, LB, LC, LD>::template vrr<float>(o, F, v);
+}
+
 template <int LA, int LB, int LC, int LD, typename R, class Epi>
 __global__ void __launch_bounds__(128, thread_min_blocks(ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD)))
 eri_thread_kernel(const int4 *__restrict__ list, int nq,
@@ -537,6 +599,10 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
             float P[8], Qn[8];
             ld8f(pbp[ib].f, P);
             ld8f(pkp[ik].f, Qn);
+            using OS = OsClass<LA, LB, LC, LD>;
+            float v[OS::NV];
+#pragma unroll
+            for (int c = 0; c < OS::NV; ++c) v[c] = 0.0f;
             for (int t = 0; t < e.w; ++t) {
                 float Q[8];
 #pragma unroll
@@ -547,17 +613,78 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
                     ++ib2;
                 }
                 if (t + 1 < e.w) ld8f(pkp[ik2].f, Qn);
-                add_prim_quartet_f32<LA, LB, LC, LD>(gf, P, Q, reinterpret_cast<float *>(acc));
+                if constexpr (OS::kOn)
+                    os_prim_quartet_f32<LA, LB, LC, LD>(gf, P, Q, v);
+                else
+                    add_prim_quartet_f32<LA, LB, LC, LD>(gf, P, Q, reinterpret_cast<float *>(acc));
                 if (ib2 != ib && t + 1 < e.w) ld8f(pbp[ib2].f, P);
                 ib = ib2;
                 ik = ik2;
             }
+            if constexpr (OS::kOn) OS::template hrr<float>(gf.AB, gf.CD, v, reinterpret_cast<float *>(acc));
             const QCtx q = make_qctx(pb, pk, e.x, e.y);
             epi.template thread_quartet<LA, LB, LC, LD, R>(q, acc, lane, live);
             continue;
         }
         PrimJK P = load_prim_jk(pbp + ib);
         PrimJK Qn = load_prim_jk(pkp + ik);
+        if constexpr (OsClass<LA, LB, LC, LD>::kOn) {
+            // Obara--Saika per primitive quartet, Head-Gordon--Pople transfer
+            // once per item on the contracted [e0|f0]
+            using OS = OsClass<LA, LB, LC, LD>;
+            constexpr int LT = LA + LB + LC + LD;
+            R v[OS::NV];
+#pragma unroll
+            for (int c = 0; c < OS::NV; ++c) v[c] = (R)0;
+            for (int t = 0; t < e.w; ++t) {
+                const PrimJK Q = Qn;
+                int ik2 = ik + 1, ib2 = ib;
+                if (ik2 == npk) {
+                    ik2 = 0;
+                    ++ib2;
+                }
+                if (t + 1 < e.w) Qn = load_prim_jk(pkp + ik2);
+                const double zeta = P.zeta, eta = Q.zeta;
+                const double PQx = P.P[0] - Q.P[0], PQy = P.P[1] - Q.P[1], PQz = P.P[2] - Q.P[2];
+                const double rs = rsqrt_nr(zeta + eta);
+                const double izpe = rs * rs;
+                const double T = zeta * eta * izpe * (PQx * PQx + PQy * PQy + PQz * PQz);
+                const double pre = P.K * Q.K * rs;
+                double F[LT + 1];
+                boys_os<LT>(T, F);
+                R Fs[LT + 1];
+#pragma unroll
+                for (int m = 0; m <= LT; ++m) Fs[m] = (R)(F[m] * pre);
+                OsGeom<R> g;
+                const double rz = eta * izpe, re = zeta * izpe;
+                g.PA[0] = P.P[0] - Ax;
+                g.PA[1] = P.P[1] - Ay;
+                g.PA[2] = P.P[2] - Az;
+                g.QC[0] = Q.P[0] - Cx;
+                g.QC[1] = Q.P[1] - Cy;
+                g.QC[2] = Q.P[2] - Cz;
+                g.WP[0] = -rz * PQx;
+                g.WP[1] = -rz * PQy;
+                g.WP[2] = -rz * PQz;
+                g.WQ[0] = re * PQx;
+                g.WQ[1] = re * PQy;
+                g.WQ[2] = re * PQz;
+                g.rz = rz;
+                g.re = re;
+                g.oo2z = 0.5 * P.izeta;
+                g.oo2e = 0.5 * Q.izeta;
+                g.oo2ze = 0.5 * izpe;
+                OS::template vrr<R>(g, Fs, v);
+                if (ib2 != ib && t + 1 < e.w) P = load_prim_jk(pbp + ib2);
+                ib = ib2;
+                ik = ik2;
+            }
+            const R AB[3] = {(R)ABx, (R)ABy, (R)ABz}, CD[3] = {(R)CDx, (R)CDy, (R)CDz};
+            OS::template hrr<R>(AB, CD, v, acc);
+            const QCtx q = make_qctx(pb, pk, e.x, e.y);
+            epi.template thread_quartet<LA, LB, LC, LD, R>(q, acc, lane, live);
+            continue;
+        }
         for (int t = 0; t < e.w; ++t) {
             const PrimJK Q = Qn;
             // next primitive quartet's ket pair is fetched while this one computes

@@ -216,21 +216,30 @@ def main():
     print("worst relative error:", worst)
 
 
-# Compact Boys rows for the 1- and 2-root Fock-build kernels: for each order
-# M in BOYSROW_ORDERS and grid point T_k = k/32 (k = 0..BOYSROW_NGRID-1) one
-# 64-byte row [F_M(T_k), ..., F_{M+6}(T_k), exp(-T_k)], so a lane fetches
-# everything for F_M(T) (7-term Taylor, |T - T_k| <= 1/64) and exp(-T)
-# with two 256-bit loads.
+# Compact Boys rows for the Fock-build kernels, one 64-byte row per grid point
+# T_k = k/32 (k = 0..BOYSROW_NGRID-1), Taylor coefficients already divided by
+# j! so the device evaluates plain Horner polynomials in d = T_k - T
+# (|d| <= 1/64; F_m(T_k - d) = sum_j F_(m+j)(T_k) d^j / j! since
+# dF_m/dT = -F_(m+1)):
+#   pqb_boys_row1:  c_j = F_j(T_k)/j!, j = 0..7.  F_0 = P(d) and F_1 = P'(d)
+#                   of the same polynomial (truncation below 5e-17 relative),
+#                   with no exp(-T).
+#   pqb_boys_rowM, M = 3, 4:  c_j = F_(M+j)(T_k)/j!, j = 0..6, then exp(-T_k);
+#                   F_M by Horner, exp(-T) = exp(-T_k) exp(d), then the
+#                   downward recursion F_m = (2T F_(m+1) + exp(-T))/(2m+1).
+# FP32 copies (32 bytes) for the mixed-precision kernels: row1 c_0..c_4;
+# rowM c_0..c_3 and exp(-T_k) (4-term series: 3e-9 relative at |d| <= 1/64).
 BOYSROW_STEP_INV = 32
-BOYSROW_ORDERS = (1, 3)
+BOYSROW_ORDERS = (1, 3, 4)
 BOYSROW_NGRID = int(BOYS_TMAX * BOYSROW_STEP_INV) + 2
 
 
 def main_boys_rows():
     here = os.path.dirname(os.path.abspath(__file__))
     lines = ["// Generated by gen_tables.py --boys-rows -- do not edit.",
-             "// Row k of pqb_boys_rowM: F_M(T_k) .. F_(M+6)(T_k), exp(-T_k) at T_k = k/%d (40-digit mpmath)."
+             "// Row k at T_k = k/%d (40-digit mpmath): pqb_boys_row1 holds F_j(T_k)/j!, j = 0..7;"
              % BOYSROW_STEP_INV,
+             "// pqb_boys_rowM (M = 3, 4) holds F_(M+j)(T_k)/j!, j = 0..6, then exp(-T_k).",
              "#pragma once",
              "#define PQB_BOYSROW_STEP_INV %d" % BOYSROW_STEP_INV,
              "#define PQB_BOYSROW_NGRID %d" % BOYSROW_NGRID,
@@ -241,17 +250,17 @@ def main_boys_rows():
         rows[M] = []
         for k in range(BOYSROW_NGRID):
             T = mp.mpf(k) / BOYSROW_STEP_INV
-            row = [boys(M + j, T) for j in range(7)] + [mp.exp(-T)]
+            if M == 1:
+                row = [boys(j, T) / mp.factorial(j) for j in range(8)]
+            else:
+                row = [boys(M + j, T) / mp.factorial(j) for j in range(7)] + [mp.exp(-T)]
             rows[M].append(row)
             lines.append("  " + ", ".join("%.17e" % float(v) for v in row) + ",")
         lines.append("};")
-    # FP32 rows for the mixed-precision kernels: F_M .. F_(M+3)(T_k), exp(-T_k),
-    # three zeros (32 bytes: one 256-bit load; a 4-term Taylor series is
-    # accurate to 3e-9 relative for |T - T_k| <= 1/64)
     for M in BOYSROW_ORDERS:
         lines.append("PQB_TABQ __align__(64) float pqb_boys_row%d_f32[PQB_BOYSROW_NGRID * 8] = {" % M)
         for row in rows[M]:
-            vals = [row[0], row[1], row[2], row[3], row[7], 0, 0, 0]
+            vals = row[:5] + [0, 0, 0] if M == 1 else row[:4] + [row[7], 0, 0, 0]
             lines.append("  " + ", ".join("%.9ef" % float(v) for v in vals) + ",")
         lines.append("};")
     with open(os.path.join(here, "boys_rows.inc"), "w") as f:

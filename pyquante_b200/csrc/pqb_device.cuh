@@ -137,39 +137,102 @@ __device__ __forceinline__ void ld4(const double *p, double &a, double &b, doubl
         : "l"(__cvta_generic_to_global(p)));
 }
 
-// F_m(T), m = 0..M for M = 1 or 3, from one 64-byte row of pqb_boys_rowM
-// (boys_rows.inc: F_M .. F_(M+6) and exp(-T_k) at T_k = k/32): F_M by a
-// 7-term Taylor series about the nearest T_k (|T - T_k| <= 1/64, remainder
-// below 5e-17 F_M), exp(-T) = exp(-T_k) exp(-(T - T_k)) with an 8-term
-// series, then the downward recursion F_m = (2T F_(m+1) + exp(-T))/(2m+1).
-// T >= PQB_BOYSROW_TMAX uses the large-T forms of boys<M>.
-template <int M>
-__device__ __forceinline__ void boys_row(double T, double *F)
+// F_0 (NF = 1) or F_0, F_1 (NF = 2) from one 64-byte row of pqb_boys_row1
+// (boys_rows.inc: c_j = F_j(T_k)/j!, j = 0..7, T_k = k/32): with
+// d = T_k - T (|d| <= 1/64), F_0(T) = P(d) = sum_j c_j d^j and
+// F_1(T) = -dF_0/dT = P'(d), both by one Horner pass (truncation below
+// 5e-17 relative); no exp(-T).  For T >= PQB_BOYSROW_TMAX:
+// F_0 = sqrt(pi/T)/2 and F_1 = F_0/(2T), the exp(-T) term of F_1 being below
+// 3e-17 of it there.
+template <int NF>
+__device__ __forceinline__ void boys_row1(double T, double *F)
 {
-    static_assert(M == 1 || M == 3, "rows exist for M = 1 and 3");
+    static_assert(NF == 1 || NF == 2, "F_0 or F_0, F_1");
     if (T < PQB_BOYSROW_TMAX) {
         const int k = __double2int_rn(T * PQB_BOYSROW_STEP_INV);
-        const double d = k * (1.0 / PQB_BOYSROW_STEP_INV) - T;   // -(T - T_k)
-        const double *row = (M == 1 ? pqb_boys_row1 : pqb_boys_row3) + 8 * k;
-        double r[8];
-        ld4(row, r[0], r[1], r[2], r[3]);
-        ld4(row + 4, r[4], r[5], r[6], r[7]);
-        double f = r[6];
+        const double d = k * (1.0 / PQB_BOYSROW_STEP_INV) - T;
+        const double *row = pqb_boys_row1 + 8 * k;
+        double c[8];
+        ld4(row, c[0], c[1], c[2], c[3]);
+        ld4(row + 4, c[4], c[5], c[6], c[7]);
+        double p = c[7], q = 0.0;
 #pragma unroll
-        for (int j = 5; j >= 0; --j) f = fma(f, d * (1.0 / (j + 1)), r[j]);
+        for (int j = 6; j >= 0; --j) {
+            if (NF > 1) q = j == 6 ? p : fma(q, d, p);
+            p = fma(p, d, c[j]);
+        }
+        F[0] = p;
+        if (NF > 1) F[1] = q;
+    } else {
+        F[0] = 0.88622692545275801365 * rsqrt_nr(T);   // sqrt(pi)/2 / sqrt(T)
+        if (NF > 1) F[1] = F[0] * (0.5 * rcp_nr(T));
+    }
+}
+
+// F_m(T), m = 0..M for M = 3 or 4, from one 64-byte row of pqb_boys_rowM
+// (c_j = F_(M+j)(T_k)/j!, j = 0..6, and exp(-T_k)): F_M by Horner in
+// d = T_k - T, exp(-T) = exp(-T_k) exp(d) with a 7-term series (both below
+// 5e-17 relative for |d| <= 1/64), then the downward recursion
+// F_m = (2T F_(m+1) + exp(-T))/(2m+1).  T >= PQB_BOYSROW_TMAX: the large-T
+// forms F_0 = sqrt(pi/T)/2, F_(m+1) = ((2m+1) F_m - exp(-T))/(2T).
+template <int M>
+__device__ __forceinline__ void boys_rowm(double T, double *F)
+{
+    static_assert(M == 3 || M == 4, "rows exist for M = 3 and 4");
+    if (T < PQB_BOYSROW_TMAX) {
+        const int k = __double2int_rn(T * PQB_BOYSROW_STEP_INV);
+        const double d = k * (1.0 / PQB_BOYSROW_STEP_INV) - T;
+        const double *row = (M == 3 ? pqb_boys_row3 : pqb_boys_row4) + 8 * k;
+        double c[8];
+        ld4(row, c[0], c[1], c[2], c[3]);
+        ld4(row + 4, c[4], c[5], c[6], c[7]);
+        double f = c[6];
+#pragma unroll
+        for (int j = 5; j >= 0; --j) f = fma(f, d, c[j]);
         F[M] = f;
-        double ed = 1.0;
-#pragma unroll
-        for (int j = 8; j >= 1; --j) ed = fma(ed, d * (1.0 / j), 1.0);
-        const double e = r[7] * ed, t2 = 2.0 * T;
+        double ed = 1.0 / 720.0;
+        ed = fma(ed, d, 1.0 / 120.0);
+        ed = fma(ed, d, 1.0 / 24.0);
+        ed = fma(ed, d, 1.0 / 6.0);
+        ed = fma(ed, d, 0.5);
+        ed = fma(ed, d, 1.0);
+        ed = fma(ed, d, 1.0);
+        const double e = c[7] * ed, t2 = 2.0 * T;
 #pragma unroll
         for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * (1.0 / (2 * m + 1));
     } else {
         const double it = rcp_nr(T);
-        F[0] = 0.88622692545275801365 * rsqrt_nr(T);   // sqrt(pi)/2 / sqrt(T)
+        F[0] = 0.88622692545275801365 * rsqrt_nr(T);
         const double e = exp(-T), h = 0.5 * it;
 #pragma unroll
         for (int m = 0; m < M; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+    }
+}
+
+// F_m(T), m = 0..M for M = 1, 3 or 4 from the compact rows.
+template <int M>
+__device__ __forceinline__ void boys_row(double T, double *F)
+{
+    if constexpr (M == 1)
+        boys_row1<2>(T, F);
+    else
+        boys_rowm<M>(T, F);
+}
+
+// F_0 .. F_LT for the Obara--Saika classes (LT = LA+LB+LC+LD <= 4).
+template <int LT>
+__device__ __forceinline__ void boys_os(double T, double *F)
+{
+    static_assert(LT <= 4, "compact rows up to F_4");
+    if constexpr (LT <= 1) {
+        boys_row1<LT + 1>(T, F);
+    } else if constexpr (LT <= 3) {
+        double G[4];
+        boys_rowm<3>(T, G);
+#pragma unroll
+        for (int m = 0; m <= LT; ++m) F[m] = G[m];
+    } else {
+        boys_rowm<4>(T, F);
     }
 }
 
@@ -186,30 +249,86 @@ __device__ __forceinline__ void ld8f(const float *p, float *r)
         : "l"(__cvta_generic_to_global(p)));
 }
 
-// F_m(T), m = 0..M for M = 1 or 3, T < PQB_BOYSROW_TMAX, from one 32-byte row
-// of pqb_boys_rowM_f32 (F_M .. F_(M+3), exp(-T_k) at T_k = k/32): 4-term
-// Taylor series (remainder < 3e-9 F_M), exp(-T) = exp(-T_k) exp(-(T - T_k))
-// (4-term series), downward recursion.
-template <int M>
-__device__ __forceinline__ void boys_row_f32(float T, float *F)
+// Single-precision rows (T < PQB_BOYSROW_TMAX): row1_f32 holds
+// c_j = F_j(T_k)/j!, j = 0..4 (F_0 = P(d), F_1 = P'(d)); rowM_f32 (M = 3, 4)
+// holds F_(M+j)(T_k)/j!, j = 0..3, and exp(-T_k) (4-term series, 3e-9
+// relative at |d| <= 1/64), then the downward recursion.
+template <int NF>
+__device__ __forceinline__ void boys_row1_f32(float T, float *F)
 {
-    static_assert(M == 1 || M == 3, "rows exist for M = 1 and 3");
+    const int k = __float2int_rn(T * PQB_BOYSROW_STEP_INV);
+    const float d = k * (1.0f / PQB_BOYSROW_STEP_INV) - T;   // -(T - T_k)
+    float c[8];
+    ld8f(pqb_boys_row1_f32 + 8 * k, c);
+    float p = c[4], q = 0.0f;
+#pragma unroll
+    for (int j = 3; j >= 0; --j) {
+        if (NF > 1) q = j == 3 ? p : fmaf(q, d, p);
+        p = fmaf(p, d, c[j]);
+    }
+    F[0] = p;
+    if (NF > 1) F[1] = q;
+}
+
+template <int M>
+__device__ __forceinline__ void boys_rowm_f32(float T, float *F)
+{
+    static_assert(M == 3 || M == 4, "rows exist for M = 3 and 4");
     const int k = __float2int_rn(T * PQB_BOYSROW_STEP_INV);
     const float d = k * (1.0f / PQB_BOYSROW_STEP_INV) - T;   // -(T - T_k)
     float r[8];
-    ld8f((M == 1 ? pqb_boys_row1_f32 : pqb_boys_row3_f32) + 8 * k, r);
+    ld8f((M == 3 ? pqb_boys_row3_f32 : pqb_boys_row4_f32) + 8 * k, r);
     float f = r[3];
-    f = fmaf(f, d * (1.0f / 3.0f), r[2]);
-    f = fmaf(f, d * 0.5f, r[1]);
+    f = fmaf(f, d, r[2]);
+    f = fmaf(f, d, r[1]);
     f = fmaf(f, d, r[0]);
     F[M] = f;
-    float ed = fmaf(d, 1.0f / 4.0f, 1.0f);
-    ed = fmaf(d * (1.0f / 3.0f), ed, 1.0f);
-    ed = fmaf(d * 0.5f, ed, 1.0f);
-    ed = fmaf(d, ed, 1.0f);
+    float ed = fmaf(d, 1.0f / 6.0f, 0.5f);
+    ed = fmaf(ed, d, 1.0f);
+    ed = fmaf(ed, d, 1.0f);
     const float e = r[4] * ed, t2 = 2.0f * T;
 #pragma unroll
     for (int m = M - 1; m >= 0; --m) F[m] = fmaf(t2, F[m + 1], e) * (1.0f / (2 * m + 1));
+}
+
+template <int M>
+__device__ __forceinline__ void boys_row_f32(float T, float *F)
+{
+    if constexpr (M == 1)
+        boys_row1_f32<2>(T, F);
+    else
+        boys_rowm_f32<M>(T, F);
+}
+
+// F_0 .. F_LT in single precision for the Obara--Saika classes; above the
+// rows the large-T forms (in FP64, rounded afterwards).
+template <int LT>
+__device__ __forceinline__ void boys_os_f32(float T, float *F)
+{
+    static_assert(LT <= 4, "compact rows up to F_4");
+    if (T >= (float)PQB_BOYSROW_TMAX) {
+        const double Td = (double)T, it = rcp_nr(Td);
+        double G[LT + 1];
+        G[0] = 0.88622692545275801365 * rsqrt_nr(Td);
+        if (LT > 0) {
+            const double e = LT > 1 ? exp(-Td) : 0.0, h = 0.5 * it;
+#pragma unroll
+            for (int m = 0; m < LT; ++m) G[m + 1] = ((2 * m + 1) * G[m] - e) * h;
+        }
+#pragma unroll
+        for (int m = 0; m <= LT; ++m) F[m] = (float)G[m];
+        return;
+    }
+    if constexpr (LT <= 1) {
+        boys_row1_f32<LT + 1>(T, F);
+    } else if constexpr (LT <= 3) {
+        float G[4];
+        boys_rowm_f32<3>(T, G);
+#pragma unroll
+        for (int m = 0; m <= LT; ++m) F[m] = G[m];
+    } else {
+        boys_rowm_f32<4>(T, F);
+    }
 }
 
 // Root r of the n-point rule at T < pqb_rys_tasym[n] from the single-precision
