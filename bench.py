@@ -645,6 +645,17 @@ def main():
     e2e_ms = e2e("fp64")
     e2e_mixed_ms = e2e("mixed")
 
+    # UHF: two densities digesting every integral of one pass (pqb_jk_direct2)
+    # against one single-density build (the library replays its own graphs)
+    Db = (0.8 * D).contiguous()
+    uhf_ms = uhf_single_ms = None
+    if world == 1:
+        for _ in range(a.warmup):
+            eng.jk2(D, Db, "fp64", SCHWARZ, FP32_THRESH)
+            eng.jk(D, "fp64", SCHWARZ, FP32_THRESH, J=J, K=K)
+        uhf_ms = _timed(lambda: eng.jk2(D, Db, "fp64", SCHWARZ, FP32_THRESH), a.steps, stream, flush)
+        uhf_single_ms = _timed(lambda: eng.jk(D, "fp64", SCHWARZ, FP32_THRESH, J=J, K=K), a.steps, stream, flush)
+
     # roofline: per-class FP64 timing of the direct J/K kernels
     per_class = []
     nlaunch = 3   # density scaling and two symmetrise kernels per build
@@ -723,6 +734,9 @@ def main():
                          "peak_source": "measured DFMA probe (pqb_fp64_peak) on this GPU",
                          "slowest_class_alone": "(%d%d|%d%d)" % tuple(dom["cls"]),
                          "slowest_class_alone_tflops": dom["tflops"]},
+            "uhf_two_density": {"ms_per_build": uhf_ms, "single_density_ms": uhf_single_ms,
+                                "cost_vs_single": (uhf_ms / uhf_single_ms) if uhf_ms else None,
+                                "api": "BasisEngine.jk2 -> pqb_jk_direct2 (Ja, Ka, Jb, Kb in one pass), FP64"},
             "gpu_launches": nlaunch * a.steps,
             "clocks": clk.summary(),
         }

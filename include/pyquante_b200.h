@@ -137,6 +137,15 @@ int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream);
  * must not overlap on different streams (see PQB_PARAM_GRAPH). */
 int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode, void *stream);
 
+/* J and K of two densities from one pass over the integrals: every
+ * integral is evaluated once and digested against Da and Db.  Replaces the
+ * four calls getJ(Ints, Da), getJ(Ints, Db), getK(Ints, Da), getK(Ints, Db)
+ * of the reference's UHF iteration (PyQuante/hartree_fock.py:233-236, the
+ * same pattern in PyQuante2.py:200-202 and rohf.py:332-335).  Same rules as
+ * pqb_jk_direct for each density. */
+int pqb_jk_direct2(pqb_ctx *ctx, const double *Da, const double *Db, double *Ja, double *Ka, double *Jb, double *Kb,
+                   int mode, void *stream);
+
 /* One class list of the plan only (part 0 FP64 list / 1 FP32-eligible list,
  * class 0..20), accumulating unsymmetrised contributions into Jacc/Kacc
  * (not cleared).  The contributions are those of the element-scaled density

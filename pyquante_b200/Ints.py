@@ -23,7 +23,7 @@ from . import _lib
 from .Basis.basis import BasisSet, sym2powerlist  # noqa: F401  (re-exported like the reference)
 from .engine import BasisEngine, FunctionTable, eri_functions, jk_packed, oneint
 
-__all__ = ["getbasis", "getints", "get1ints", "get2ints", "getJ", "getK", "get2JmK", "getS", "getT", "getV",
+__all__ = ["getbasis", "getints", "get1ints", "get2ints", "getJ", "getK", "get2JmK", "getJK2", "getS", "getT", "getV",
            "ijkl2intindex", "PackedInts", "DirectInts", "sym2powerlist"]
 
 
@@ -216,6 +216,31 @@ def _jk(Ints, D):
         t = torch.as_tensor(np.asarray(Ints, dtype=np.float64), device="cuda")
     Dd, _ = _as_device(D, t.device)
     return jk_packed(t.contiguous(), Dd)
+
+
+def getJK2(Ints, Da, Db):
+    """(Ja, Jb, Ka, Kb) of two densities: the four calls getJ(Ints, Da),
+    getJ(Ints, Db), getK(Ints, Da), getK(Ints, Db) of the reference's UHF
+    iteration (PyQuante/hartree_fock.py:233-236).  Integral-direct handles
+    evaluate every integral once for both densities (pqb_jk_direct2); stored
+    integrals run one build per density.  Both results are remembered like a
+    getJ/getK build, so later getJ/getK calls with either density reuse them."""
+    if isinstance(Ints, DirectInts):
+        Dad, _ = _as_device(Da, Ints.engine.device)
+        Dbd, _ = _as_device(Db, Ints.engine.device)
+        if Dad.shape == Dbd.shape and torch.equal(Dad, Dbd):
+            J, K = _jk(Ints, Da)
+            return _back(J, Da), _back(J.clone(), Db), _back(K, Da), _back(K.clone(), Db)
+        Ja, Ka, Jb, Kb = Ints.engine.jk2(Dad, Dbd, Ints.precision, Ints.schwarz, Ints.fp32_threshold)
+        key = (Ints.precision, Ints.schwarz, Ints.fp32_threshold)
+        cache = Ints.__dict__.setdefault("_jk_cache", [])
+        for Dd, J, K in ((Dbd, Jb, Kb), (Dad, Ja, Ka)):
+            cache.insert(0, (key, Dd.clone(), J.clone(), K.clone()))
+        del cache[_JK_CACHE:]
+        return _back(Ja, Da), _back(Jb, Db), _back(Ka, Da), _back(Kb, Db)
+    Ja, Ka = _jk(Ints, Da)
+    Jb, Kb = _jk(Ints, Db)
+    return _back(Ja, Da), _back(Jb, Db), _back(Ka, Da), _back(Kb, Db)
 
 
 def getJ(Ints, D):

@@ -184,11 +184,13 @@ struct WarpRuns {
 // blocks (ab, cd, ac, ad, bc, bd) are summed in registers, and each block
 // element goes to global memory with one atomic.  Block mode: the weighted
 // integrals go to a shared tile; each output element is then one thread's
-// reduction over the tile (no shared-memory atomics).
-struct EpiJK {
-    const double *D;        // pre-scaled density
-    double *Jacc, *Kacc;
-    const float *Df;        // its single-precision copy (FP32 lists of the mixed mode), or null
+// reduction over the tile (no shared-memory atomics).  With NDEN = 2 both
+// densities are digested from the same integrals (UHF).
+template <int NDEN>
+struct EpiJKn {
+    const double *D[NDEN];        // pre-scaled densities
+    double *Jacc[NDEN], *Kacc[NDEN];
+    const float *Df[NDEN];        // their single-precision copies (FP32 lists of the mixed mode), or null
     static constexpr bool kTile = true;
 
     // (called by every lane of the warp; a lane past the end of the item list
@@ -206,12 +208,15 @@ struct EpiJK {
         // Kacc[b,c] by lanes that also share the ket's first shell
         const WarpRuns rb((long long)q.bra, lane);
         const WarpRuns rbc(((long long)q.bra << 32) | (unsigned)q.sc, lane);
+        // every density digests the same integrals, one after the other
+#pragma unroll
+        for (int s = 0; s < NDEN; ++s) {
         const T *Db;
         if constexpr (std::is_same_v<T, float>)
-            Db = Df + q.bo;
+            Db = Df[s] + q.bo;
         else
-            Db = D + q.bo;
-        double *Jb = Jacc + q.bo, *Kb = Kacc + q.bo;
+            Db = D[s] + q.bo;
+        double *Jb = Jacc[s] + q.bo, *Kb = Kacc[s] + q.bo;
         const int64_t nm = q.nm;
         const T *Da = Db + q.fa * nm, *Dbr = Db + q.fb * nm, *Dc = Db + q.fc * nm;
         // Coulomb: Jacc[a,b] and Jacc[c,d]
@@ -327,6 +332,7 @@ struct EpiJK {
                     if (kbd[d] != (T)0) atomicAdd(Kb + (q.fb + b) * nm + q.fd + d, (double)kbd[d]);
             }
         }
+        }
     }
 
     // block mode: the tile row of bra component (ia, ib) holds its NCD
@@ -341,11 +347,12 @@ struct EpiJK {
         constexpr int ST = kTileStride<LA, LB, LC, LD>;
         const bool bd = q.sa == q.sb, kd = q.sc == q.sd, qd = q.bra == q.ket, af = q.fa > q.fb;
         const int64_t nm = q.nm;
-        const double *Dc = D + q.bo + q.fc * nm + q.fd;
         // runtime bra indices: the bra and quartet factors of comp_weight in closed form
         const double wb = bd ? (ia > ib ? 1.0 : (ia == ib ? 0.5 : 0.0)) : 1.0;
         const int x0 = (bd || af) ? ia : ib, y0 = (bd || af) ? ib : ia;
-        double jab = 0.0;
+        double jab[NDEN];
+#pragma unroll
+        for (int s = 0; s < NDEN; ++s) jab[s] = 0.0;
         double *row = V + (ia * NB + ib) * ST;
 #pragma unroll
         for (int c = 0; c < NC; ++c)
@@ -356,10 +363,13 @@ struct EpiJK {
                 const double wq = qd ? (x0 != x1 ? (x0 > x1 ? 1.0 : 0.0) : (y0 != y1 ? (y0 > y1 ? 1.0 : 0.0) : 0.5))
                                      : 1.0;
                 const double v = (double)acc[c * ND + d] * (wb * wk * wq);
-                jab = fma(v, __ldg(Dc + c * nm + d), jab);
+#pragma unroll
+                for (int s = 0; s < NDEN; ++s) jab[s] = fma(v, __ldg(D[s] + q.bo + (q.fc + c) * nm + q.fd + d), jab[s]);
                 row[c * ND + d] = v;
             }
-        if (jab != 0.0) atomicAdd(Jacc + q.bo + (q.fa + ia) * nm + q.fb + ib, 2.0 * jab);
+#pragma unroll
+        for (int s = 0; s < NDEN; ++s)
+            if (jab[s] != 0.0) atomicAdd(Jacc[s] + q.bo + (q.fa + ia) * nm + q.fb + ib, 2.0 * jab[s]);
     }
 
     // outputs of one quartet: Jacc[c,d] (NCD), Kacc[a,c], Kacc[a,d],
@@ -371,7 +381,10 @@ struct EpiJK {
         constexpr int ST = kTileStride<LA, LB, LC, LD>;
         constexpr int O1 = NCD, O2 = O1 + NA * NC, O3 = O2 + NA * ND, O4 = O3 + NB * NC, O5 = O4 + NB * ND;
         const int64_t nm = q.nm;
-        const double *Db = D + q.bo;
+#pragma unroll
+        for (int sd = 0; sd < NDEN; ++sd) {
+        const double *Db = D[sd] + q.bo;
+        double *Jo = Jacc[sd], *Ko = Kacc[sd];
         for (int o = t; o < O5; o += nt) {
             double s = 0.0;
             double *dst;
@@ -381,36 +394,44 @@ struct EpiJK {
                     for (int b = 0; b < NB; ++b)
                         s = fma(V[(a * NB + b) * ST + c * ND + d], __ldg(Db + (q.fa + a) * nm + q.fb + b), s);
                 s *= 2.0;
-                dst = Jacc + q.bo + (q.fc + c) * nm + q.fd + d;
+                dst = Jo + q.bo + (q.fc + c) * nm + q.fd + d;
             } else if (o < O2) {              // Kacc[a,c] = sum_bd v D_bd
                 const int a = (o - O1) / NC, c = (o - O1) - ((o - O1) / NC) * NC;
                 for (int b = 0; b < NB; ++b)
                     for (int d = 0; d < ND; ++d)
                         s = fma(V[(a * NB + b) * ST + c * ND + d], __ldg(Db + (q.fb + b) * nm + q.fd + d), s);
-                dst = Kacc + q.bo + (q.fa + a) * nm + q.fc + c;
+                dst = Ko + q.bo + (q.fa + a) * nm + q.fc + c;
             } else if (o < O3) {              // Kacc[a,d] = sum_bc v D_bc
                 const int a = (o - O2) / ND, d = (o - O2) - ((o - O2) / ND) * ND;
                 for (int b = 0; b < NB; ++b)
                     for (int c = 0; c < NC; ++c)
                         s = fma(V[(a * NB + b) * ST + c * ND + d], __ldg(Db + (q.fb + b) * nm + q.fc + c), s);
-                dst = Kacc + q.bo + (q.fa + a) * nm + q.fd + d;
+                dst = Ko + q.bo + (q.fa + a) * nm + q.fd + d;
             } else if (o < O4) {              // Kacc[b,c] = sum_ad v D_ad
                 const int b = (o - O3) / NC, c = (o - O3) - ((o - O3) / NC) * NC;
                 for (int a = 0; a < NA; ++a)
                     for (int d = 0; d < ND; ++d)
                         s = fma(V[(a * NB + b) * ST + c * ND + d], __ldg(Db + (q.fa + a) * nm + q.fd + d), s);
-                dst = Kacc + q.bo + (q.fb + b) * nm + q.fc + c;
+                dst = Ko + q.bo + (q.fb + b) * nm + q.fc + c;
             } else {                          // Kacc[b,d] = sum_ac v D_ac
                 const int b = (o - O4) / ND, d = (o - O4) - ((o - O4) / ND) * ND;
                 for (int a = 0; a < NA; ++a)
                     for (int c = 0; c < NC; ++c)
                         s = fma(V[(a * NB + b) * ST + c * ND + d], __ldg(Db + (q.fa + a) * nm + q.fc + c), s);
-                dst = Kacc + q.bo + (q.fb + b) * nm + q.fd + d;
+                dst = Ko + q.bo + (q.fb + b) * nm + q.fd + d;
             }
             if (s != 0.0) atomicAdd(dst, s);
         }
+        }
     }
 };
+
+// One density (RHF, or one spin at a time) and two (UHF's alpha and beta
+// densities digesting the same integrals in one pass).
+using EpiJK = EpiJKn<1>;
+using EpiJK2 = EpiJKn<2>;
+
+
 
 // Schwarz: Q2[pair] = max over components of |(ij|ij)| (diagonal quartets).
 struct EpiSchwarz {

@@ -11,7 +11,7 @@ cudaError_t launch_jk_f32(int qc, const int4 *list, int nq, const PairInfo *pair
                           cudaStream_t st, int nsm)
 {
     (void)n;
-    EpiJK epi{Dscaled, Jacc, Kacc, Dscaled_f};
+    EpiJK epi{{Dscaled}, {Jacc}, {Kacc}, {Dscaled_f}};
     return launch_eri<float>(qc, list, nq, pairs, prims, epi, st, nsm);
 }
 }  // namespace pqb

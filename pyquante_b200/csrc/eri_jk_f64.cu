@@ -7,7 +7,7 @@ cudaError_t launch_jk_f64(int qc, const int4 *list, int nq, const PairInfo *pair
                           const double *Dscaled, double *Jacc, double *Kacc, int n, cudaStream_t st, int nsm)
 {
     (void)n;
-    EpiJK epi{Dscaled, Jacc, Kacc, nullptr};
+    EpiJK epi{{Dscaled}, {Jacc}, {Kacc}, {nullptr}};
     return launch_eri<double>(qc, list, nq, pairs, prims, epi, st, nsm);
 }
 }  // namespace pqb

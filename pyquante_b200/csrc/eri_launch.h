@@ -12,7 +12,7 @@
 
 namespace pqb {
 struct EpiPacked;
-struct EpiJK;
+template <int NDEN> struct EpiJKn;
 struct EpiSchwarz;
 
 cudaError_t launch_packed_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
@@ -22,6 +22,13 @@ cudaError_t launch_jk_f64(int qc, const int4 *list, int nq, const PairInfo *pair
 cudaError_t launch_jk_f32(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                           const double *Dscaled, const float *Dscaled_f, double *Jacc, double *Kacc, int n,
                           cudaStream_t st, int nsm);
+// two densities (UHF alpha and beta) digesting the same integrals
+cudaError_t launch_jk2_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+                           const double *const Dscaled[2], double *const Jacc[2], double *const Kacc[2],
+                           cudaStream_t st, int nsm);
+cudaError_t launch_jk2_f32(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+                           const double *const Dscaled[2], const float *const Dscaled_f[2], double *const Jacc[2],
+                           double *const Kacc[2], cudaStream_t st, int nsm);
 cudaError_t launch_schwarz_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                                unsigned long long *Q2bits, const double *fscale, cudaStream_t st, int nsm);
 cudaError_t launch_grad_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,

@@ -48,6 +48,8 @@ struct pqb_ctx {
     // d_Dscaled, and J, K are scaled by the same factors when symmetrised
     double *d_escale = nullptr, *d_Dscaled = nullptr;
     float *d_Dscaled_f = nullptr;    // single-precision copy for the FP32 lists
+    double *d_Dscaled2 = nullptr;    // the second density of pqb_jk_direct2 (allocated on first use)
+    float *d_Dscaled2_f = nullptr;
     unsigned long long *d_q2 = nullptr;
     std::vector<PairInfo> pairs;
     std::vector<double> Q;           // Schwarz factors (host)
@@ -90,9 +92,11 @@ struct pqb_ctx {
     bool use_graph = true;
     int plan_threads = 0;            // host threads of pqb_plan (0: automatic)
     cudaStream_t cap_stream = nullptr;
-    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
-    bool graph_warm[2] = {false, false};   // one eager build first (one-time launch setup stays out of the capture)
+    // graphs: [mode] for one density, [2 + mode] for two (pqb_jk_direct2)
+    cudaGraphExec_t graph_exec[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool graph_warm[4] = {false, false, false, false};   // one eager build first (one-time launch setup stays out of the capture)
     double *d_Jacc = nullptr, *d_Kacc = nullptr;
+    double *d_Jacc2 = nullptr, *d_Kacc2 = nullptr;   // second density's graph accumulators
     // small scratch
     double *d_atoms = nullptr;
     size_t atoms_cap = 0;
@@ -1137,7 +1141,7 @@ static cudaError_t ensure_streams(pqb_ctx *ctx)
 
 static void drop_graphs(pqb_ctx *ctx)
 {
-    for (int gi = 0; gi < 2; ++gi) {
+    for (int gi = 0; gi < 4; ++gi) {
         if (ctx->graph_exec[gi]) cudaGraphExecDestroy(ctx->graph_exec[gi]);
         ctx->graph_exec[gi] = nullptr;
         ctx->graph_warm[gi] = false;
@@ -1149,7 +1153,13 @@ static void release_basis(pqb_ctx *ctx)
     drop_graphs(ctx);
     free_dev(ctx->d_Jacc);
     free_dev(ctx->d_Kacc);
-    ctx->d_Jacc = ctx->d_Kacc = nullptr;
+    free_dev(ctx->d_Jacc2);
+    free_dev(ctx->d_Kacc2);
+    ctx->d_Jacc = ctx->d_Kacc = ctx->d_Jacc2 = ctx->d_Kacc2 = nullptr;
+    free_dev(ctx->d_Dscaled2);
+    free_dev(ctx->d_Dscaled2_f);
+    ctx->d_Dscaled2 = nullptr;
+    ctx->d_Dscaled2_f = nullptr;
     free_dev(ctx->d_pairs);
     free_dev(ctx->d_prims);
     free_dev(ctx->d_fscale);
@@ -1755,15 +1765,20 @@ int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
     }
 }
 
-// The class launches of one build into the accumulators Jacc, Kacc (zeroed
-// here) on stream st, forked over the context's streams and joined back;
-// they read the scaled density in d_Dscaled / d_Dscaled_f.
-static int launch_build(pqb_ctx *ctx, double *Jacc, double *Kacc, int mode, cudaStream_t st)
+// The class launches of one build into the accumulators Jacc[s], Kacc[s]
+// (zeroed here) of nden = 1 or 2 densities on stream st, forked over the
+// context's streams and joined back; they read the scaled densities
+// (d_Dscaled / d_Dscaled_f, and d_Dscaled2 / d_Dscaled2_f for the second).
+static int launch_build(pqb_ctx *ctx, int nden, double *const Jacc[2], double *const Kacc[2], int mode,
+                        cudaStream_t st)
 {
     const int n = ctx->nbf;
-    PQB_CK(ctx, cudaMemsetAsync(Jacc, 0, sizeof(double) * ctx->dense_len, st));
-    PQB_CK(ctx, cudaMemsetAsync(Kacc, 0, sizeof(double) * ctx->dense_len, st));
-    const double *Ds = ctx->d_Dscaled;
+    for (int s = 0; s < nden; ++s) {
+        PQB_CK(ctx, cudaMemsetAsync(Jacc[s], 0, sizeof(double) * ctx->dense_len, st));
+        PQB_CK(ctx, cudaMemsetAsync(Kacc[s], 0, sizeof(double) * ctx->dense_len, st));
+    }
+    const double *Ds[2] = {ctx->d_Dscaled, ctx->d_Dscaled2};
+    const float *Dsf[2] = {ctx->d_Dscaled_f, ctx->d_Dscaled2_f};
     // fork: class launches spread over the context's streams, heaviest first
     PQB_CK(ctx, cudaEventRecord(ctx->ev_fork, st));
     for (int k = 0; k < pqb_ctx::kStreams; ++k) PQB_CK(ctx, cudaStreamWaitEvent(ctx->streams[k], ctx->ev_fork, 0));
@@ -1777,18 +1792,26 @@ static int launch_build(pqb_ctx *ctx, double *Jacc, double *Kacc, int mode, cuda
         cost[i] = ctx->order == 1 ? (double)(c * 2 + (1 - part))
                                   : (double)ctx->plan_prims[part][c] * (1 + c) * (part == 1 && mode == PQB_MIXED ? 0.5 : 1.0);
     }
-    std::sort(order, order + 2 * kNumQuartetClass, [&](int a, int b) { return cost[a] > cost[b]; });
+    std::sort(order, order + 2 * kNumQuartetClass, [&](int x, int y) { return cost[x] > cost[y]; });
     for (int i = 0, k = 0; i < 2 * kNumQuartetClass; ++i) {
         const int part = order[i] / kNumQuartetClass, c = order[i] % kNumQuartetClass;
         const int nq = (int)ctx->plan_cnt[part][c];
         if (nq == 0) continue;
         cudaStream_t sk = ctx->streams[k++ % ctx->nstreams];
         const int4 *list = ctx->d_plan + ctx->plan_off[part][c];
-        if (part == 1 && mode == PQB_MIXED)
-            PQB_CK(ctx, launch_jk_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, ctx->d_Dscaled_f, Jacc, Kacc, n, sk,
+        const bool f32 = part == 1 && mode == PQB_MIXED;
+        if (nden == 2) {
+            if (f32)
+                PQB_CK(ctx, launch_jk2_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, Dsf, Jacc, Kacc, sk, ctx->nsm));
+            else
+                PQB_CK(ctx, launch_jk2_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, Jacc, Kacc, sk, ctx->nsm));
+        } else if (f32) {
+            PQB_CK(ctx, launch_jk_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds[0], Dsf[0], Jacc[0], Kacc[0], n, sk,
                                       ctx->nsm));
-        else
-            PQB_CK(ctx, launch_jk_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, Jacc, Kacc, n, sk, ctx->nsm));
+        } else {
+            PQB_CK(ctx, launch_jk_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds[0], Jacc[0], Kacc[0], n, sk,
+                                      ctx->nsm));
+        }
     }
     // join
     for (int k = 0; k < pqb_ctx::kStreams; ++k) {
@@ -1798,29 +1821,38 @@ static int launch_build(pqb_ctx *ctx, double *Jacc, double *Kacc, int mode, cuda
     return PQB_OK;
 }
 
-// Capture launch_build into the ctx-owned accumulators as a graph for mode
-// (index gi), once; later builds replay it with one launch.
-static int ensure_build_graph(pqb_ctx *ctx, int mode, int gi)
+// Both accumulators of a pair or neither: a failed second allocation leaves
+// no half-made pair behind.
+static int ensure_acc_pair(pqb_ctx *ctx, double *&J, double *&K)
+{
+    if (J && K) return PQB_OK;
+    free_dev(J);
+    free_dev(K);
+    J = K = nullptr;
+    const size_t bytes = sizeof(double) * std::max<long long>(ctx->dense_len, 1);
+    cudaError_t e = cudaMalloc(&J, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&K, bytes);
+    if (e != cudaSuccess) {
+        free_dev(J);
+        free_dev(K);
+        J = K = nullptr;
+        return fail(ctx, PQB_E_CUDA, "graph accumulators: %s", cudaGetErrorString(e));
+    }
+    return PQB_OK;
+}
+
+// Capture launch_build into the ctx-owned accumulators as a graph for
+// (nden, mode) (index gi), once; later builds replay it with one launch.
+static int ensure_build_graph(pqb_ctx *ctx, int nden, int mode, int gi)
 {
     if (ctx->graph_exec[gi]) return PQB_OK;
     if (!ctx->cap_stream) PQB_CK(ctx, cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
-    if (!ctx->d_Jacc || !ctx->d_Kacc) {
-        // both or neither: a failed second allocation leaves no half-made pair
-        free_dev(ctx->d_Jacc);
-        free_dev(ctx->d_Kacc);
-        ctx->d_Jacc = ctx->d_Kacc = nullptr;
-        const size_t bytes = sizeof(double) * std::max<long long>(ctx->dense_len, 1);
-        cudaError_t e = cudaMalloc(&ctx->d_Jacc, bytes);
-        if (e == cudaSuccess) e = cudaMalloc(&ctx->d_Kacc, bytes);
-        if (e != cudaSuccess) {
-            free_dev(ctx->d_Jacc);
-            free_dev(ctx->d_Kacc);
-            ctx->d_Jacc = ctx->d_Kacc = nullptr;
-            return fail(ctx, PQB_E_CUDA, "graph accumulators: %s", cudaGetErrorString(e));
-        }
-    }
+    int rc = ensure_acc_pair(ctx, ctx->d_Jacc, ctx->d_Kacc);
+    if (rc == PQB_OK && nden == 2) rc = ensure_acc_pair(ctx, ctx->d_Jacc2, ctx->d_Kacc2);
+    if (rc != PQB_OK) return rc;
+    double *const Ja[2] = {ctx->d_Jacc, ctx->d_Jacc2}, *const Ka[2] = {ctx->d_Kacc, ctx->d_Kacc2};
     PQB_CK(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
-    const int rc = launch_build(ctx, ctx->d_Jacc, ctx->d_Kacc, mode, ctx->cap_stream);
+    rc = launch_build(ctx, nden, Ja, Ka, mode, ctx->cap_stream);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(ctx->cap_stream, &g);   // always ends the capture
     if (rc != PQB_OK || e != cudaSuccess) {
@@ -1836,44 +1868,83 @@ static int ensure_build_graph(pqb_ctx *ctx, int mode, int gi)
     return PQB_OK;
 }
 
+// J and K of nden densities D[s] into J[s], K[s].
+static int jk_direct_impl(pqb_ctx *ctx, int nden, const double *const D[2], double *const J[2], double *const K[2],
+                          int mode, void *stream)
+{
+    const int n = ctx->nbf;
+    cudaStream_t st = (cudaStream_t)stream;
+    PQB_CK(ctx, ensure_streams(ctx));
+    if (nden == 2 && !ctx->d_Dscaled2) {
+        const size_t len = std::max<long long>(ctx->dense_len, 1);
+        PQB_CK(ctx, cudaMalloc(&ctx->d_Dscaled2, sizeof(double) * len));
+        const cudaError_t e = cudaMalloc(&ctx->d_Dscaled2_f, sizeof(float) * len);
+        if (e != cudaSuccess) {
+            free_dev(ctx->d_Dscaled2);
+            ctx->d_Dscaled2 = nullptr;
+            ctx->d_Dscaled2_f = nullptr;
+            return fail(ctx, PQB_E_CUDA, "second scaled density: %s", cudaGetErrorString(e));
+        }
+    }
+    double *Dsc[2] = {ctx->d_Dscaled, ctx->d_Dscaled2};
+    float *Dsf[2] = {ctx->d_Dscaled_f, ctx->d_Dscaled2_f};
+    for (int s = 0; s < nden; ++s)
+        scale_elements_kernel<<<ctx->nsm * 4, 256, 0, st>>>(D[s], ctx->d_escale, Dsc[s], Dsf[s], ctx->dense_len);
+    const int64_t P = (int64_t)n * (n + 1) / 2;
+    // graph replay for a single molecule when the caller is not capturing
+    // (a caller's own capture records the launches themselves)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PQB_CK(ctx, cudaStreamIsCapturing(st, &cs));
+    const int gi = (nden == 2 ? 2 : 0) + (mode == PQB_MIXED ? 1 : 0);
+    if (ctx->use_graph && ctx->nmol == 1 && cs == cudaStreamCaptureStatusNone && ctx->graph_warm[gi]) {
+        const int rc = ensure_build_graph(ctx, nden, mode, gi);
+        if (rc != PQB_OK) return rc;
+        PQB_CK(ctx, cudaGraphLaunch(ctx->graph_exec[gi], st));
+        const double *Ja[2] = {ctx->d_Jacc, ctx->d_Jacc2}, *Ka[2] = {ctx->d_Kacc, ctx->d_Kacc2};
+        for (int s = 0; s < nden; ++s) {
+            symmetrize_into_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(Ja[s], J[s], n, ctx->d_escale);
+            symmetrize_into_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(Ka[s], K[s], n, ctx->d_escale);
+        }
+        PQB_CK(ctx, cudaGetLastError());
+        return PQB_OK;
+    }
+    const int rc = launch_build(ctx, nden, J, K, mode, st);
+    if (rc != PQB_OK) return rc;
+    if (cs == cudaStreamCaptureStatusNone) ctx->graph_warm[gi] = true;
+    for (int s = 0; s < nden; ++s) {
+        if (ctx->nmol == 1) {
+            symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J[s], n, ctx->d_escale);
+            symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K[s], n, ctx->d_escale);
+        } else {
+            symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(J[s], ctx->d_mol_off, ctx->d_mol_n, ctx->d_escale);
+            symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(K[s], ctx->d_mol_off, ctx->d_mol_n, ctx->d_escale);
+        }
+    }
+    PQB_CK(ctx, cudaGetLastError());
+    return PQB_OK;
+}
+
 int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode, void *stream)
 {
     if (!ctx || !D || !J || !K) return fail(ctx, PQB_E_ARG, "pqb_jk_direct: bad arguments");
     if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_jk_direct: call pqb_plan first");
     if (mode != PQB_FP64 && mode != PQB_MIXED) return fail(ctx, PQB_E_ARG, "pqb_jk_direct: mode %d", mode);
     PQB_CK(ctx, cudaSetDevice(ctx->device));
-    cudaStream_t st = (cudaStream_t)stream;
-    const int n = ctx->nbf;
-    PQB_CK(ctx, ensure_streams(ctx));
-    scale_elements_kernel<<<ctx->nsm * 4, 256, 0, st>>>(D, ctx->d_escale, ctx->d_Dscaled, ctx->d_Dscaled_f,
-                                                         ctx->dense_len);
-    const int64_t P = (int64_t)n * (n + 1) / 2;
-    // graph replay for a single molecule when the caller is not capturing
-    // (a caller's own capture records the launches themselves)
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    PQB_CK(ctx, cudaStreamIsCapturing(st, &cs));
-    const int gi = mode == PQB_MIXED ? 1 : 0;
-    if (ctx->use_graph && ctx->nmol == 1 && cs == cudaStreamCaptureStatusNone && ctx->graph_warm[gi]) {
-        const int rc = ensure_build_graph(ctx, mode, gi);
-        if (rc != PQB_OK) return rc;
-        PQB_CK(ctx, cudaGraphLaunch(ctx->graph_exec[gi], st));
-        symmetrize_into_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(ctx->d_Jacc, J, n, ctx->d_escale);
-        symmetrize_into_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(ctx->d_Kacc, K, n, ctx->d_escale);
-        PQB_CK(ctx, cudaGetLastError());
-        return PQB_OK;
-    }
-    const int rc = launch_build(ctx, J, K, mode, st);
-    if (rc != PQB_OK) return rc;
-    if (cs == cudaStreamCaptureStatusNone) ctx->graph_warm[gi] = true;
-    if (ctx->nmol == 1) {
-        symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J, n, ctx->d_escale);
-        symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K, n, ctx->d_escale);
-    } else {
-        symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(J, ctx->d_mol_off, ctx->d_mol_n, ctx->d_escale);
-        symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(K, ctx->d_mol_off, ctx->d_mol_n, ctx->d_escale);
-    }
-    PQB_CK(ctx, cudaGetLastError());
-    return PQB_OK;
+    const double *Dv[2] = {D, nullptr};
+    double *Jv[2] = {J, nullptr}, *Kv[2] = {K, nullptr};
+    return jk_direct_impl(ctx, 1, Dv, Jv, Kv, mode, stream);
+}
+
+int pqb_jk_direct2(pqb_ctx *ctx, const double *Da, const double *Db, double *Ja, double *Ka, double *Jb, double *Kb,
+                   int mode, void *stream)
+{
+    if (!ctx || !Da || !Db || !Ja || !Ka || !Jb || !Kb) return fail(ctx, PQB_E_ARG, "pqb_jk_direct2: bad arguments");
+    if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_jk_direct2: call pqb_plan first");
+    if (mode != PQB_FP64 && mode != PQB_MIXED) return fail(ctx, PQB_E_ARG, "pqb_jk_direct2: mode %d", mode);
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    const double *Dv[2] = {Da, Db};
+    double *Jv[2] = {Ja, Jb}, *Kv[2] = {Ka, Kb};
+    return jk_direct_impl(ctx, 2, Dv, Jv, Kv, mode, stream);
 }
 
 int pqb_dense_len(const pqb_ctx *ctx, int64_t *len)

@@ -218,6 +218,19 @@ class BasisEngine:
         self.ctx.check(self.ctx.lib.pqb_jk_direct(self.ctx.h, ptr(D), ptr(J), ptr(K), m, stream_ptr(stream)))
         return J, K
 
+    def jk2(self, Da, Db, mode="fp64", schwarz=1e-12, fp32_threshold=1e-5, stream=None):
+        """J and K of two densities (UHF alpha and beta) from one pass over the
+        integrals: (Ja, Ka, Jb, Kb)."""
+        self._need_shells()
+        self.plan(schwarz, fp32_threshold)
+        Da = Da.to(device=self.device, dtype=torch.float64).contiguous()
+        Db = Db.to(device=self.device, dtype=torch.float64).contiguous()
+        out = [torch.empty_like(Da) for _ in range(4)]
+        m = _lib.PQB_MIXED if mode == "mixed" else _lib.PQB_FP64
+        self.ctx.check(self.ctx.lib.pqb_jk_direct2(self.ctx.h, ptr(Da), ptr(Db), *(ptr(x) for x in out), m,
+                                                   stream_ptr(stream)))
+        return tuple(out)
+
     def oneint(self, atoms, stream=None):
         return oneint(self.ft, atoms, self.ctx, stream)
 

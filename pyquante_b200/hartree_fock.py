@@ -11,7 +11,7 @@ import numpy as np
 import torch
 
 from .Convergence import DIIS
-from .Ints import get2JmK, getbasis, getints, getJ, getK
+from .Ints import get2JmK, getbasis, getints, getJ, getJK2, getK  # noqa: F401  (getJ/getK re-exported)
 from .LA2 import geigh, mkdens, trace2
 
 logger = logging.getLogger("pyquante")
@@ -89,8 +89,9 @@ def uhf(atoms, **opts):
     """Unrestricted HF (PyQuante/hartree_fock.py:151-253): defaults
     ConvCriteria 1e-5, MaxIter 40, density averaging 0.5 on; F_a = h + J_a +
     J_b - K_a; E = (E_a + E_b)/2 + E_nuc with E_x = tr(D_x h) + tr(D_x F_x).
-    The J/K of both densities come from the same engine call pattern as
-    the reference (getJ/getK)."""
+    The reference's getJ(Da), getJ(Db), getK(Da), getK(Db) come from one
+    getJK2 call: integral-direct, both densities digest every integral of
+    one pass."""
     ConvCriteria = opts.get("ConvCriteria", 1e-5)
     MaxIter = opts.get("MaxIter", 40)
     DoAveraging = opts.get("DoAveraging", True)
@@ -115,8 +116,9 @@ def uhf(atoms, **opts):
                 Da = averaging * Da + (1 - averaging) * Da0
                 Db = averaging * Db + (1 - averaging) * Db0
             Da0, Db0 = Da, Db
-        Ja, Jb = getJ(Ints, Da), getJ(Ints, Db)
-        Ka, Kb = getK(Ints, Da), getK(Ints, Db)
+        # getJ(Da), getJ(Db), getK(Da), getK(Db) of the reference, from one
+        # pass over the integrals
+        Ja, Jb, Ka, Kb = getJK2(Ints, Da, Db)
         Fa = h + Ja + Jb - Ka
         Fb = h + Ja + Jb - Kb
         orbea, orbsa = geigh(Fa, S)

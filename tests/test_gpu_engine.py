@@ -379,8 +379,10 @@ def test_rhf_reference_unit_test_energies():
 def test_uhf_reference_no_energy(monkeypatch):
     """NO / 6-31G** UHF at 2.12955 bohr, the reference's Tests/no_uhf.py
     (-129.247769 within 1e-4, uhf defaults).  The same uhf iterations on the
-    oracle's integrals (numpy J/K) must give the GPU energy to 1e-7, and each
-    iteration's getJ(Da), getJ(Db), getK(Da), getK(Db) runs two builds."""
+    oracle's integrals (numpy J/K) must give the GPU energy to 1e-7.  Each
+    iteration asks getJK2 for the reference's getJ(Da), getJ(Db), getK(Da),
+    getK(Db): two stored-integral builds at most; the integral-direct UHF
+    (one pass for both densities) lands on the same energy."""
     from pyquante_b200 import hartree_fock as HF
     from pyquante_b200.Molecule import Molecule
     no = Molecule("NO", atomlist=[(7, (0.0, 0.0, 0.0)), (8, (2.12955, 0.0, 0.0))], multiplicity=2)
@@ -392,22 +394,52 @@ def test_uhf_reference_no_energy(monkeypatch):
         return real(t, D)
 
     monkeypatch.setattr(Ints, "jk_packed", counted)
-    gets = []
-    for name in ("getJ", "getK"):
-        f = getattr(HF, name)
-        monkeypatch.setattr(HF, name, lambda I, D, f=f: (gets.append(1), f(I, D))[1])
+    calls = []
+    f = HF.getJK2
+    monkeypatch.setattr(HF, "getJK2", lambda I, Da, Db: (calls.append(1), f(I, Da, Db))[1])
     e_gpu, _, _ = HF.uhf(no)
     assert abs(e_gpu - (-129.247769)) < 1e-4
-    assert 0 < len(builds) <= len(gets) // 2
+    assert 0 < len(builds) <= 2 * len(calls)
+    monkeypatch.setattr(HF, "getJK2", f)
+    e_direct, _, _ = HF.uhf(no, direct=True, schwarz=0.0)
+    assert abs(e_direct - e_gpu) < 1e-8
     # the same driver on the oracle's integrals
     bs = BasisSet(no, "6-31g**")
     obfs = oracle_bfs(bs)
     S, h = O.orc_get1ints(obfs, atoms_of(no))
     ref = O.orc_get2ints(obfs)
-    monkeypatch.setattr(HF, "getJ", lambda I, D: O.getJK(I, D)[0])
-    monkeypatch.setattr(HF, "getK", lambda I, D: O.getJK(I, D)[1])
+
+    def oracle_jk2(I, Da, Db):
+        (Ja, Ka), (Jb, Kb) = O.getJK(I, Da), O.getJK(I, Db)
+        return Ja, Jb, Ka, Kb
+
+    monkeypatch.setattr(HF, "getJK2", oracle_jk2)
     e_orc, _, _ = HF.uhf(no, bfs=bs.bfs, integrals=(S, h, ref))
     assert abs(e_gpu - e_orc) < 1e-7
+
+
+def test_two_density_build_equals_two_single_builds():
+    """pqb_jk_direct2 digests every integral against both densities in one
+    pass: J and K of each equal a single-density build (FP64 and mixed, on
+    the launch-by-launch first call and on graph replays)."""
+    mol = geometries.water_cluster(3, seed=2)
+    bs = BasisSet(mol, "6-31g**")
+    eng = BasisEngine(bs.bfs)
+    n = len(bs)
+    Da = torch.as_tensor(_rand_density(n, 11), device="cuda")
+    Db = torch.as_tensor(_rand_density(n, 12) * 0.7, device="cuda")
+    for mode in ("fp64", "mixed"):
+        Ja, Ka = (x.clone() for x in eng.jk(Da, mode, 1e-12, 1e-5))
+        Jb, Kb = (x.clone() for x in eng.jk(Db, mode, 1e-12, 1e-5))
+        for _ in range(3):
+            J2a, K2a, J2b, K2b = eng.jk2(Da, Db, mode, 1e-12, 1e-5)
+            for got, want in ((J2a, Ja), (K2a, Ka), (J2b, Jb), (K2b, Kb)):
+                assert float((got - want).abs().max()) < 1e-12 * float(want.abs().max()), mode
+    # through the API: DirectInts getJK2 -> the one-pass build
+    d = Ints.get2ints(bs, direct=True)
+    Jda, Jdb, Kda, Kdb = Ints.getJK2(d, Da.cpu().numpy(), Db.cpu().numpy())
+    Jo, Ko = eng.jk(Db, "fp64", 1e-12, 1e-5)
+    assert np.abs(Jdb - Jo.cpu().numpy()).max() < ERI_TOL and np.abs(Kdb - Ko.cpu().numpy()).max() < ERI_TOL
 
 
 def test_single_function_and_zero_density_edge_cases():

@@ -148,6 +148,12 @@ def test_package_scf_drivers_on_oracle_integrals(monkeypatch):
     monkeypatch.setattr(HF, "getJ", lambda I, D: O.getJK(I, D)[0])
     monkeypatch.setattr(HF, "getK", lambda I, D: O.getJK(I, D)[1])
 
+    def oracle_jk2(I, Da, Db):
+        (Ja, Ka), (Jb, Kb) = O.getJK(I, Da), O.getJK(I, Db)
+        return Ja, Jb, Ka, Kb
+
+    monkeypatch.setattr(HF, "getJK2", oracle_jk2)
+
     def oracle_integrals(mol, basis):
         bs = BasisSet(mol, basis)
         bfs = [O.BF(bf.origin, bf.powers, list(zip(bf.pexps, bf.pcoefs))) for bf in bs.bfs]
