@@ -154,6 +154,26 @@ int pqb_jk_direct2(pqb_ctx *ctx, const double *Da, const double *Db, double *Ja,
 int pqb_jk_direct_class(pqb_ctx *ctx, const double *D, double *Jacc, double *Kacc, int part, int qclass, int mode,
                         void *stream);
 
+/* AO -> MO transformation for MP2 (replaces the Python loops of
+ * PyQuante/MP.py:20-75 TransformIntsMP2 and :77-97 MP2).  The quarter
+ * transformations are FP64 GEMMs the caller runs (cuBLAS); these move the
+ * data between them.  All pointers are device memory; no context.
+ * pqb_mo_unpack_rows: out[r][k][l] = (IJ|kl) for the packed bra rows
+ *   IJ = row0 .. row0+nrows-1 of the packed array ints (len = P(P+1)/2,
+ *   P = nbf(nbf+1)/2): out holds nrows * nbf * nbf doubles.
+ * pqb_mo_unpack_pairs: out[(mu*nbf + nu)*ncol + c] = Y[pair(mu,nu)*ncol + c]
+ *   (rows stored per packed AO pair, unpacked to both orders).
+ * pqb_mo_pack: moints[ijkl2intindex(a,i,b,j)] = Z[((a*nmo + i)*nocc + b)*nmo + j]
+ *   for a, b < nocc, i, j < nmo (len = Q(Q+1)/2, Q = nmo(nmo+1)/2: the
+ *   packed MO array TransformIntsMP2 returns; other slots are left as is).
+ * pqb_mp2_pairs: Epair[a*nocc + b] = sum_rs (ar|bs)(2(ar|bs) - (as|br)) /
+ *   (e_a + e_b - e_r - e_s) from V[((a*nvirt + r)*nocc + b)*nvirt + s]. */
+int pqb_mo_unpack_rows(const double *ints, int64_t len, int nbf, int64_t row0, int nrows, double *out, void *stream);
+int pqb_mo_unpack_pairs(const double *Y, int nbf, int64_t ncol, double *out, void *stream);
+int pqb_mo_pack(const double *Z, int nocc, int nmo, double *moints, int64_t len, void *stream);
+int pqb_mp2_pairs(const double *V, int nocc, int nvirt, const double *e_occ, const double *e_virt, double *Epair,
+                  void *stream);
+
 /* The same J and K from stored packed integrals (device). */
 int pqb_jk_packed(pqb_ctx *ctx, const double *ints, int64_t len, const double *D, double *J, double *K, int nbf,
                   void *stream);

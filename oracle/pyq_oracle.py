@@ -366,6 +366,67 @@ def rhf(atoms, S, h, ints, nclosed, conv=1e-10, maxiter=100, diis=False):
     return energy, orbe, orbs
 
 
+# -------------------------------------------------------------------- MP2 --
+def transform_ints_mp2_loops(ints, orbs, nclosed):
+    """PyQuante/MP.py:20-75 (TransformIntsMP2) step by step: sigma -> b,
+    mu -> a, eta -> j, nu -> i over the packed AO integrals, stored at
+    ijkl2intindex(a, i, b, j) of a packed MO array.  O(N^5) Python loops:
+    small bases only."""
+    nbf, nmo = orbs.shape
+    totlen = nmo * (nmo + 1) * (nmo * nmo + nmo + 2) // 8
+    occs, mos, bfs = range(nclosed), range(nmo), range(nbf)
+    temp = np.zeros((nbf, nbf, nclosed, nbf))
+    tempvec = np.zeros(nbf)
+    for mu in bfs:
+        for nu in bfs:
+            for eta in bfs:
+                for b in occs:
+                    for sigma in bfs:
+                        tempvec[sigma] = ints[ijkl2intindex(mu, nu, sigma, eta)]
+                    temp[mu, nu, b, eta] = orbs[:, b] @ tempvec
+    temp2 = np.zeros((nclosed, nbf, nclosed, nbf))
+    for nu in bfs:
+        for eta in bfs:
+            for b in occs:
+                for a in occs:
+                    temp2[a, nu, b, eta] = orbs[:, a] @ temp[:, nu, b, eta]
+    temp = np.zeros((nclosed, nbf, nclosed, nmo))
+    for a in occs:
+        for nu in bfs:
+            for b in occs:
+                for j in mos:
+                    temp[a, nu, b, j] = orbs[:, j] @ temp2[a, nu, b, :]
+    moints = np.zeros(totlen)
+    for a in occs:
+        for j in mos:
+            for b in occs:
+                for i in mos:
+                    moints[ijkl2intindex(a, i, b, j)] = orbs[:, i] @ temp[a, :, b, j]
+    return moints
+
+
+def transform_ovov(ints, orbs, nclosed, nmo=None):
+    """(a i|b j) = sum C_mu,a C_nu,i C_la,b C_si,j (mu nu|la si) as a dense
+    [nocc, nmo, nocc, nmo] array (numpy einsum over the unpacked integrals)."""
+    nbf = orbs.shape[0]
+    C = orbs if nmo is None else orbs[:, :nmo]
+    full = unpack(ints, nbf)
+    Co = orbs[:, :nclosed]
+    t = np.einsum("mnls,sj->mnlj", full, C)
+    t = np.einsum("mnlj,lb->mnbj", t, Co)
+    t = np.einsum("mnbj,ni->mibj", t, C)
+    return np.einsum("mibj,ma->aibj", t, Co)
+
+
+def mp2(ints, orbs, orbe, nclosed, nvirt):
+    """PyQuante/MP.py:77-97: sum over occupied a, b and virtual r, s of
+    (ar|bs)(2(ar|bs) - (as|br))/(e_a + e_b - e_r - e_s)."""
+    V = transform_ovov(ints, orbs, nclosed)[:, nclosed:nclosed + nvirt, :, nclosed:nclosed + nvirt]
+    eo, ev = orbe[:nclosed], orbe[nclosed:nclosed + nvirt]
+    den = eo[:, None, None, None] + eo[None, None, :, None] - ev[None, :, None, None] - ev[None, None, None, :]
+    return float((V * (2 * V - V.transpose(0, 3, 2, 1)) / den).sum())
+
+
 # --------------------------------------------------------------- gradient --
 def _deriv_parts(bf, x):
     """d phi / dA_x of a contracted function on centre A as up to two

@@ -56,6 +56,10 @@ SIGNATURES = {
     "pqb_grad_2e": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
     "pqb_grad_1e": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _c_dbl_p,
                                    _c_dbl_p, _vp, _vp, _vp, _vp]),
+    "pqb_mo_unpack_rows": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int, ctypes.c_int64, ctypes.c_int, _vp, _vp]),
+    "pqb_mo_unpack_pairs": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int64, _vp, _vp]),
+    "pqb_mo_pack": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int64, _vp]),
+    "pqb_mp2_pairs": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),
     "pqb_ijkl2intindex": (ctypes.c_int64, [ctypes.c_int64] * 4),
     "pqb_boys_eval": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "pqb_rys_eval": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),

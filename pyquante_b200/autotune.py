@@ -2,7 +2,7 @@
 primitive-quartet chunk of a work item (2 .. 128), and the number of
 streams the class launches share.
 
-    python -m pyquante_b200.autotune            # tunes (H2O)8 / 6-31G** on cuda:0
+    python -m pyquante_b200.autotune [--mode fp64|mixed] [--out PATH]   # (H2O)8 / 6-31G** on cuda:0
 
 The objective is the whole Fock-build time (CUDA events, median of 5,
 after an L2 flush): the class kernels run concurrently on several streams,
@@ -126,6 +126,8 @@ def tune(eng, D, mode="mixed", schwarz=1e-12, fp32_threshold=1e-5, verbose=True)
 
 
 def main():
+    import argparse
+
     import torch
     from . import Ints, geometries
     from .Basis.basis import BasisSet
@@ -138,10 +140,14 @@ def main():
     S, h = Ints.get1ints(bs, mol)
     _, C = geigh(torch.as_tensor(h, device="cuda"), torch.as_tensor(S, device="cuda"))
     D = mkdens(C, 0, mol.get_nel() // 2).contiguous()
-    res = tune(eng, D)
-    with open(TUNED, "w") as f:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"], help="build to tune (default: FP64)")
+    ap.add_argument("--out", default=TUNED, help="where to write the result (default: tuned.json here)")
+    a = ap.parse_args()
+    res = tune(eng, D, mode=a.mode)
+    with open(a.out, "w") as f:
         json.dump(res, f, indent=1)
-    print("wrote", TUNED)
+    print("wrote", a.out)
 
 
 if __name__ == "__main__":

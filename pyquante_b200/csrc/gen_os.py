@@ -269,6 +269,39 @@ def emit_class(LA, LB, LC, LD):
     return L, vrr_ops(t), len(steps)
 
 
+def emitted_flops(lines):
+    """(vrr, hrr) FP64 flops of the emitted bodies (FMA = 2, MUL/ADD = 1;
+    a constant multiple k * coefficient, once per primitive quartet,
+    counts 1)."""
+    out = {"vrr": 0, "hrr": 0}
+    fn = None
+    for ln in lines:
+        s = ln.strip()
+        if "void vrr(" in s:
+            fn = "vrr"
+            continue
+        if "void hrr(" in s:
+            fn = "hrr"
+            continue
+        if fn is None or s.startswith(("template", "static", "//", "(void)")) or "=" not in s:
+            continue
+        rhs = s.split("=", 1)[1]
+        n = 2 * rhs.count("fma(") + rhs.count(" * ") + (1 if "+=" in s else 0)
+        out[fn] += n
+    return out["vrr"], out["hrr"]
+
+
+_FLOPS = {}
+
+
+def class_flops(LA, LB, LC, LD):
+    """Cached (vrr flops per primitive quartet, hrr flops per item)."""
+    key = (LA, LB, LC, LD)
+    if key not in _FLOPS:
+        _FLOPS[key] = emitted_flops(emit_class(*key)[0])
+    return _FLOPS[key]
+
+
 def as_python(lines):
     """The emitted vrr/hrr bodies as Python functions (a host-side check of
     the generated code itself: the same expressions, FMA as a*b + c)."""
@@ -316,7 +349,10 @@ def main():
 
 def count():
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
-    from pyquante_b200.flops import prim_quartet_flops
+    from pyquante_b200 import flops
+    _saved = flops._OS
+    flops._OS = set()          # the Rys model of every class, for comparison
+    prim_quartet_flops = flops.prim_quartet_flops
     pairs = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
     for cb in range(6):
         for ck in range(cb + 1):
@@ -325,6 +361,7 @@ def count():
             steps, _ = hrr_plan(*cls)
             print("(%d%d|%d%d) LT=%d  OS vrr %5d ops (+%d Boys orders) hrr %4d/item   rys model %6d flops" %
                   (cls + (sum(cls), vrr_ops(t), sum(cls) + 1, len(steps), prim_quartet_flops(*cls))))
+    flops._OS = _saved
 
 
 if __name__ == "__main__":

@@ -1,8 +1,18 @@
-"""Algorithmic FP operation counts of the ERI kernels (FMA = 2 flops), per
-primitive quartet of each class, counted from the loop structure of
-csrc/pqb_device.cuh (rys_root, rys2d) and csrc/eri_engine.cuh (assembly).
-Used for the roofline of the direct J/K and packed-integral kernels.
+"""Algorithmic FP64 operation counts of the ERI kernels (FMA = 2 flops), per
+primitive quartet and per work item of each class, counted from the code the
+kernels run.  Used for the roofline of the direct J/K and packed-integral
+kernels; cross-checked against ncu's executed dfma/dadd/dmul counts.
 
+Obara--Saika classes (LA+LB+LC+LD = LT <= 4, csrc/os_classes.inc):
+  setup     PQ, zeta+eta, 1/sqrt (Newton step), 1/(zeta+eta), T, prefactor: 24
+  Boys      LT <= 1: grid index and offset 3, Horner 14 (+12 for F_1);
+            LT 2, 3: 3 + F_3 Horner 12 + exp series 12 + 2 + recursion 3 x 3 = 38;
+            LT 4:    the same with four recursion steps = 41
+  prefactor (LT+1) products
+  geometry  PA, QC, rz, re, WP, WQ, 1/(2 zeta), 1/(2 eta), 1/(2(zeta+eta)): 17
+  VRR       the emitted vertical recurrence (gen_os.class_flops)
+  per item  the emitted horizontal transfer, plus the J/K digestion
+Rys classes (the block-mode classes, 3+ roots):
   roots     NR roots x 2 series (root, weight) x Clenshaw(14 coef): 13 x (FMA+sub)
             + final (FMA+sub)                                     = 84 / root
   setup     T, prefactor: 20
@@ -11,11 +21,14 @@ Used for the roofline of the direct J/K and packed-integral kernels.
             + ket HRR:   (NB+1) x sum_{d=1..LD} (MK-d+1) x 2
             + bra HRR:   (LC+1)(LD+1) x sum_{b=1..LB} (NB-b+1) x 2
   assembly  NAB x NCD x NR x 3   (one MUL + one FMA per component per root)
-where NB = LA+LB, MK = LC+LD, NR = (LA+LB+LC+LD)/2 + 1.
-Per shell quartet, the J/K digestion adds NAB x NCD x 16 (scales, six
-D products).
+  where NB = LA+LB, MK = LC+LD, NR = (LA+LB+LC+LD)/2 + 1.
+Per work item, the J/K digestion adds NAB x NCD x 16 (weights, six D
+products).
 """
+from .csrc import gen_os
+
 PAIR_CLASSES = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
+_OS = set(gen_os.OS_CLASSES)
 
 
 def ncart(L):
@@ -31,6 +44,10 @@ def quartet_class_ls(qc):
     return PAIR_CLASSES[cb] + PAIR_CLASSES[ck]
 
 
+def uses_os(LA, LB, LC, LD):
+    return (LA, LB, LC, LD) in _OS
+
+
 def rys2d_flops(LA, LB, LC, LD):
     NB, MK = LA + LB, LC + LD
     f = 12
@@ -40,8 +57,20 @@ def rys2d_flops(LA, LB, LC, LD):
     return f
 
 
+def _os_boys_flops(LT):
+    if LT == 0:
+        return 3 + 14
+    if LT == 1:
+        return 3 + 14 + 12
+    return 38 if LT <= 3 else 41
+
+
 def prim_quartet_flops(LA, LB, LC, LD):
-    NR = (LA + LB + LC + LD) // 2 + 1
+    """FP64 flops per primitive quartet of class (LA LB|LC LD)."""
+    LT = LA + LB + LC + LD
+    if uses_os(LA, LB, LC, LD):
+        return 24 + _os_boys_flops(LT) + (LT + 1) + 17 + gen_os.class_flops(LA, LB, LC, LD)[0]
+    NR = LT // 2 + 1
     nab, ncd = ncart(LA) * ncart(LB), ncart(LC) * ncart(LD)
     return 20 + NR * 84 + NR * 3 * rys2d_flops(LA, LB, LC, LD) + nab * ncd * NR * 3
 
@@ -50,6 +79,13 @@ def digest_flops(LA, LB, LC, LD):
     return ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD) * 16
 
 
+def item_flops(LA, LB, LC, LD):
+    """FP64 flops per work item: the horizontal transfer (Obara--Saika
+    classes) and the J/K digestion."""
+    hrr = gen_os.class_flops(LA, LB, LC, LD)[1] if uses_os(LA, LB, LC, LD) else 0
+    return hrr + digest_flops(LA, LB, LC, LD)
+
+
 def class_flops(qc, prim_quartets, quartets):
     ls = quartet_class_ls(qc)
-    return prim_quartets * prim_quartet_flops(*ls) + quartets * digest_flops(*ls)
+    return prim_quartets * prim_quartet_flops(*ls) + quartets * item_flops(*ls)

@@ -4,7 +4,7 @@
     stored-integral J/K of the packed array (itself sample-pinned to the
     reference's compiled crys at this N), the direct FP64 RHF energy against
     the packed-integral RHF energy, and the mixed-precision energy error;
-  * C16H34 / 6-31G* (N = 308, Q = 1,132,237,791, a 9.06 GB packed array): a
+  * C16H34 / 6-31G* (N = 308, Q = 1,132,237,491, a 9.06 GB packed array): a
     sample of packed integrals in the range where the reference's 32-bit
     ijkl2intindex overflows (Src/cints.c:413-425), against the reference's
     compiled crys (tests/golden/eri_631s_c16h34_sample.npz), and the FP32
@@ -110,7 +110,7 @@ def test_c16h34_packed_sample_vs_reference_engine(c16h34):
     P = 308 * 309 // 2
     assert int(idx.max()) >= 46341 * 46342 // 2 and idx.max() < P * (P + 1) // 2
     t = eng.eri_packed()
-    assert t.numel() == 1132237791
+    assert t.numel() == P * (P + 1) // 2 == 1132237491
     got = t[torch.from_numpy(idx).cuda()].cpu().numpy()
     err = float(np.abs(got - s["value"]).max())
     print("C16H34 packed sample (%d quartets, %d in the overflow range): max |err| %.3e" %

@@ -171,3 +171,55 @@ def test_package_scf_drivers_on_oracle_integrals(monkeypatch):
     bfs, ints = oracle_integrals(no, "6-31g**")
     E, _, _ = HF.uhf(no, bfs=bfs, integrals=ints)
     assert abs(E - (-129.247769)) < 1e-4
+
+
+def _mp2_case(atoms, basis, nclosed):
+    bfs = O.build_basis(atoms, basis)
+    S, h = O.orc_get1ints(bfs, atoms)
+    ints = O.ref_get2ints(bfs, nproc=4) if O.ref_available() else O.orc_get2ints(bfs)
+    e, orbe, orbs = O.rhf(atoms, S, h, ints, nclosed, conv=1e-12, maxiter=200, diis=True)
+    return e, O.mp2(ints, orbs, orbe, nclosed, len(bfs) - nclosed)
+
+
+def test_mp2_restatement_reproduces_the_reference_answers():
+    """The restated MP2 (PyQuante/MP.py:77-97 on the 6-31G** integrals) at the
+    geometries of the reference's own MP2 tests: Tests/h2_mp2.py:15 (1e-6;
+    the GAMESS-UK value of :12 to 1e-7), Tests/he_mp2.py:12 (1e-4),
+    Tests/lih_mp2.py:15, and Tests/ch4_mp2.py:12-13 (GAMESS-UK total and
+    correction)."""
+    from pyquante_b200.Basis.p631ss import basis_data as P631SS
+    a2b = 1 / 0.529177249
+    e, emp2 = _mp2_case([(1, (1.0, 0.0, 0.0)), (1, (-1.0, 0.0, 0.0))], P631SS, 1)
+    assert abs(e + emp2 - (-1.11591861694)) < 1e-6
+    assert abs(e + emp2 - (-1.11591790)) < 1e-7
+    e, emp2 = _mp2_case([(2, (0.0, 0.0, 0.0))], P631SS, 1)
+    assert abs(e + emp2 - (-2.880637)) < 1e-4
+    e, emp2 = _mp2_case([(3, (0.0, 0.0, 0.0)), (1, (0.0, 0.0, 1.629912 * a2b))], P631SS, 2)
+    assert abs(e + emp2 - (-8.0021911)) < 1e-6
+    ch4 = [(6, (0, 0, 0)), (1, (0, 0, 1.0836058890)), (1, (1.0216334297, 0, -.3612019630)),
+           (1, (-.5108167148, .8847605034, -.3612019630)), (1, (-.5108167148, -.8847605034, -.3612019630))]
+    e, emp2 = _mp2_case([(z, tuple(c * a2b for c in r)) for z, r in ch4], P631SS, 5)
+    assert abs(e + emp2 - (-40.36985496)) < 1e-7
+    assert abs(emp2 - (-0.16815019)) < 1e-7
+
+
+def test_mp2_dense_transform_matches_the_reference_loops():
+    """The einsum transform used as the MP2 oracle equals the step-by-step
+    restatement of TransformIntsMP2 (PyQuante/MP.py:20-75), packing included,
+    on water / STO-3G."""
+    from pyquante_b200 import geometries
+    from pyquante_b200.Basis.sto3g import basis_data as STO3G
+    atoms = atoms_of(geometries.water())
+    bfs = O.build_basis(atoms, STO3G)
+    S, h = O.orc_get1ints(bfs, atoms)
+    ints = O.orc_get2ints(bfs)
+    _, orbe, orbs = O.rhf(atoms, S, h, ints, 5, conv=1e-12)
+    loops = O.transform_ints_mp2_loops(ints, orbs, 5)
+    Z = O.transform_ovov(ints, orbs, 5)
+    dense = np.zeros_like(loops)
+    for a in range(5):
+        for i in range(7):
+            for b in range(5):
+                for j in range(7):
+                    dense[O.ijkl2intindex(a, i, b, j)] = Z[a, i, b, j]
+    assert np.abs(loops - dense).max() < 1e-13
