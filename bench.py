@@ -1,7 +1,7 @@
 """Benchmark: integral-direct 2J-K Fock build on (H2O)8 / 6-31G** (N = 200).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pqb|reference]
-                    [--no-cpu-baseline] [--workload h2o8|stored|c16h34|h2o4-grad|batch]
+                    [--no-cpu-baseline] [--workload h2o8|stored|c16h34|h2o4-grad|batch|mp2]
 
 One step = one full FP64 2J-K Fock build G(D) = 2J(D) - K(D) for a fixed SCF
 density D of the seeded (H2O)8 cluster (Schwarz 1e-12).  value = nominal
@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--soak", type=int, default=3000, help="untimed builds run under the clock sampler before the "
                                                            "timed ones")
-    p.add_argument("--workload", default="h2o8", choices=["h2o8", "stored", "c16h34", "h2o4-grad", "batch"],
+    p.add_argument("--workload", default="h2o8", choices=["h2o8", "stored", "c16h34", "h2o4-grad", "batch", "mp2"],
                    help="h2o8: the headline Fock build; the others are the secondary workloads "
                         "(C16H34 threshold sweep, (H2O)4 gradient, batched SCF)")
     p.add_argument("--batch-count", type=int, default=512)
@@ -468,6 +468,46 @@ def _scf(mol, bs, precision):
     return e, Counting.builds, time.perf_counter() - t0
 
 
+def run_mp2(a):
+    """MP2 on (H2O)8 / 6-31G** (N = 200, 40 occupied orbitals): the AO -> MO
+    transformation of the packed integrals (PyQuante/MP.py:20-97) timed on
+    the device after the RHF, FP64 throughout."""
+    import torch
+
+    from pyquante_b200 import MP, Ints
+    from pyquante_b200.Basis.basis import BasisSet
+    from pyquante_b200.hartree_fock import rhf
+    mol = molecule()
+    bs = BasisSet(mol, "6-31g**")
+    n = len(bs)
+    nocc = mol.get_nel() // 2
+    S, h, ints = Ints.getints(bs, mol)
+    e, orbe, orbs = rhf(mol, bfs=bs, integrals=(S, h, ints), ConvCriteria=1e-10, MaxIter=80, DoAveraging=True)
+    for _ in range(max(a.warmup, 1)):
+        emp2 = MP.MP2(ints, orbs, orbe, nocc, n - nocc)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(a.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        emp2 = MP.MP2(ints, orbs, orbe, nocc, n - nocc)
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = float(np.median(ts))
+    nv = n - nocc
+    P = n * (n + 1) // 2
+    # GEMM flops of the two half-transformations (FMA = 2)
+    fl = 2.0 * P * (n * n * nv + n * nocc * nv) + 2.0 * nocc * nv * (n * n * nocc + n * nocc * nv)
+    print(json.dumps({"metric": "MP2 energy (AO->MO transform of packed Ints + pair energies)",
+                      "value": ms, "unit": "ms", "higher_is_better": False, "steps": a.steps, "data": "synthetic",
+                      "dtype": "f64",
+                      "config": {"workload": WORKLOAD, "nocc": nocc, "nvirt": nv, "e_rhf": e, "e_mp2": emp2,
+                                 "gemm_flops": fl, "gemm_tflops": fl / (ms * 1e-3) / 1e12,
+                                 "path": "pqb_mo_unpack_rows/pairs + cuBLAS DGEMM (torch.matmul) + pqb_mp2_pairs"}}))
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -477,7 +517,7 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         {"stored": run_stored, "c16h34": run_c16h34, "h2o4-grad": run_h2o4_grad,
-         "batch": run_batch}[a.workload](a)
+         "batch": run_batch, "mp2": run_mp2}[a.workload](a)
         return
     import ctypes
 

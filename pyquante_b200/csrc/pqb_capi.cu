@@ -1538,10 +1538,11 @@ int pqb_plan(pqb_ctx *ctx, double schwarz_thresh, double fp32_thresh, int64_t *c
             ctx->plan_prims[part][c] = pr;
             nitems[part] += n;
         }
-    // the FP64 part, then the FP32 part; classes in order within each
+    // class-major: the FP64 part of each class directly followed by its
+    // FP32-eligible part, so an FP64 build launches one list per class
     int64_t o = 0;
-    for (int part = 0; part < 2; ++part)
-        for (int c = 0; c < kNumQuartetClass; ++c) {
+    for (int c = 0; c < kNumQuartetClass; ++c)
+        for (int part = 0; part < 2; ++part) {
             ctx->plan_off[part][c] = o;
             o += ctx->plan_cnt[part][c];
         }
@@ -1649,8 +1650,8 @@ static int plan_shard_impl(pqb_ctx *ctx, int rank, int nranks)
     std::vector<int4> out;
     out.reserve(total / nranks + 64);
     int64_t off[2][kNumQuartetClass], cnt[2][kNumQuartetClass], prims[2][kNumQuartetClass];
-    for (int part = 0; part < 2; ++part)
-        for (int c = 0; c < kNumQuartetClass; ++c) {
+    for (int c = 0; c < kNumQuartetClass; ++c)      // the class-major layout of pqb_plan
+        for (int part = 0; part < 2; ++part) {
             off[part][c] = (int64_t)out.size();
             prims[part][c] = 0;
             for (int64_t q = rank; q < ctx->plan_cnt[part][c]; q += nranks) {
@@ -1793,9 +1794,13 @@ static int launch_build(pqb_ctx *ctx, int nden, double *const Jacc[2], double *c
                                   : (double)ctx->plan_prims[part][c] * (1 + c) * (part == 1 && mode == PQB_MIXED ? 0.5 : 1.0);
     }
     std::sort(order, order + 2 * kNumQuartetClass, [&](int x, int y) { return cost[x] > cost[y]; });
+    // in an FP64 build both parts of a class are one list (the plan is
+    // class-major): one launch per class, over more items
+    const bool merged = mode != PQB_MIXED;
     for (int i = 0, k = 0; i < 2 * kNumQuartetClass; ++i) {
         const int part = order[i] / kNumQuartetClass, c = order[i] % kNumQuartetClass;
-        const int nq = (int)ctx->plan_cnt[part][c];
+        if (merged && part == 1) continue;
+        const int nq = (int)(ctx->plan_cnt[part][c] + (merged ? ctx->plan_cnt[1][c] : 0));
         if (nq == 0) continue;
         cudaStream_t sk = ctx->streams[k++ % ctx->nstreams];
         const int4 *list = ctx->d_plan + ctx->plan_off[part][c];
