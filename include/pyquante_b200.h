@@ -174,6 +174,30 @@ int pqb_mo_pack(const double *Z, int nocc, int nmo, double *moints, int64_t len,
 int pqb_mp2_pairs(const double *V, int nocc, int nvirt, const double *e_occ, const double *e_virt, double *Epair,
                   void *stream);
 
+/* DFT numerical integration (replaces the Python loops of the reference's
+ * MG2 grid and SVWN functional: PyQuante/MG2.py:50-250,
+ * PyQuante/MolecularGrid.py:228-263, PyQuante/DFunctionals.py:76-138,
+ * 319-389, 603-623, and the Fxc assembly of PyQuante/dft.py:29-65).  All
+ * pointers are device memory; no context.
+ * pqb_becke_weights: w[g] = pts[4g+3] * P_owner / sum_j P_j for the points
+ *   pts[npts][4] (x, y, z, atomic-grid weight), owner[g] its atom,
+ *   atom_xyz[3*natoms], adjust[natoms*natoms] the heteronuclear size
+ *   adjustment a_jk (mu' = mu + a_jk (1 - mu^2)).
+ * pqb_grid_amps: B[g*n + i] = amplitude of basis function i (the function
+ *   table of pqb_oneint) at point g of pts[npts][4].
+ * pqb_grid_rowdot: out[g] = sum_i A[g*n + i] B[g*n + i] (the density from
+ *   B D and B).
+ * pqb_xc_svwn: per point, Slater exchange plus VWN correlation of the spin
+ *   densities rhoa, rhob, times the weight w: wf = w f_xc, wva = w v_a,
+ *   wvb = w v_b. */
+int pqb_becke_weights(int npts, const double *pts, const int *owner, int natoms, const double *atom_xyz,
+                      const double *adjust, double *w, void *stream);
+int pqb_grid_amps(int n, const double *origin, const int *powers, const int *prim_off, const double *exps,
+                  const double *cn, const double *norms, int npts, const double *pts, double *B, void *stream);
+int pqb_grid_rowdot(int npts, int n, const double *A, const double *B, double *out, void *stream);
+int pqb_xc_svwn(int npts, const double *rhoa, const double *rhob, const double *w, double *wf, double *wva,
+                double *wvb, void *stream);
+
 /* The same J and K from stored packed integrals (device). */
 int pqb_jk_packed(pqb_ctx *ctx, const double *ints, int64_t len, const double *D, double *J, double *K, int nbf,
                   void *stream);

@@ -514,3 +514,170 @@ def rhf_gradient(atoms, basis_data, D, Q):
                     g += za * zb * d[x] / np.linalg.norm(d) ** 3
             grad[a, x] = g
     return grad
+
+
+# -------------------------------------------------------------------- DFT --
+# The default grid and SVWN functional of the reference's dft()
+# (PyQuante/dft.py:116-215 with MG2 grids, PyQuante/MG2.py:50-250):
+# per atom, 32 Euler--Maclaurin radial shells (PyQuante/AtomicGrid.py:284-294,
+# SG-1 radii) times the 194-point Lebedev rule, Becke partitioning with the
+# heteronuclear size adjustment (PyQuante/MolecularGrid.py:228-263), basis
+# amplitudes, density, SVWN (PyQuante/DFunctionals.py:76-138,319-389,603-623),
+# Fxc = sum_g w v phi_i phi_j (PyQuante/dft.py:29-65).
+def dft_grid(atoms, nrad=32):
+    """(npts, 4) x, y, z, w of the reference's default molecular grid;
+    atoms: [(Z, (x, y, z))] in bohr."""
+    from pyquante_b200 import Lebedev
+    from pyquante_b200.MolecularGrid import BRAGG, POPLE_RADII
+    ang = Lebedev.points()
+    pts = []
+    owner = []
+    for ia, (z, xyz) in enumerate(atoms):
+        R = POPLE_RADII[z]
+        for i in range(1, nrad + 1):
+            w = 8.0 * np.pi * R ** 3 * (nrad + 1.0) * i ** 5 * (nrad + 1 - i) ** -7.0
+            r = R * i * i * (nrad + 1 - i) ** -2.0
+            for x, y, zz, wa in ang:
+                pts.append((r * x + xyz[0], r * y + xyz[1], r * zz + xyz[2], w * wa))
+                owner.append(ia)
+    pts = np.array(pts)
+    nat = len(atoms)
+    pos = np.array([xyz for _, xyz in atoms], dtype=float)
+
+    def cell(i, p):
+        s = 1.0
+        rip = np.linalg.norm(pos[i] - p)
+        for j in range(nat):
+            if j == i:
+                continue
+            rjp = np.linalg.norm(pos[j] - p)
+            rij = np.linalg.norm(pos[i] - pos[j])
+            mu = (rip - rjp) / rij
+            if atoms[i][0] != atoms[j][0]:
+                chi = BRAGG[atoms[i][0]] / BRAGG[atoms[j][0]]
+                u = (chi - 1.0) / (chi + 1.0)
+                a = min(max(u / (u * u - 1), -0.5), 0.5)
+                mu += a * (1 - mu * mu)
+            for _ in range(3):
+                mu = 1.5 * mu - 0.5 * mu ** 3
+            s *= 0.5 * (1 - mu)
+        return s
+
+    for g in range(len(pts)):
+        p = pts[g, :3]
+        cells = [cell(j, p) for j in range(nat)]
+        pts[g, 3] *= cells[owner[g]] / sum(cells)
+    return pts
+
+
+def bf_amps(bfs, pts):
+    """(npts, nbf) amplitudes: norm * sum_p c_p N_p x^l y^m z^n exp(-a r^2)."""
+    B = np.zeros((len(pts), len(bfs)))
+    for k, bf in enumerate(bfs):
+        d = pts[:, :3] - np.array(bf.origin)
+        r2 = (d * d).sum(1)
+        poly = d[:, 0] ** bf.powers[0] * d[:, 1] ** bf.powers[1] * d[:, 2] ** bf.powers[2]
+        B[:, k] = bf.norm * poly * sum(c * n * np.exp(-a * r2) for a, c, n in zip(bf.pexps, bf.pcoefs, bf.pnorms))
+    return B
+
+
+def svwn(rhoa, rhob, tol=1e-10):
+    """(fxc, vxc_a, vxc_b) per point: Slater exchange with X-alpha 2/3 per
+    spin plus VWN correlation (the reference's xs and cvwn)."""
+    fac = -2.25 * (2.0 / 3.0) * (3.0 / 4.0 / np.pi) ** (1.0 / 3.0)
+    n = len(rhoa)
+    f = np.zeros(n)
+    va = np.zeros(n)
+    vb = np.zeros(n)
+
+    def xx(x, b, c):
+        return x * x + b * x + c
+
+    def eps(x, a, x0, b, c):
+        q = np.sqrt(4 * c - b * b)
+        return a * (np.log(x * x / xx(x, b, c)) - b * (x0 / xx(x0, b, c)) * np.log((x - x0) ** 2 / xx(x, b, c))
+                    + (2 * b / q) * (1 - (x0 * (2 * x0 + b) / xx(x0, b, c))) * np.arctan(q / (2 * x + b)))
+
+    def deps(x, a, x0, b, c):
+        q = np.sqrt(4 * c - b * b)
+        return a * (2 / x - (2 * x + b) / xx(x, b, c) - 4 * b / ((2 * x + b) ** 2 + q * q) - (b * x0 / xx(x0, b, c))
+                    * (2 / (x - x0) - (2 * x + b) / xx(x, b, c) - 4 * (2 * x0 + b) / ((2 * x + b) ** 2 + q * q)))
+
+    P = (0.0310907, -0.10498, 3.72744, 12.9352)
+    Fm = (0.01554535, -0.32500, 7.06042, 13.0045)
+    for g in range(n):
+        for rho, vv in ((rhoa[g], va), (rhob[g], vb)):
+            r = 0.0 if rho < tol else rho
+            r3 = r ** (1.0 / 3.0)
+            f[g] += fac * r * r3
+            vv[g] += (4.0 / 3.0) * fac * r3
+        rho = rhoa[g] + rhob[g]
+        if rho < tol:
+            continue
+        zeta = (rhoa[g] - rhob[g]) / rho
+        x = (3.0 / 4.0 / np.pi / rho) ** (1.0 / 6.0)
+        ep, dep = eps(x, *P), deps(x, *P)
+        gz = 1.125 * ((1 + zeta) ** (4.0 / 3.0) + (1 - zeta) ** (4.0 / 3.0) - 2)
+        if gz < tol:
+            f[g] += ep * rho
+            va[g] += ep - (x / 6.0) * dep
+            vb[g] += ep - (x / 6.0) * dep
+            continue
+        ef, def_ = eps(x, *Fm), deps(x, *Fm)
+        e = ep + gz * (ef - ep)
+        f[g] += e * rho
+        dg = 1.5 * ((1 + zeta) ** (1.0 / 3.0) - (1 - zeta) ** (1.0 / 3.0))
+        dx = dep + gz * (def_ - dep)
+        dgg = (ef - ep) * dg
+        va[g] += e - (x / 6.0) * dx + dgg * (1 - zeta)
+        vb[g] += e - (x / 6.0) * dx - dgg * (1 + zeta)
+    return f, va, vb
+
+
+def get_xc(B, w, D, nel):
+    """(Exc, Fxc) of PyQuante/dft.py:29-65 for a closed-shell (spin-averaged)
+    density D = C_occ C_occ^T: rho_a = rho_b = sum_ij B_i D_ij B_j, floored at
+    1e-9, renormalised to nel electrons."""
+    rho = ((B @ D) * B).sum(1)
+    rho[rho < 1e-9] = 0.0
+    rho *= nel / (w @ (2 * rho))
+    f, va, _ = svwn(rho, rho)
+    return float(w @ f), B.T @ (B * (w * va)[:, None])
+
+
+def dft(atoms, S, h, ints, bfs, nclosed, conv=1e-10, maxiter=100):
+    """PyQuante/dft.py:116-215 (closed shell, SVWN): F = h + 2J + Fxc,
+    E = 2 tr(D h) + 2 tr(D J) + Exc + E_nuc, with the DIIS of rhf()."""
+    pts = dft_grid(atoms)
+    B = bf_amps(bfs, pts)
+    w = pts[:, 3]
+    nel = 2 * nclosed
+    en = enuke(atoms)
+    orbe, orbs = geigh(h, S)
+    eold = 0.0
+    Fs, Es = [], []
+    energy = 0.0
+    for _ in range(maxiter):
+        D = orbs[:, :nclosed] @ orbs[:, :nclosed].T
+        J, _ = getJK(ints, D)
+        exc, fxc = get_xc(B, w, D, nel)
+        F = h + 2 * J + fxc
+        err = (F @ D @ S - S @ D @ F).ravel()
+        if abs(err).max() >= 1e-13:
+            Fs.append(F)
+            Es.append(err)
+            del Fs[:-8], Es[:-8]
+            m = len(Es)
+            a = np.zeros((m + 1, m + 1))
+            a[:m, :m] = np.array(Es) @ np.array(Es).T
+            a[m, :m] = a[:m, m] = -1.0
+            b = np.zeros(m + 1)
+            b[m] = -1.0
+            c = np.linalg.solve(a, b)
+            F = sum(c[i] * Fs[i] for i in range(m))
+        orbe, orbs = geigh(F, S)
+        energy = float(2 * (D * h).sum() + 2 * (D * J).sum() + exc + en)
+        if abs(energy - eold) < conv:
+            break
+        eold = energy
+    return energy, orbe, orbs

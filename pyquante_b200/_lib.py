@@ -60,6 +60,10 @@ SIGNATURES = {
     "pqb_mo_unpack_pairs": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int64, _vp, _vp]),
     "pqb_mo_pack": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int64, _vp]),
     "pqb_mp2_pairs": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "pqb_becke_weights": (ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "pqb_grid_amps": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp]),
+    "pqb_grid_rowdot": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "pqb_xc_svwn": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "pqb_ijkl2intindex": (ctypes.c_int64, [ctypes.c_int64] * 4),
     "pqb_boys_eval": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "pqb_rys_eval": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),

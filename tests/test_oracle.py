@@ -223,3 +223,32 @@ def test_mp2_dense_transform_matches_the_reference_loops():
                 for j in range(7):
                     dense[O.ijkl2intindex(a, i, b, j)] = Z[a, i, b, j]
     assert np.abs(loops - dense).max() < 1e-13
+
+
+def test_lebedev_rule_is_exact_and_matches_the_published_values():
+    """The refined 194-point rule integrates every even monomial of degree
+    <= 22 exactly (its odd ones vanish by symmetry) and stays within the
+    rounding of the published 12-digit values."""
+    from pyquante_b200 import Lebedev as L
+    P = L.points()
+    for i, j, k in L.monomials():
+        got = float((P[:, 3] * P[:, 0] ** (2 * i) * P[:, 1] ** (2 * j) * P[:, 2] ** (2 * k)).sum())
+        assert abs(got - L.exact_average(i, j, k)) < 1e-15
+    Q = L.points(L.PUBLISHED)
+    assert np.abs(np.sort(P, axis=0) - np.sort(Q, axis=0)).max() < 5e-12
+
+
+def test_dft_restatement_reproduces_the_reference_answers():
+    """The restated SVWN DFT on the reference's default grid
+    (PyQuante/dft.py:116-215): He / 6-31G** at Tests/he_dft.py:12 (1e-6) and
+    H2 at 0.70 A at Tests/h2_dft.py:10 (1e-4)."""
+    from pyquante_b200.Basis.p631ss import basis_data as P631SS
+
+    def run(atoms, nclosed):
+        bfs = O.build_basis(atoms, P631SS)
+        S, h = O.orc_get1ints(bfs, atoms)
+        return O.dft(atoms, S, h, O.orc_get2ints(bfs), bfs, nclosed)[0]
+
+    assert abs(run([(2, (0.0, 0.0, 0.0))], 1) - (-2.8266976)) < 1e-6
+    r = 0.70 / 0.529177249
+    assert abs(run([(1, (0.0, 0.0, r / 2)), (1, (0.0, 0.0, -r / 2))], 1) - (-1.132710)) < 1e-4
