@@ -132,7 +132,9 @@ int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream);
 
 /* Integral-direct J_ij = sum_kl (ij|kl) D_kl and K_ij = sum_kl (ik|jl) D_kl
  * for a symmetric density D (device, nbf x nbf, row-major); J and K are
- * overwritten.  mode = PQB_FP64 or PQB_MIXED.  The context's scratch (scaled
+ * overwritten.  K may be NULL: then only the Coulomb digestion runs and J
+ * alone is written (the getJ of PyQuante/dft.py:209 and :312).
+ * mode = PQB_FP64 or PQB_MIXED.  The context's scratch (scaled
  * density, graph accumulators) is shared by its calls: calls on one context
  * must not overlap on different streams (see PQB_PARAM_GRAPH). */
 int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode, void *stream);

@@ -127,6 +127,9 @@ class DirectInts:
     def jk(self, D):
         return self.engine.jk(D, self.precision, self.schwarz, self.fp32_threshold)
 
+    def j(self, D):
+        return self.engine.j(D, self.precision, self.schwarz, self.fp32_threshold)
+
 
 def _general_packed(bfs, eng):
     """Packed integrals for function lists that do not form s/p/d shells:
@@ -184,7 +187,7 @@ def _back(x, orig):
 _JK_CACHE = 2   # densities remembered per integral object (uhf: alpha and beta)
 
 
-def _jk(Ints, D):
+def _jk(Ints, D, coulomb_only=False):
     """J and K of D.  One build gives both, and PyQuante's callers ask for
     them one at a time: getJ(Ints, D) then getK(Ints, D), and uhf does
     getJ(Da), getJ(Db), getK(Da), getK(Db).  So PackedInts and DirectInts
@@ -201,11 +204,14 @@ def _jk(Ints, D):
                else (Ints.tensor.data_ptr(), Ints.tensor.numel(), Ints.tensor._version))
         cache = Ints.__dict__.setdefault("_jk_cache", [])
         for i, (k, Dc, Jc, Kc) in enumerate(cache):
-            if k == key and Dc.shape == Dd.shape and torch.equal(Dc, Dd):
+            if k == key and Dc.shape == Dd.shape and torch.equal(Dc, Dd) and (Kc is not None or coulomb_only):
                 cache.insert(0, cache.pop(i))
-                return Jc.clone(), Kc.clone()
-        J, K = Ints.jk(Dd) if direct else jk_packed(Ints.tensor.contiguous(), Dd)
-        cache.insert(0, (key, Dd.clone(), J.clone(), K.clone()))
+                return Jc.clone(), (None if Kc is None else Kc.clone())
+        if direct and coulomb_only:
+            J, K = Ints.j(Dd), None
+        else:
+            J, K = Ints.jk(Dd) if direct else jk_packed(Ints.tensor.contiguous(), Dd)
+        cache.insert(0, (key, Dd.clone(), J.clone(), None if K is None else K.clone()))
         del cache[_JK_CACHE:]
         return J, K
     if isinstance(Ints, torch.Tensor):
@@ -243,9 +249,12 @@ def getJK2(Ints, Da, Db):
     return _back(Ja, Da), _back(Jb, Db), _back(Ka, Da), _back(Kb, Db)
 
 
-def getJ(Ints, D):
-    """J_ij = sum_kl (ij|kl) D_kl (PyQuante/Ints.py:195-208)."""
-    J, _ = _jk(Ints, D)
+def getJ(Ints, D, coulomb_only=False):
+    """J_ij = sum_kl (ij|kl) D_kl (PyQuante/Ints.py:195-208).  One build gives
+    J and K, so a following getK(Ints, D) costs nothing; ``coulomb_only=True``
+    (the DFT driver, which never asks for K) runs the integral-direct
+    Coulomb digestion alone instead."""
+    J, _ = _jk(Ints, D, coulomb_only)
     return _back(J, D)
 
 

@@ -185,8 +185,9 @@ struct WarpRuns {
 // element goes to global memory with one atomic.  Block mode: the weighted
 // integrals go to a shared tile; each output element is then one thread's
 // reduction over the tile (no shared-memory atomics).  With NDEN = 2 both
-// densities are digested from the same integrals (UHF).
-template <int NDEN>
+// densities are digested from the same integrals (UHF); WITHK = false keeps
+// the Coulomb terms alone.
+template <int NDEN, bool WITHK = true>
 struct EpiJKn {
     const double *D[NDEN];        // pre-scaled densities
     double *Jacc[NDEN], *Kacc[NDEN];
@@ -256,6 +257,7 @@ struct EpiJKn {
                 for (int d = 0; d < ND; ++d)
                     if (jcd[c][d] != (T)0) atomicAdd(Jb + (q.fc + c) * nm + q.fd + d, 2.0 * (double)jcd[c][d]);
         }
+        if constexpr (!WITHK) continue;   // Coulomb only
         // exchange rows of the bra's first shell: Kacc[a,c] += v D_bd, Kacc[a,d] += v D_bc
         {
             T dbd[NB][ND], dbc[NB][NC];
@@ -379,7 +381,8 @@ struct EpiJKn {
     {
         constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NCD = NC * ND;
         constexpr int ST = kTileStride<LA, LB, LC, LD>;
-        constexpr int O1 = NCD, O2 = O1 + NA * NC, O3 = O2 + NA * ND, O4 = O3 + NB * NC, O5 = O4 + NB * ND;
+        constexpr int O1 = NCD, O2 = O1 + NA * NC, O3 = O2 + NA * ND, O4 = O3 + NB * NC,
+                      O5 = WITHK ? O4 + NB * ND : O1;
         const int64_t nm = q.nm;
 #pragma unroll
         for (int sd = 0; sd < NDEN; ++sd) {
@@ -430,6 +433,8 @@ struct EpiJKn {
 // densities digesting the same integrals in one pass).
 using EpiJK = EpiJKn<1>;
 using EpiJK2 = EpiJKn<2>;
+// Coulomb only (DFT's getJ): no exchange products, no K atomics
+using EpiJ = EpiJKn<1, false>;
 
 
 

@@ -12,7 +12,7 @@
 
 namespace pqb {
 struct EpiPacked;
-template <int NDEN> struct EpiJKn;
+template <int NDEN, bool WITHK> struct EpiJKn;
 struct EpiSchwarz;
 
 cudaError_t launch_packed_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
@@ -22,6 +22,11 @@ cudaError_t launch_jk_f64(int qc, const int4 *list, int nq, const PairInfo *pair
 cudaError_t launch_jk_f32(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                           const double *Dscaled, const float *Dscaled_f, double *Jacc, double *Kacc, int n,
                           cudaStream_t st, int nsm);
+// J alone (the Coulomb digestion, no exchange)
+cudaError_t launch_j_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+                         const double *Dscaled, double *Jacc, cudaStream_t st, int nsm);
+cudaError_t launch_j_f32(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
+                         const double *Dscaled, const float *Dscaled_f, double *Jacc, cudaStream_t st, int nsm);
 // two densities (UHF alpha and beta) digesting the same integrals
 cudaError_t launch_jk2_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                            const double *const Dscaled[2], double *const Jacc[2], double *const Kacc[2],

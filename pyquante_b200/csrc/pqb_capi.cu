@@ -92,9 +92,10 @@ struct pqb_ctx {
     bool use_graph = true;
     int plan_threads = 0;            // host threads of pqb_plan (0: automatic)
     cudaStream_t cap_stream = nullptr;
-    // graphs: [mode] for one density, [2 + mode] for two (pqb_jk_direct2)
-    cudaGraphExec_t graph_exec[4] = {nullptr, nullptr, nullptr, nullptr};
-    bool graph_warm[4] = {false, false, false, false};   // one eager build first (one-time launch setup stays out of the capture)
+    // graphs: [mode] for one density, [2 + mode] for two (pqb_jk_direct2),
+    // [4 + mode] for J alone
+    cudaGraphExec_t graph_exec[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool graph_warm[6] = {false, false, false, false, false, false};   // one eager build first (one-time launch setup stays out of the capture)
     double *d_Jacc = nullptr, *d_Kacc = nullptr;
     double *d_Jacc2 = nullptr, *d_Kacc2 = nullptr;   // second density's graph accumulators
     // small scratch
@@ -1141,7 +1142,7 @@ static cudaError_t ensure_streams(pqb_ctx *ctx)
 
 static void drop_graphs(pqb_ctx *ctx)
 {
-    for (int gi = 0; gi < 4; ++gi) {
+    for (int gi = 0; gi < 6; ++gi) {
         if (ctx->graph_exec[gi]) cudaGraphExecDestroy(ctx->graph_exec[gi]);
         ctx->graph_exec[gi] = nullptr;
         ctx->graph_warm[gi] = false;
@@ -1770,13 +1771,15 @@ int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
 // (zeroed here) of nden = 1 or 2 densities on stream st, forked over the
 // context's streams and joined back; they read the scaled densities
 // (d_Dscaled / d_Dscaled_f, and d_Dscaled2 / d_Dscaled2_f for the second).
+// Kacc[0] == nullptr (one density): the Coulomb matrix alone.
 static int launch_build(pqb_ctx *ctx, int nden, double *const Jacc[2], double *const Kacc[2], int mode,
                         cudaStream_t st)
 {
     const int n = ctx->nbf;
+    const bool jonly = nden == 1 && !Kacc[0];
     for (int s = 0; s < nden; ++s) {
         PQB_CK(ctx, cudaMemsetAsync(Jacc[s], 0, sizeof(double) * ctx->dense_len, st));
-        PQB_CK(ctx, cudaMemsetAsync(Kacc[s], 0, sizeof(double) * ctx->dense_len, st));
+        if (!jonly) PQB_CK(ctx, cudaMemsetAsync(Kacc[s], 0, sizeof(double) * ctx->dense_len, st));
     }
     const double *Ds[2] = {ctx->d_Dscaled, ctx->d_Dscaled2};
     const float *Dsf[2] = {ctx->d_Dscaled_f, ctx->d_Dscaled2_f};
@@ -1805,7 +1808,12 @@ static int launch_build(pqb_ctx *ctx, int nden, double *const Jacc[2], double *c
         cudaStream_t sk = ctx->streams[k++ % ctx->nstreams];
         const int4 *list = ctx->d_plan + ctx->plan_off[part][c];
         const bool f32 = part == 1 && mode == PQB_MIXED;
-        if (nden == 2) {
+        if (jonly) {
+            if (f32)
+                PQB_CK(ctx, launch_j_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds[0], Dsf[0], Jacc[0], sk, ctx->nsm));
+            else
+                PQB_CK(ctx, launch_j_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds[0], Jacc[0], sk, ctx->nsm));
+        } else if (nden == 2) {
             if (f32)
                 PQB_CK(ctx, launch_jk2_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, Dsf, Jacc, Kacc, sk, ctx->nsm));
             else
@@ -1848,14 +1856,15 @@ static int ensure_acc_pair(pqb_ctx *ctx, double *&J, double *&K)
 
 // Capture launch_build into the ctx-owned accumulators as a graph for
 // (nden, mode) (index gi), once; later builds replay it with one launch.
-static int ensure_build_graph(pqb_ctx *ctx, int nden, int mode, int gi)
+static int ensure_build_graph(pqb_ctx *ctx, int nden, bool jonly, int mode, int gi)
 {
     if (ctx->graph_exec[gi]) return PQB_OK;
     if (!ctx->cap_stream) PQB_CK(ctx, cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
     int rc = ensure_acc_pair(ctx, ctx->d_Jacc, ctx->d_Kacc);
     if (rc == PQB_OK && nden == 2) rc = ensure_acc_pair(ctx, ctx->d_Jacc2, ctx->d_Kacc2);
     if (rc != PQB_OK) return rc;
-    double *const Ja[2] = {ctx->d_Jacc, ctx->d_Jacc2}, *const Ka[2] = {ctx->d_Kacc, ctx->d_Kacc2};
+    double *const Ja[2] = {ctx->d_Jacc, ctx->d_Jacc2};
+    double *const Ka[2] = {jonly ? nullptr : ctx->d_Kacc, ctx->d_Kacc2};
     PQB_CK(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
     rc = launch_build(ctx, nden, Ja, Ka, mode, ctx->cap_stream);
     cudaGraph_t g = nullptr;
@@ -1873,10 +1882,12 @@ static int ensure_build_graph(pqb_ctx *ctx, int nden, int mode, int gi)
     return PQB_OK;
 }
 
-// J and K of nden densities D[s] into J[s], K[s].
+// J and K of nden densities D[s] into J[s], K[s] (K[0] == nullptr with one
+// density: J alone).
 static int jk_direct_impl(pqb_ctx *ctx, int nden, const double *const D[2], double *const J[2], double *const K[2],
                           int mode, void *stream)
 {
+    const bool jonly = nden == 1 && !K[0];
     const int n = ctx->nbf;
     cudaStream_t st = (cudaStream_t)stream;
     PQB_CK(ctx, ensure_streams(ctx));
@@ -1900,15 +1911,16 @@ static int jk_direct_impl(pqb_ctx *ctx, int nden, const double *const D[2], doub
     // (a caller's own capture records the launches themselves)
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     PQB_CK(ctx, cudaStreamIsCapturing(st, &cs));
-    const int gi = (nden == 2 ? 2 : 0) + (mode == PQB_MIXED ? 1 : 0);
+    const int gi = (jonly ? 4 : (nden == 2 ? 2 : 0)) + (mode == PQB_MIXED ? 1 : 0);
     if (ctx->use_graph && ctx->nmol == 1 && cs == cudaStreamCaptureStatusNone && ctx->graph_warm[gi]) {
-        const int rc = ensure_build_graph(ctx, nden, mode, gi);
+        const int rc = ensure_build_graph(ctx, nden, jonly, mode, gi);
         if (rc != PQB_OK) return rc;
         PQB_CK(ctx, cudaGraphLaunch(ctx->graph_exec[gi], st));
         const double *Ja[2] = {ctx->d_Jacc, ctx->d_Jacc2}, *Ka[2] = {ctx->d_Kacc, ctx->d_Kacc2};
         for (int s = 0; s < nden; ++s) {
             symmetrize_into_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(Ja[s], J[s], n, ctx->d_escale);
-            symmetrize_into_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(Ka[s], K[s], n, ctx->d_escale);
+            if (!jonly)
+                symmetrize_into_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(Ka[s], K[s], n, ctx->d_escale);
         }
         PQB_CK(ctx, cudaGetLastError());
         return PQB_OK;
@@ -1919,10 +1931,11 @@ static int jk_direct_impl(pqb_ctx *ctx, int nden, const double *const D[2], doub
     for (int s = 0; s < nden; ++s) {
         if (ctx->nmol == 1) {
             symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(J[s], n, ctx->d_escale);
-            symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K[s], n, ctx->d_escale);
+            if (!jonly) symmetrize_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(K[s], n, ctx->d_escale);
         } else {
             symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(J[s], ctx->d_mol_off, ctx->d_mol_n, ctx->d_escale);
-            symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(K[s], ctx->d_mol_off, ctx->d_mol_n, ctx->d_escale);
+            if (!jonly)
+                symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(K[s], ctx->d_mol_off, ctx->d_mol_n, ctx->d_escale);
         }
     }
     PQB_CK(ctx, cudaGetLastError());
@@ -1931,7 +1944,7 @@ static int jk_direct_impl(pqb_ctx *ctx, int nden, const double *const D[2], doub
 
 int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode, void *stream)
 {
-    if (!ctx || !D || !J || !K) return fail(ctx, PQB_E_ARG, "pqb_jk_direct: bad arguments");
+    if (!ctx || !D || !J) return fail(ctx, PQB_E_ARG, "pqb_jk_direct: bad arguments");
     if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_jk_direct: call pqb_plan first");
     if (mode != PQB_FP64 && mode != PQB_MIXED) return fail(ctx, PQB_E_ARG, "pqb_jk_direct: mode %d", mode);
     PQB_CK(ctx, cudaSetDevice(ctx->device));

@@ -2,7 +2,7 @@
 (PyQuante/dft.py:29-215): the default grid (pyquante_b200.MolecularGrid,
 32 Euler--Maclaurin shells x 194 Lebedev points per atom, Becke
 partitioning), the SVWN functional, F = h + 2J + Fxc with J from
-``Ints.getJ`` (stored or integral-direct), DIIS on by default, and
+``Ints.getJ`` (stored, or integral-direct with the Coulomb digestion alone), DIIS on by default, and
 E = 2 tr(D h) + 2 tr(D J) + Exc + E_nuc with the spin-averaged density
 D = C_occ C_occ^T (+ half the open shells).
 
@@ -87,7 +87,7 @@ def dft(atoms, **kwargs):
     for it in range(MaxIter):
         D = mkdens_spinavg(orbs, nclosed, nopen)
         gr.setdens(D)
-        J = getJ(Ints, D)
+        J = getJ(Ints, D, coulomb_only=True)
         Exc, Fxc = getXC(gr, nel, functional=functional)
         F = h + 2 * J + Fxc
         if avg is not None:

@@ -218,6 +218,17 @@ class BasisEngine:
         self.ctx.check(self.ctx.lib.pqb_jk_direct(self.ctx.h, ptr(D), ptr(J), ptr(K), m, stream_ptr(stream)))
         return J, K
 
+    def j(self, D, mode="fp64", schwarz=1e-12, fp32_threshold=1e-5, J=None, stream=None):
+        """Integral-direct Coulomb matrix alone (no exchange digestion)."""
+        self._need_shells()
+        self.plan(schwarz, fp32_threshold)
+        D = D.to(device=self.device, dtype=torch.float64).contiguous()
+        if J is None:
+            J = torch.empty_like(D)
+        m = _lib.PQB_MIXED if mode == "mixed" else _lib.PQB_FP64
+        self.ctx.check(self.ctx.lib.pqb_jk_direct(self.ctx.h, ptr(D), ptr(J), None, m, stream_ptr(stream)))
+        return J
+
     def jk2(self, Da, Db, mode="fp64", schwarz=1e-12, fp32_threshold=1e-5, stream=None):
         """J and K of two densities (UHF alpha and beta) from one pass over the
         integrals: (Ja, Ka, Jb, Kb)."""

@@ -442,6 +442,28 @@ def test_two_density_build_equals_two_single_builds():
     assert np.abs(Jdb - Jo.cpu().numpy()).max() < ERI_TOL and np.abs(Kdb - Ko.cpu().numpy()).max() < ERI_TOL
 
 
+def test_coulomb_only_build_equals_the_j_of_the_full_build():
+    """pqb_jk_direct with K = NULL runs the Coulomb digestion alone: its J
+    equals the full build's (FP64 and mixed, first call and graph replays);
+    through the API, getJ(coulomb_only=True) then getK on the same density
+    still gives the full build's K."""
+    mol = geometries.water_cluster(3, seed=2)
+    bs = BasisSet(mol, "6-31g**")
+    eng = BasisEngine(bs.bfs)
+    D = torch.as_tensor(_rand_density(len(bs), 13), device="cuda")
+    for mode in ("fp64", "mixed"):
+        Jf, Kf = (x.clone() for x in eng.jk(D, mode, 1e-12, 1e-5))
+        for _ in range(3):
+            J = eng.j(D, mode, 1e-12, 1e-5)
+            assert float((J - Jf).abs().max()) < 1e-12 * float(Jf.abs().max()), mode
+    d = Ints.get2ints(bs, direct=True)
+    Dn = D.cpu().numpy()
+    J = Ints.getJ(d, Dn, coulomb_only=True)
+    K = Ints.getK(d, Dn)
+    Jf, Kf = eng.jk(D, "fp64", 1e-12, 1e-5)
+    assert np.abs(J - Jf.cpu().numpy()).max() < ERI_TOL and np.abs(K - Kf.cpu().numpy()).max() < ERI_TOL
+
+
 def test_single_function_and_zero_density_edge_cases():
     """He / STO-3G has one function and one unique integral: packed, direct
     and stored J/K against the oracle; a zero density gives J = K = 0."""
