@@ -1,7 +1,7 @@
 """Benchmark: integral-direct 2J-K Fock build on (H2O)8 / 6-31G** (N = 200).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pqb|reference]
-                    [--no-cpu-baseline] [--workload h2o8|stored|c16h34|h2o4-grad|batch|mp2]
+                    [--no-cpu-baseline] [--workload h2o8|stored|c16h34|h2o4-grad|batch|mp2|dft]
 
 One step = one full FP64 2J-K Fock build G(D) = 2J(D) - K(D) for a fixed SCF
 density D of the seeded (H2O)8 cluster (Schwarz 1e-12).  value = nominal
@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--soak", type=int, default=3000, help="untimed builds run under the clock sampler before the "
                                                            "timed ones")
-    p.add_argument("--workload", default="h2o8", choices=["h2o8", "stored", "c16h34", "h2o4-grad", "batch", "mp2"],
+    p.add_argument("--workload", default="h2o8", choices=["h2o8", "stored", "c16h34", "h2o4-grad", "batch", "mp2", "dft"],
                    help="h2o8: the headline Fock build; the others are the secondary workloads "
                         "(C16H34 threshold sweep, (H2O)4 gradient, batched SCF)")
     p.add_argument("--batch-count", type=int, default=512)
@@ -508,6 +508,64 @@ def run_mp2(a):
                                  "path": "pqb_mo_unpack_rows/pairs + cuBLAS DGEMM (torch.matmul) + pqb_mp2_pairs"}}))
 
 
+def run_dft(a):
+    """SVWN DFT on (H2O)8 / 6-31G** (N = 200) with the reference's default
+    grid (24 atoms x 32 x 194 points): one Coulomb-only direct build and one
+    exchange-correlation build (density on the grid, functional, Fxc) timed
+    on the device, and the whole SCF."""
+    import torch
+
+    from pyquante_b200 import Ints
+    from pyquante_b200.Basis.basis import BasisSet
+    from pyquante_b200.dft import dft, getXC
+    from pyquante_b200.MolecularGrid import MolecularGrid
+    mol = molecule()
+    bs = BasisSet(mol, "6-31g**")
+    t0 = time.perf_counter()
+    e, orbe, orbs = dft(mol, bfs=bs, direct=True, ConvCriteria=1e-8, MaxIter=60)
+    scf_s = time.perf_counter() - t0
+    nocc = mol.get_nel() // 2
+    C = torch.as_tensor(orbs, device="cuda")
+    D = (C[:, :nocc] @ C[:, :nocc].T).contiguous()
+    gr = MolecularGrid(mol)
+    gr.set_bf_amps(bs.bfs)
+    direct = Ints.get2ints(bs, direct=True)
+
+    def xc():
+        gr.setdens(D)
+        return getXC(gr, mol.get_nel())
+
+    def jonly():
+        return direct.engine.j(D, "fp64", 1e-12, 1e-5)
+
+    def jk():
+        return direct.engine.jk(D, "fp64", 1e-12, 1e-5)
+
+    out = {}
+    for name, fn in (("xc_ms", xc), ("coulomb_only_ms", jonly), ("j_and_k_ms", jk)):
+        for _ in range(max(a.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(a.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        out[name] = float(np.median(ts))
+    npts, nbf = gr.ng, gr.nbf
+    print(json.dumps({"metric": "SVWN DFT Fock-build parts on (H2O)8", "value": out["xc_ms"] + out["coulomb_only_ms"],
+                      "unit": "ms (XC + Coulomb build)", "higher_is_better": False, "steps": a.steps,
+                      "data": "synthetic", "dtype": "f64",
+                      "config": dict(out, workload=WORKLOAD, grid_points=npts, nbf=nbf, energy=e, scf_s=scf_s,
+                                     bfgrid_bytes=8 * npts * nbf,
+                                     path="pqb_grid_amps/pqb_grid_rowdot/pqb_xc_svwn + cuBLAS DGEMM; "
+                                          "pqb_jk_direct with K = NULL")}))
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -517,7 +575,7 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         {"stored": run_stored, "c16h34": run_c16h34, "h2o4-grad": run_h2o4_grad,
-         "batch": run_batch, "mp2": run_mp2}[a.workload](a)
+         "batch": run_batch, "mp2": run_mp2, "dft": run_dft}[a.workload](a)
         return
     import ctypes
 

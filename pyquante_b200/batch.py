@@ -11,17 +11,19 @@ torch) runs on the blocks padded per size bucket:
       J, K = pqb_jk_direct(D)            (one launch per class for the batch)
       F = h + 2J - K,  E = tr(Dh) + tr(DF) + E_nuc   (hartree_fock.py:29-38)
       Pulay DIIS per molecule            (Convergence.py:73-136)
-      F' = X^T F X, eigh, C = X C'        Cholesky X (LA2.py:47-75,113-116)
+      D' = projector on the occupied states of F' = X^T F X by batched
+    canonical purification (or eigh), D = X D' X^T   (Cholesky X, LA2.py:47-75,113-116)
 
 The molecules are grouped into at most 8 buckets of similar basis size
 for the dense work, so small molecules are not padded to the largest one.
 The Fock-build part of an iteration (densities, block gather/scatter, the
 multi-stream J/K launches, F and E of every bucket) is captured once in a
-CUDA graph and replayed; DIIS and the eigensolves run eagerly per bucket.
-A molecule is converged when its energy changes by less than ``conv`` (its
+CUDA graph and replayed; DIIS and the density update run eagerly per
+bucket, as batched GEMMs.  A molecule is converged when its energy changes
+by less than ``conv`` and its commutator FDS - SDF is below ``err_tol`` (its
 SCF time is the time of that iteration); converged molecules keep their
-last solution, and from the next iteration on their DIIS step and
-eigensolve (torch runs one eigensolve per molecule) are skipped.
+last solution, and from the next iteration on their DIIS step and density
+update are skipped.
 """
 import ctypes
 import time
@@ -146,15 +148,63 @@ class _Bucket:
         e, V = torch.linalg.eigh(X.transpose(1, 2) @ Fm @ X + shift)
         return X @ V
 
+    def density(self, Fm, ia=None, tol=1e-13, maxit=200):
+        """Densities D = X P X^T of the Fock matrices Fm without an
+        eigensolver: P, the projector on the nocc lowest states of
+        F' = X^T F X, by the canonical purification of Palser and
+        Manolopoulos (Phys. Rev. B 58, 12704 (1998)) -- batched GEMMs only.
+        Padded dimensions sit above the real spectrum and stay empty."""
+        X = self.X if ia is None else self.X.index_select(0, ia)
+        pad = self.pad if ia is None else self.pad.index_select(0, ia)
+        nocc = self.occ.sum(1) if ia is None else self.occ.index_select(0, ia).sum(1)
+        Fp = X.transpose(1, 2) @ Fm @ X
+        Fp = 0.5 * (Fp + Fp.transpose(1, 2))
+        nb = Fp.shape[-1]
+        # Gershgorin bounds of the real block; padded states just above them
+        radius = Fp.abs().sum(-1) - Fp.diagonal(dim1=1, dim2=2).abs()
+        d = Fp.diagonal(dim1=1, dim2=2)
+        hi = torch.where(pad, torch.full_like(d, -1e300), d + radius).amax(1)
+        lo = torch.where(pad, torch.full_like(d, 1e300), d - radius).amin(1)
+        top = hi + 1.0
+        Fp = Fp + torch.diag_embed(pad.to(Fp.dtype) * (top[:, None] - d))
+        hi = torch.maximum(hi, top)
+        mu = Fp.diagonal(dim1=1, dim2=2).sum(1) / nb
+        lam = torch.minimum(nocc / (hi - mu), (nb - nocc) / (mu - lo))
+        eye = torch.eye(nb, dtype=Fp.dtype, device=Fp.device)
+        P = (lam / nb)[:, None, None] * (mu[:, None, None] * eye - Fp) + (nocc / nb)[:, None, None] * eye
+        for _ in range(maxit):
+            P2 = P @ P
+            P3 = P2 @ P
+            num = (P2 - P3).diagonal(dim1=1, dim2=2).sum(1)
+            den = (P - P2).diagonal(dim1=1, dim2=2).sum(1)
+            done = den.abs() < tol * nb          # idempotent to rounding: keep
+            if bool(done.all()):
+                break
+            c = torch.where(done, torch.full_like(num, 0.5), num / torch.where(done, torch.ones_like(den), den))
+            c = c.clamp(0.0, 1.0)
+            hi_branch = ((1 + c)[:, None, None] * P2 - P3) / c.clamp(min=1e-300)[:, None, None]
+            lo_branch = ((1 - 2 * c)[:, None, None] * P + (1 + c)[:, None, None] * P2 - P3) / \
+                (1 - c).clamp(min=1e-300)[:, None, None]
+            Pn = torch.where((c >= 0.5)[:, None, None], hi_branch, lo_branch)
+            P = torch.where(done[:, None, None], P, Pn)
+        return X @ P @ X.transpose(1, 2)
+
 
 def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, graph=True, schwarz=1e-12,
-                fp32_threshold=1e-5, device=None, max_buckets=8):
+                fp32_threshold=1e-5, device=None, max_buckets=8, solver="purify", err_tol=1e-6):
     """Solve RHF for every (molecule, basis) in ``systems`` together.
 
     The Fock build of every iteration is one engine call for all molecules;
     the dense FP64 algebra runs per size bucket (molecules padded to the
-    bucket's largest basis).  Returns a dict: energies, iterations,
-    per-molecule SCF times (s), total time (s), and the plan counts."""
+    bucket's largest basis).  ``solver='purify'`` (default) gets each new
+    density from the DIIS Fock matrix by batched canonical purification
+    (GEMMs only, no per-molecule eigensolver); ``'eigh'`` diagonalises.
+    A molecule is converged when its energy changes by less than ``conv``
+    and its commutator max|FDS - SDF| is below ``err_tol``.  Returns a
+    dict: energies, iterations, per-molecule SCF times (s), total time (s),
+    and the plan counts."""
+    if solver not in ("purify", "eigh"):
+        raise ValueError("solver must be 'purify' or 'eigh'")
     t_start = time.perf_counter()
     eng = BatchEngine(systems, device)
     dev = eng.device
@@ -168,16 +218,22 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
         S_list.append(Sb)
         h_list.append(Tb + Vb)
     buckets = [_Bucket(idx, eng, S_list, h_list, dev) for idx in _bucket_edges(np.array(eng.n), max_buckets)]
+    def new_density(bk, Fm, ia=None):
+        if solver == "purify":
+            return bk.density(Fm, ia)
+        C = bk.solve(Fm, ia)
+        occ = bk.occ if ia is None else bk.occ.index_select(0, ia)
+        Co = C * occ[:, None, :]
+        return Co @ Co.transpose(1, 2)
+
     for bk in buckets:
-        bk.C.copy_(bk.solve(bk.h))
+        bk.D.copy_(new_density(bk, bk.h))
     Dflat = torch.zeros(eng.dense_len, **f64)
     Jf = torch.zeros_like(Dflat)
     Kf = torch.zeros_like(Dflat)
 
     def fock_build():
         for bk in buckets:
-            Co = bk.C * bk.occ[:, None, :]
-            bk.D.copy_(Co @ Co.transpose(1, 2))
             Dflat.index_copy_(0, bk.flat, bk.D.reshape(-1).index_select(0, bk.pos))
         eng.jk(Dflat, Jf, Kf, precision)
         for bk in buckets:
@@ -239,13 +295,14 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
             c = torch.where((info == 0)[:, None], c, torch.nn.functional.one_hot(
                 torch.full((Bb,), k - 1, device=dev), k + 1).to(torch.float64))
             Fd = (c[:, :k, None, None] * torch.stack(bk.Fs, dim=1)).sum(dim=1)
+            emax = err.abs().amax(dim=(1, 2))
+            energy = bk.E.clone()
             if act.all():
-                bk.C.copy_(bk.solve(Fd))
+                bk.D.copy_(new_density(bk, Fd))
             else:
                 ia = torch.from_numpy(np.nonzero(act)[0]).to(dev)
-                bk.C.index_copy_(0, ia, bk.solve(Fd.index_select(0, ia), ia))
-            energy = bk.E.clone()
-            newly = (~bdone[q]) & ((energy - eold[q]).abs() < conv)
+                bk.D.index_copy_(0, ia, new_density(bk, Fd.index_select(0, ia), ia))
+            newly = (~bdone[q]) & ((energy - eold[q]).abs() < conv) & (emax < err_tol)
             eold[q] = torch.where(bdone[q], eold[q], energy)
             bdone[q] = bdone[q] | newly
         flags = [(bd.cpu().numpy(), e.cpu().numpy()) for bd, e in zip(bdone, eold)]
