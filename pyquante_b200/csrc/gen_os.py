@@ -291,14 +291,32 @@ def emitted_flops(lines):
     return out["vrr"], out["hrr"]
 
 
+def geometry_flops(lines):
+    """Flops of the per-primitive-quartet coefficients the emitted VRR
+    reads (the kernel computes the others, but the compiler drops them):
+    PA_i, QC_i (a subtraction each), WP_i, WQ_i (a product each, after
+    rho/zeta or rho/eta), the three 1/(2x) factors."""
+    body = "\n".join(ln for ln in lines if "g." in ln)
+    n = sum(1 for f in ("PA", "QC", "WP", "WQ") for i in range(3) if "g.%s[%d]" % (f, i) in body)
+    if "g.WP[" in body or "g.rz" in body:
+        n += 1
+    if "g.WQ[" in body or "g.re" in body:
+        n += 1
+    n += sum(1 for f in ("oo2z", "oo2e", "oo2ze") if "g.%s" % f in body)
+    return n
+
+
 _FLOPS = {}
 
 
 def class_flops(LA, LB, LC, LD):
-    """Cached (vrr flops per primitive quartet, hrr flops per item)."""
+    """Cached (flops per primitive quartet of the VRR and of the coefficients
+    it reads, hrr flops per item)."""
     key = (LA, LB, LC, LD)
     if key not in _FLOPS:
-        _FLOPS[key] = emitted_flops(emit_class(*key)[0])
+        lines = emit_class(*key)[0]
+        v, h = emitted_flops(lines)
+        _FLOPS[key] = (v + geometry_flops(lines), h)
     return _FLOPS[key]
 
 

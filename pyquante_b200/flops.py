@@ -9,8 +9,9 @@ Obara--Saika classes (LA+LB+LC+LD = LT <= 4, csrc/os_classes.inc):
             LT 2, 3: 3 + F_3 Horner 12 + exp series 12 + 2 + recursion 3 x 3 = 38;
             LT 4:    the same with four recursion steps = 41
   prefactor (LT+1) products
-  geometry  PA, QC, rz, re, WP, WQ, 1/(2 zeta), 1/(2 eta), 1/(2(zeta+eta)): 17
-  VRR       the emitted vertical recurrence (gen_os.class_flops)
+  VRR       the emitted vertical recurrence and the coefficients it reads
+            (PA, QC, WP, WQ components, rho/zeta, rho/eta, the 1/(2x) factors;
+            gen_os.class_flops)
   per item  the emitted horizontal transfer, plus the J/K digestion
 Rys classes (the block-mode classes, 3+ roots):
   roots     NR roots x 2 series (root, weight) x Clenshaw(14 coef): 13 x (FMA+sub)
@@ -69,7 +70,7 @@ def prim_quartet_flops(LA, LB, LC, LD):
     """FP64 flops per primitive quartet of class (LA LB|LC LD)."""
     LT = LA + LB + LC + LD
     if uses_os(LA, LB, LC, LD):
-        return 24 + _os_boys_flops(LT) + (LT + 1) + 17 + gen_os.class_flops(LA, LB, LC, LD)[0]
+        return 24 + _os_boys_flops(LT) + (LT + 1) + gen_os.class_flops(LA, LB, LC, LD)[0]
     NR = LT // 2 + 1
     nab, ncd = ncart(LA) * ncart(LB), ncart(LC) * ncart(LD)
     return 20 + NR * 84 + NR * 3 * rys2d_flops(LA, LB, LC, LD) + nab * ncd * NR * 3
