@@ -14,8 +14,9 @@
 // component as crys.contr_coulomb does (Src/crys.c:34-54).
 //
 // Two execution modes:
-//  * thread mode (NAB*NCD <= 54 in FP64, <= 81 in FP32): one thread per quartet,
-//    2-D integrals and all contracted components live in registers.
+//  * thread mode (NAB*NCD <= 81, which is every class with L <= 4): one
+//    thread per work item; the recurrence intermediates and all contracted
+//    components live in registers.
 //  * block mode (larger classes): a 256-thread block holds NSQ = 256/NAB
 //    quartets; per primitive quartet the roots (NSQ*NR tasks) and the 2-D
 //    integrals (NSQ*NR*3 tasks) go to shared memory, then every thread
@@ -609,9 +610,14 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
         R acc[NAB * NCD];
 #pragma unroll
         for (int c = 0; c < NAB * NCD; ++c) acc[c] = (R)0;
-        const int npk = pk.nprim;
+        // primitive quartet g of the item = (bra primitive g % npb, ket
+        // primitive g / npb): the bra index runs fastest, so the lanes of a
+        // warp (which share the bra pair) step through the same bra
+        // primitives and each lane fetches its own ket primitive pair only
+        // once per npb steps
+        const int npb = pb.nprim;
         const PrimPair *pbp = prims + pb.prim_off, *pkp = prims + pk.prim_off;
-        int ib = e.z / npk, ik = e.z - (e.z / npk) * npk;
+        int ik = e.z / npb, ib = e.z - (e.z / npb) * npb;
         if constexpr (std::is_same_v<R, float>) {
             // FP32 list of the mixed mode: single-precision primitive data
             QuartetGeomF gf;
@@ -622,28 +628,33 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
                 gf.AB[x] = (float)pb.AB[x];
                 gf.CD[x] = (float)pk.AB[x];
             }
-            float P[8], Qn[8];
-            ld8f(pbp[ib].f, P);
-            ld8f(pkp[ik].f, Qn);
+            float Pn[8], Q[8];
+            ld8f(pbp[ib].f, Pn);
+            ld8f(pkp[ik].f, Q);
             using OS = OsClass<LA, LB, LC, LD>;
             float v[OS::NV];
 #pragma unroll
             for (int c = 0; c < OS::NV; ++c) v[c] = 0.0f;
             for (int t = 0; t < e.w; ++t) {
-                float Q[8];
+                float P[8];
 #pragma unroll
-                for (int c = 0; c < 8; ++c) Q[c] = Qn[c];
-                int ik2 = ik + 1, ib2 = ib;
-                if (ik2 == npk) {
-                    ik2 = 0;
-                    ++ib2;
+                for (int c = 0; c < 8; ++c) P[c] = Pn[c];
+                int ib2 = ib + 1, ik2 = ik;
+                if (ib2 == npb) {
+                    ib2 = 0;
+                    ++ik2;
                 }
-                if (t + 1 < e.w) ld8f(pkp[ik2].f, Qn);
+                if (t + 1 < e.w) ld8f(pbp[ib2].f, Pn);
+                float Qn[8];
+                if (ik2 != ik && t + 1 < e.w) ld8f(pkp[ik2].f, Qn);
                 if constexpr (OS::kOn)
                     os_prim_quartet_f32<LA, LB, LC, LD>(gf, P, Q, v);
                 else
                     add_prim_quartet_f32<LA, LB, LC, LD>(gf, P, Q, reinterpret_cast<float *>(acc));
-                if (ib2 != ib && t + 1 < e.w) ld8f(pbp[ib2].f, P);
+                if (ik2 != ik && t + 1 < e.w) {
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) Q[c] = Qn[c];
+                }
                 ib = ib2;
                 ik = ik2;
             }
@@ -652,8 +663,8 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
             epi.template thread_quartet<LA, LB, LC, LD, R>(q, acc, lane, live);
             continue;
         }
-        PrimJK P = load_prim_jk(pbp + ib);
-        PrimJK Qn = load_prim_jk(pkp + ik);
+        PrimJK Pn = load_prim_jk(pbp + ib);
+        PrimJK Q = load_prim_jk(pkp + ik);
         if constexpr (OsClass<LA, LB, LC, LD>::kOn) {
             // Obara--Saika per primitive quartet, Head-Gordon--Pople transfer
             // once per item on the contracted [e0|f0]
@@ -663,13 +674,16 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
 #pragma unroll
             for (int c = 0; c < OS::NV; ++c) v[c] = (R)0;
             for (int t = 0; t < e.w; ++t) {
-                const PrimJK Q = Qn;
-                int ik2 = ik + 1, ib2 = ib;
-                if (ik2 == npk) {
-                    ik2 = 0;
-                    ++ib2;
+                const PrimJK P = Pn;
+                int ib2 = ib + 1, ik2 = ik;
+                if (ib2 == npb) {
+                    ib2 = 0;
+                    ++ik2;
                 }
-                if (t + 1 < e.w) Qn = load_prim_jk(pkp + ik2);
+                if (t + 1 < e.w) Pn = load_prim_jk(pbp + ib2);
+                // the next ket primitive pair, fetched a step ahead
+                PrimJK Qn = Q;
+                if (ik2 != ik && t + 1 < e.w) Qn = load_prim_jk(pkp + ik2);
                 const double zeta = P.zeta, eta = Q.zeta;
                 const double PQx = P.P[0] - Q.P[0], PQy = P.P[1] - Q.P[1], PQz = P.P[2] - Q.P[2];
                 const double rs = rsqrt_nr(zeta + eta);
@@ -701,7 +715,7 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
                 g.oo2e = 0.5 * Q.izeta;
                 g.oo2ze = 0.5 * izpe;
                 OS::template vrr<R>(g, Fs, v);
-                if (ib2 != ib && t + 1 < e.w) P = load_prim_jk(pbp + ib2);
+                Q = Qn;
                 ib = ib2;
                 ik = ik2;
             }
@@ -712,14 +726,14 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
             continue;
         }
         for (int t = 0; t < e.w; ++t) {
-            const PrimJK Q = Qn;
-            // next primitive quartet's ket pair is fetched while this one computes
-            int ik2 = ik + 1, ib2 = ib;
-            if (ik2 == npk) {
-                ik2 = 0;
-                ++ib2;
+            const PrimJK P = Pn;
+            // the next bra primitive pair is fetched while this one computes
+            int ib2 = ib + 1, ik2 = ik;
+            if (ib2 == npb) {
+                ib2 = 0;
+                ++ik2;
             }
-            if (t + 1 < e.w) Qn = load_prim_jk(pkp + ik2);
+            if (t + 1 < e.w) Pn = load_prim_jk(pbp + ib2);
             const double zeta = P.zeta, eta = Q.zeta;
             const double PQx = P.P[0] - Q.P[0], PQy = P.P[1] - Q.P[1], PQz = P.P[2] - Q.P[2];
             const double rs = rsqrt_nr(zeta + eta);
@@ -749,7 +763,7 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
                         acc[ab * NCD + cd] += gx[ox] * gy[oy] * gz[oz];
                     }
             }
-            if (ib2 != ib && t + 1 < e.w) P = load_prim_jk(pbp + ib2);
+            if (ik2 != ik && t + 1 < e.w) Q = load_prim_jk(pkp + ik2);
             ib = ib2;
             ik = ik2;
         }
@@ -761,6 +775,11 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
 // ----------------------------------------------------------- block mode --
 constexpr int kBlockThreads = 256;
 
+// Shared-memory budget of the 2-D integrals of one round of a block: PB
+// primitive quartets per slot go through the roots, 2-D and assembly phases
+// together (two barriers per round), as many as fit in the budget (at most 4).
+constexpr size_t kBlockRoundBytes = 64 * 1024;
+
 template <int LA, int LB, int LC, int LD, typename R, class Epi>
 struct BlockLayout {
     static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
@@ -768,7 +787,11 @@ struct BlockLayout {
     static constexpr int NR = (LA + LB + LC + LD) / 2 + 1;
     static constexpr int G2D = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
     static constexpr int NSQ = kBlockThreads / NAB;
-    static constexpr size_t g_bytes = ((size_t)NSQ * 3 * NR * G2D * sizeof(R) + 15) / 16 * 16;
+    static constexpr size_t pq_bytes = (size_t)NSQ * 3 * NR * G2D * sizeof(R);   // one primitive quartet per slot
+    static constexpr int PB = pq_bytes * 4 <= kBlockRoundBytes ? 4
+                              : pq_bytes * 3 <= kBlockRoundBytes ? 3
+                              : pq_bytes * 2 <= kBlockRoundBytes ? 2 : 1;
+    static constexpr size_t g_bytes = (PB * pq_bytes + 15) / 16 * 16;
     // the integral tile of a tiled epilogue reuses the 2-D integral buffer
     static constexpr size_t tile_bytes = Epi::kTile ? (size_t)NSQ * NAB * (NCD + 1) * sizeof(double) : 0;
     static constexpr size_t bytes = g_bytes > tile_bytes ? g_bytes : tile_bytes;
@@ -790,12 +813,12 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
 {
     using Lay = BlockLayout<LA, LB, LC, LD, R, Epi>;
     constexpr int NB = Lay::NB, NC = Lay::NC, ND = Lay::ND, NAB = Lay::NAB, NCD = Lay::NCD;
-    constexpr int NR = Lay::NR, G2D = Lay::G2D, NSQ = Lay::NSQ;
+    constexpr int NR = Lay::NR, G2D = Lay::G2D, NSQ = Lay::NSQ, PB = Lay::PB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *sg = reinterpret_cast<R *>(smem_raw);
     __shared__ SlotData sd[NSQ];
-    __shared__ SlotPrim sp[NSQ];
-    __shared__ double su[NSQ][NR], sw[NSQ][NR];
+    __shared__ SlotPrim sp[PB][NSQ];
+    __shared__ double su[PB][NSQ][NR], sw[PB][NSQ][NR];
     __shared__ int s_maxpp;
 
     const int tid = threadIdx.x;
@@ -845,10 +868,13 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
 #pragma unroll
         for (int c = 0; c < NCD; ++c) acc[c] = (R)0;
 
-        for (int pp = 0; pp < maxpp; ++pp) {
+        for (int pp0 = 0; pp0 < maxpp; pp0 += PB) {
+            // this round: primitive quartets pp0 .. pp0 + nb - 1 of every slot
+            const int nb = maxpp - pp0 < PB ? maxpp - pp0 : PB;
             // roots and weights (with the primitive-quartet prefactor)
-            for (int t = tid; t < NSQ * NR; t += kBlockThreads) {
-                const int s = t / NR, r = t - s * NR;
+            for (int t = tid; t < nb * NSQ * NR; t += kBlockThreads) {
+                const int b = t / (NSQ * NR), rem = t - b * (NSQ * NR), s = rem / NR, r = rem - s * NR;
+                const int pp = pp0 + b;
                 const SlotData &S = sd[s];
                 if (pp < S.npp) {
                     const int g = S.pp0 + pp;
@@ -867,10 +893,10 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
                     } else {
                         rys_root(NR, r, T, u, w);
                     }
-                    su[s][r] = u;
-                    sw[s][r] = w * P.K * Q.K * rsqrt(zpe);
+                    su[b][s][r] = u;
+                    sw[b][s][r] = w * P.K * Q.K * rsqrt(zpe);
                     if (r == 0) {
-                        SlotPrim &p = sp[s];
+                        SlotPrim &p = sp[b][s];
                         p.zeta = P.zeta;
                         p.eta = Q.zeta;
                         p.PQ[0] = PQx;
@@ -882,40 +908,44 @@ __global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__
                         }
                     }
                 } else {
-                    su[s][r] = 0.0;
-                    sw[s][r] = 0.0;
+                    su[b][s][r] = 0.0;
+                    sw[b][s][r] = 0.0;
                     if (r == 0) {
-                        SlotPrim &p = sp[s];
+                        SlotPrim &p = sp[b][s];
                         p.zeta = p.eta = 1.0;
                         for (int x = 0; x < 3; ++x) p.PA[x] = p.QC[x] = p.PQ[x] = 0.0;
                     }
                 }
             }
             __syncthreads();
-            // 2-D integrals, one (slot, root, axis) per task; weight on x
-            for (int t = tid; t < NSQ * NR * 3; t += kBlockThreads) {
-                const int s = t / (NR * 3), rem = t - s * NR * 3, r = rem / 3, x = rem - r * 3;
-                const SlotPrim &p = sp[s];
-                rys2d<LA, LB, LC, LD, R>(su[s][r], p.zeta, p.eta, p.PA[x], p.QC[x], p.PQ[x], sd[s].AB[x], sd[s].CD[x],
-                                         x == 0 ? sw[s][r] : 1.0, sg + ((size_t)(s * 3 + x) * NR + r) * G2D);
+            // 2-D integrals, one (round quartet, slot, root, axis) per task; weight on x
+            for (int t = tid; t < nb * NSQ * NR * 3; t += kBlockThreads) {
+                const int b = t / (NSQ * NR * 3), rb = t - b * (NSQ * NR * 3);
+                const int s = rb / (NR * 3), rem = rb - s * NR * 3, r = rem / 3, x = rem - r * 3;
+                const SlotPrim &p = sp[b][s];
+                rys2d<LA, LB, LC, LD, R>(su[b][s][r], p.zeta, p.eta, p.PA[x], p.QC[x], p.PQ[x], sd[s].AB[x],
+                                         sd[s].CD[x], x == 0 ? sw[b][s][r] : 1.0,
+                                         sg + ((size_t)((b * NSQ + s) * 3 + x) * NR + r) * G2D);
             }
             __syncthreads();
             // assembly: this thread's bra pair (ia, ib) times every ket pair
             if (active) {
-                const R *gx = sg + (size_t)(slot * 3 + 0) * NR * G2D + ox;
-                const R *gy = sg + (size_t)(slot * 3 + 1) * NR * G2D + oy;
-                const R *gz = sg + (size_t)(slot * 3 + 2) * NR * G2D + oz;
+                for (int b = 0; b < nb; ++b) {
+                    const R *gx = sg + (size_t)((b * NSQ + slot) * 3 + 0) * NR * G2D + ox;
+                    const R *gy = sg + (size_t)((b * NSQ + slot) * 3 + 1) * NR * G2D + oy;
+                    const R *gz = sg + (size_t)((b * NSQ + slot) * 3 + 2) * NR * G2D + oz;
 #pragma unroll
-                for (int r = 0; r < NR; ++r)
+                    for (int r = 0; r < NR; ++r)
 #pragma unroll
-                    for (int ic = 0; ic < NC; ++ic)
+                        for (int ic = 0; ic < NC; ++ic)
 #pragma unroll
-                        for (int id = 0; id < ND; ++id) {
-                            const int cx = cart_lx(LC, ic) * (LD + 1) + cart_lx(LD, id);
-                            const int cy = cart_ly(LC, ic) * (LD + 1) + cart_ly(LD, id);
-                            const int cz = cart_lz(LC, ic) * (LD + 1) + cart_lz(LD, id);
-                            acc[ic * ND + id] += gx[r * G2D + cx] * gy[r * G2D + cy] * gz[r * G2D + cz];
-                        }
+                            for (int id = 0; id < ND; ++id) {
+                                const int cx = cart_lx(LC, ic) * (LD + 1) + cart_lx(LD, id);
+                                const int cy = cart_ly(LC, ic) * (LD + 1) + cart_ly(LD, id);
+                                const int cz = cart_lz(LC, ic) * (LD + 1) + cart_lz(LD, id);
+                                acc[ic * ND + id] += gx[r * G2D + cx] * gy[r * G2D + cy] * gz[r * G2D + cz];
+                            }
+                }
             }
         }
 

@@ -146,8 +146,11 @@ __global__ void symmetrize_kernel(double *M, int n, const double *__restrict__ S
     M[(int64_t)j * n + i] = s;
 }
 
-// symmetrize_kernel from the accumulator A into M (every element of M written)
-__global__ void symmetrize_into_kernel(const double *__restrict__ A, double *M, int n, const double *__restrict__ S)
+// The graph path's epilogue: J and K (K2 == nullptr: J alone) from their
+// accumulators, which are left zeroed for the next replay of the build graph
+// (so the graph holds no memset nodes).
+__global__ void symmetrize_take_kernel(double *__restrict__ A1, double *__restrict__ M1, double *__restrict__ A2,
+                                       double *__restrict__ M2, int n, const double *__restrict__ S)
 {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t P = (int64_t)n * (n + 1) / 2;
@@ -156,10 +159,20 @@ __global__ void symmetrize_into_kernel(const double *__restrict__ A, double *M, 
     while ((int64_t)i * (i + 1) / 2 > t) --i;
     while ((int64_t)(i + 1) * (i + 2) / 2 <= t) ++i;
     int j = (int)(t - (int64_t)i * (i + 1) / 2);
-    double s = A[(int64_t)i * n + j] + A[(int64_t)j * n + i];
-    if (S) s *= S[(int64_t)i * n + j];
-    M[(int64_t)i * n + j] = s;
-    M[(int64_t)j * n + i] = s;
+    const int64_t ij = (int64_t)i * n + j, ji = (int64_t)j * n + i;
+    const double sc = S ? S[ij] : 1.0;
+    const double s1 = (A1[ij] + A1[ji]) * sc;
+    A1[ij] = 0.0;
+    A1[ji] = 0.0;
+    M1[ij] = s1;
+    M1[ji] = s1;
+    if (A2) {
+        const double s2 = (A2[ij] + A2[ji]) * sc;
+        A2[ij] = 0.0;
+        A2[ji] = 0.0;
+        M2[ij] = s2;
+        M2[ji] = s2;
+    }
 }
 
 // Batched form: one CUDA block per molecule block of a block-diagonal layout.
@@ -1772,12 +1785,14 @@ int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream)
 // context's streams and joined back; they read the scaled densities
 // (d_Dscaled / d_Dscaled_f, and d_Dscaled2 / d_Dscaled2_f for the second).
 // Kacc[0] == nullptr (one density): the Coulomb matrix alone.
+// zero: clear the accumulators first (the graph's accumulators are kept
+// zeroed by symmetrize_take_kernel instead).
 static int launch_build(pqb_ctx *ctx, int nden, double *const Jacc[2], double *const Kacc[2], int mode,
-                        cudaStream_t st)
+                        cudaStream_t st, bool zero = true)
 {
     const int n = ctx->nbf;
     const bool jonly = nden == 1 && !Kacc[0];
-    for (int s = 0; s < nden; ++s) {
+    for (int s = 0; s < nden && zero; ++s) {
         PQB_CK(ctx, cudaMemsetAsync(Jacc[s], 0, sizeof(double) * ctx->dense_len, st));
         if (!jonly) PQB_CK(ctx, cudaMemsetAsync(Kacc[s], 0, sizeof(double) * ctx->dense_len, st));
     }
@@ -1845,6 +1860,9 @@ static int ensure_acc_pair(pqb_ctx *ctx, double *&J, double *&K)
     const size_t bytes = sizeof(double) * std::max<long long>(ctx->dense_len, 1);
     cudaError_t e = cudaMalloc(&J, bytes);
     if (e == cudaSuccess) e = cudaMalloc(&K, bytes);
+    // zeroed once here; each use leaves them zeroed (symmetrize_take_kernel)
+    if (e == cudaSuccess) e = cudaMemset(J, 0, bytes);
+    if (e == cudaSuccess) e = cudaMemset(K, 0, bytes);
     if (e != cudaSuccess) {
         free_dev(J);
         free_dev(K);
@@ -1866,7 +1884,7 @@ static int ensure_build_graph(pqb_ctx *ctx, int nden, bool jonly, int mode, int 
     double *const Ja[2] = {ctx->d_Jacc, ctx->d_Jacc2};
     double *const Ka[2] = {jonly ? nullptr : ctx->d_Kacc, ctx->d_Kacc2};
     PQB_CK(ctx, cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
-    rc = launch_build(ctx, nden, Ja, Ka, mode, ctx->cap_stream);
+    rc = launch_build(ctx, nden, Ja, Ka, mode, ctx->cap_stream, false);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(ctx->cap_stream, &g);   // always ends the capture
     if (rc != PQB_OK || e != cudaSuccess) {
@@ -1916,12 +1934,10 @@ static int jk_direct_impl(pqb_ctx *ctx, int nden, const double *const D[2], doub
         const int rc = ensure_build_graph(ctx, nden, jonly, mode, gi);
         if (rc != PQB_OK) return rc;
         PQB_CK(ctx, cudaGraphLaunch(ctx->graph_exec[gi], st));
-        const double *Ja[2] = {ctx->d_Jacc, ctx->d_Jacc2}, *Ka[2] = {ctx->d_Kacc, ctx->d_Kacc2};
-        for (int s = 0; s < nden; ++s) {
-            symmetrize_into_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(Ja[s], J[s], n, ctx->d_escale);
-            if (!jonly)
-                symmetrize_into_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(Ka[s], K[s], n, ctx->d_escale);
-        }
+        double *Ja[2] = {ctx->d_Jacc, ctx->d_Jacc2}, *Ka[2] = {ctx->d_Kacc, ctx->d_Kacc2};
+        for (int s = 0; s < nden; ++s)
+            symmetrize_take_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(
+                Ja[s], J[s], jonly ? nullptr : Ka[s], jonly ? nullptr : K[s], n, ctx->d_escale);
         PQB_CK(ctx, cudaGetLastError());
         return PQB_OK;
     }
