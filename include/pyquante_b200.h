@@ -260,8 +260,12 @@ int pqb_grad_1e(pqb_ctx *ctx, int n, const double *origin, const int *powers, co
 int64_t pqb_ijkl2intindex(int64_t i, int64_t j, int64_t k, int64_t l);
 
 /* Kernel-level checks: F_0..F_m(T_i) into F[i*(m+1)+k] (m <= 16), and the
- * n-root Rys rule (n <= 5) at T_i into u[i*n+r], w[i*n+r].  Device arrays. */
+ * n-root Rys rule (n <= 5) at T_i into u[i*n+r], w[i*n+r].  Device arrays.
+ * pqb_boys_rows_eval: F_0..F_lt (lt <= 4) by the form the thread-mode
+ * Fock-build kernels use (compact Taylor rows, large-T asymptotics, no
+ * branches), into F[i*(lt+1)+k]. */
 int pqb_boys_eval(pqb_ctx *ctx, int m, int count, const double *T, double *F, void *stream);
+int pqb_boys_rows_eval(pqb_ctx *ctx, int lt, int count, const double *T, double *F, void *stream);
 int pqb_rys_eval(pqb_ctx *ctx, int nroots, int count, const double *T, double *u, double *w, void *stream);
 
 #ifdef __cplusplus

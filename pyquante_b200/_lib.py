@@ -66,6 +66,7 @@ SIGNATURES = {
     "pqb_xc_svwn": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "pqb_ijkl2intindex": (ctypes.c_int64, [ctypes.c_int64] * 4),
     "pqb_boys_eval": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
+    "pqb_boys_rows_eval": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "pqb_rys_eval": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),
 }
 

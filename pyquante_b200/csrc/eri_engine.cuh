@@ -686,12 +686,12 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
                 if (ik2 != ik && t + 1 < e.w) Qn = load_prim_jk(pkp + ik2);
                 const double zeta = P.zeta, eta = Q.zeta;
                 const double PQx = P.P[0] - Q.P[0], PQy = P.P[1] - Q.P[1], PQz = P.P[2] - Q.P[2];
-                const double rs = rsqrt_nr(zeta + eta);
+                const double rs = rsqrt_nr_unchecked(zeta + eta);   // exponent sums: 1e-36 < x < 1e36
                 const double izpe = rs * rs;
                 const double T = zeta * eta * izpe * (PQx * PQx + PQy * PQy + PQz * PQz);
                 const double pre = P.K * Q.K * rs;
                 double F[LT + 1];
-                boys_os<LT>(T, F);
+                boys_os_bf<LT>(T, F);
                 R Fs[LT + 1];
 #pragma unroll
                 for (int m = 0; m <= LT; ++m) Fs[m] = (R)(F[m] * pre);
@@ -806,8 +806,9 @@ struct SlotPrim {
     double zeta, eta, PA[3], QC[3], PQ[3];
 };
 
+// (the classes with at most six ket components fit three blocks per SM)
 template <int LA, int LB, int LC, int LD, typename R, class Epi>
-__global__ void __launch_bounds__(kBlockThreads) eri_block_kernel(const int4 *__restrict__ list, int nq,
+__global__ void __launch_bounds__(kBlockThreads, ncart(LC) * ncart(LD) <= 6 ? 3 : 0) eri_block_kernel(const int4 *__restrict__ list, int nq,
                                                                   const PairInfo *__restrict__ pairs,
                                                                   const PrimPair *__restrict__ prims, Epi epi)
 {

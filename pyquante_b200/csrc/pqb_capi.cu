@@ -1030,6 +1030,23 @@ __global__ void boys_eval_kernel(int m, int count, const double *T, double *F)
     for (int k = 0; k <= m; ++k) F[(int64_t)t * (m + 1) + k] = f[k];
 }
 
+// F_0 .. F_lt by the branch-free compact-row form of the thread-mode kernels
+// (boys_os_bf)
+__global__ void boys_rows_eval_kernel(int lt, int count, const double *T, double *F)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    double f[5];
+    switch (lt) {
+    case 0: boys_os_bf<0>(T[t], f); break;
+    case 1: boys_os_bf<1>(T[t], f); break;
+    case 2: boys_os_bf<2>(T[t], f); break;
+    case 3: boys_os_bf<3>(T[t], f); break;
+    default: boys_os_bf<4>(T[t], f); break;
+    }
+    for (int k = 0; k <= lt; ++k) F[(int64_t)t * (lt + 1) + k] = f[k];
+}
+
 __global__ void rys_eval_kernel(int nr, int count, const double *T, double *u, double *w)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2298,6 +2315,16 @@ int pqb_boys_eval(pqb_ctx *ctx, int m, int count, const double *T, double *F, vo
     if (count == 0) return PQB_OK;
     PQB_CK(ctx, cudaSetDevice(ctx->device));
     boys_eval_kernel<<<(count + 127) / 128, 128, 0, (cudaStream_t)stream>>>(m, count, T, F);
+    PQB_CK(ctx, cudaGetLastError());
+    return PQB_OK;
+}
+
+int pqb_boys_rows_eval(pqb_ctx *ctx, int lt, int count, const double *T, double *F, void *stream)
+{
+    if (!ctx || lt < 0 || lt > 4 || count < 0 || !T || !F) return fail(ctx, PQB_E_ARG, "pqb_boys_rows_eval: bad arguments");
+    if (count == 0) return PQB_OK;
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    boys_rows_eval_kernel<<<(count + 127) / 128, 128, 0, (cudaStream_t)stream>>>(lt, count, T, F);
     PQB_CK(ctx, cudaGetLastError());
     return PQB_OK;
 }

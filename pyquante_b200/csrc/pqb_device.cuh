@@ -209,6 +209,92 @@ __device__ __forceinline__ void boys_rowm(double T, double *F)
     }
 }
 
+// Branch-free forms for the thread-mode kernels, whose lanes mix small and
+// large T: every lane evaluates the table polynomial (at a clamped row) and
+// the large-T form, then keeps one.  In the large-T form (T >= 40)
+//   F_0 = sqrt(pi/T)/2 = (sqrt(pi)/2) y, y = 1/sqrt(T), 1/(2T) = y^2/2,
+//   F_(m+1) = ((2m+1) F_m - exp(-T)) / (2T),
+// exp(-T) enters F_m at below 2e-12 of its value, so the hardware
+// single-precision 2^x estimate (ex2.approx, relative error < 2^-22; it is
+// 0 beyond T = 87, where the term is below 1e-30 of F_m) is exact enough.
+// T must be positive and below 1e36 (exponent sums times squared distances
+// of a molecule).
+__device__ __forceinline__ double rsqrt_nr_unchecked(double x)
+{
+    float yf;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"((float)x));
+    const double y = (double)yf;
+    const double e = fma(-x * y, y, 1.0);
+    return fma(y * e, fma(e, 0.375, 0.5), y);
+}
+
+__device__ __forceinline__ double exp_neg_estimate(double T)
+{
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"((float)T * -1.44269504088896341f));
+    return (double)r;
+}
+
+template <int NF>
+__device__ __forceinline__ void boys_row1_bf(double T, double *F)
+{
+    static_assert(NF == 1 || NF == 2, "F_0 or F_0, F_1");
+    const bool big = T >= PQB_BOYSROW_TMAX;
+    int k = __double2int_rn(T * PQB_BOYSROW_STEP_INV);
+    k = k < PQB_BOYSROW_NGRID - 1 ? k : PQB_BOYSROW_NGRID - 1;
+    const double d = k * (1.0 / PQB_BOYSROW_STEP_INV) - T;
+    const double *row = pqb_boys_row1 + 8 * k;
+    double c[8];
+    ld4(row, c[0], c[1], c[2], c[3]);
+    ld4(row + 4, c[4], c[5], c[6], c[7]);
+    double p = c[7], q = 0.0;
+#pragma unroll
+    for (int j = 6; j >= 0; --j) {
+        if (NF > 1) q = j == 6 ? p : fma(q, d, p);
+        p = fma(p, d, c[j]);
+    }
+    const double y = rsqrt_nr_unchecked(T);
+    const double a0 = 0.88622692545275801365 * y;
+    F[0] = big ? a0 : p;
+    if (NF > 1) F[1] = big ? a0 * (0.5 * y * y) : q;
+}
+
+template <int M>
+__device__ __forceinline__ void boys_rowm_bf(double T, double *F)
+{
+    static_assert(M == 3 || M == 4, "rows exist for M = 3 and 4");
+    const bool big = T >= PQB_BOYSROW_TMAX;
+    int k = __double2int_rn(T * PQB_BOYSROW_STEP_INV);
+    k = k < PQB_BOYSROW_NGRID - 1 ? k : PQB_BOYSROW_NGRID - 1;
+    const double d = k * (1.0 / PQB_BOYSROW_STEP_INV) - T;
+    const double *row = (M == 3 ? pqb_boys_row3 : pqb_boys_row4) + 8 * k;
+    double c[8];
+    ld4(row, c[0], c[1], c[2], c[3]);
+    ld4(row + 4, c[4], c[5], c[6], c[7]);
+    double f = c[6];
+#pragma unroll
+    for (int j = 5; j >= 0; --j) f = fma(f, d, c[j]);
+    double ed = 1.0 / 720.0;
+    ed = fma(ed, d, 1.0 / 120.0);
+    ed = fma(ed, d, 1.0 / 24.0);
+    ed = fma(ed, d, 1.0 / 6.0);
+    ed = fma(ed, d, 0.5);
+    ed = fma(ed, d, 1.0);
+    ed = fma(ed, d, 1.0);
+    const double y = rsqrt_nr_unchecked(T), h = 0.5 * y * y;
+    // small T: F_M from the row, downward recursion; large T: upward
+    const double e = big ? exp_neg_estimate(T) : c[7] * ed, t2 = 2.0 * T;
+    double Ft[M + 1], Fa[M + 1];
+    Ft[M] = f;
+#pragma unroll
+    for (int m = M - 1; m >= 0; --m) Ft[m] = fma(t2, Ft[m + 1], e) * (1.0 / (2 * m + 1));
+    Fa[0] = 0.88622692545275801365 * y;
+#pragma unroll
+    for (int m = 0; m < M; ++m) Fa[m + 1] = ((2 * m + 1) * Fa[m] - e) * h;
+#pragma unroll
+    for (int m = 0; m <= M; ++m) F[m] = big ? Fa[m] : Ft[m];
+}
+
 // F_m(T), m = 0..M for M = 1, 3 or 4 from the compact rows.
 template <int M>
 __device__ __forceinline__ void boys_row(double T, double *F)
@@ -233,6 +319,23 @@ __device__ __forceinline__ void boys_os(double T, double *F)
         for (int m = 0; m <= LT; ++m) F[m] = G[m];
     } else {
         boys_rowm<4>(T, F);
+    }
+}
+
+// The same, branch-free (boys_row1_bf, boys_rowm_bf).
+template <int LT>
+__device__ __forceinline__ void boys_os_bf(double T, double *F)
+{
+    static_assert(LT <= 4, "compact rows up to F_4");
+    if constexpr (LT <= 1) {
+        boys_row1_bf<LT + 1>(T, F);
+    } else if constexpr (LT <= 3) {
+        double G[4];
+        boys_rowm_bf<3>(T, G);
+#pragma unroll
+        for (int m = 0; m <= LT; ++m) F[m] = G[m];
+    } else {
+        boys_rowm_bf<4>(T, F);
     }
 }
 

@@ -49,6 +49,35 @@ def test_boys_device_matches_40_digit_values():
     assert abs(cints.Fgamma(0.5, 6.8) - 0.073447516533246701) < 1e-8
 
 
+def test_compact_row_boys_of_the_thread_kernels():
+    """The branch-free compact-row Boys form of the thread-mode kernels
+    (pqb_boys_rows_eval): F_m, m <= 4, against the 40-digit values, and
+    F_0..F_4 on a dense sweep of T (both sides of the table's end at T = 40,
+    where the exp(-T) estimate enters the large-T recursion) against the
+    general evaluation, 2e-14 relative."""
+    ctx = _lib.context()
+    g = json.load(open(os.path.join(GOLDEN, "boys.json")))
+    for m in (0, 1, 2, 4):
+        rows = [r for r in g["mpmath"] if r[0] == m]
+        T = torch.tensor([r[1] for r in rows], dtype=torch.float64, device="cuda")
+        F = torch.empty(len(rows) * (m + 1), dtype=torch.float64, device="cuda")
+        ctx.check(ctx.lib.pqb_boys_rows_eval(ctx.h, m, len(rows), _lib.ptr(T), _lib.ptr(F), _lib.stream_ptr()))
+        got = F.view(len(rows), m + 1)[:, m].cpu().numpy()
+        ref = np.array([r[2] for r in rows])
+        assert np.all(np.abs(got - ref) <= 2e-14 * np.abs(ref)), (m, got, ref)
+    T = torch.cat([torch.linspace(0.0, 45.0, 40001, dtype=torch.float64),
+                   torch.linspace(39.9, 40.1, 2001, dtype=torch.float64),
+                   torch.logspace(1.6, 6.0, 2001, dtype=torch.float64)]).cuda()
+    n = T.numel()
+    for lt in range(5):
+        Fr = torch.empty(n * (lt + 1), dtype=torch.float64, device="cuda")
+        Fg = torch.empty(n * (lt + 1), dtype=torch.float64, device="cuda")
+        ctx.check(ctx.lib.pqb_boys_rows_eval(ctx.h, lt, n, _lib.ptr(T), _lib.ptr(Fr), _lib.stream_ptr()))
+        ctx.check(ctx.lib.pqb_boys_eval(ctx.h, lt, n, _lib.ptr(T), _lib.ptr(Fg), _lib.stream_ptr()))
+        rel = ((Fr - Fg).abs() / Fg.abs()).max().item()
+        assert rel < 2e-14, (lt, rel)
+
+
 def test_rys_roots_weights_match_40_digit_values():
     ctx = _lib.context()
     g = np.load(os.path.join(GOLDEN, "rys.npz"))
