@@ -395,8 +395,8 @@ def run_h2o4_grad(a):
 def run_batch(a):
     """512 water clusters, k ~ U{1..12}, basis 50/50 STO-3G / 6-31G*: one
     batched mixed-precision SCF (DIIS, conv 1e-8 plus a commutator test,
-    densities by batched purification, CUDA-graph Fock build) vs a loop of
-    single solves over a random sample."""
+    densities by batched purification, each iteration one CUDA graph
+    replay) vs a loop of single solves over a random sample."""
     from pyquante_b200 import geometries
     from pyquante_b200.batch import batched_rhf
     from pyquante_b200.hartree_fock import rhf
@@ -427,7 +427,8 @@ def run_batch(a):
                    "scf_seconds": res["scf_seconds"], "setup_seconds": res["total_seconds"] - res["scf_seconds"],
                    "per_molecule_scf_s_p50": float(np.percentile(res["scf_times"], 50)),
                    "per_molecule_scf_s_p99": float(np.percentile(res["scf_times"], 99)),
-                   "cuda_graph": res["graph"], "plan": res["plan"],
+                   "cuda_graph": res["graph"], "whole_iteration_graph": res["whole_iteration_graph"],
+                   "plan": res["plan"],
                    "single_solve_loop": {"sample": len(pick), "molecules_per_s": len(pick) / st.sum(),
                                          "p50_s": float(np.percentile(st, 50)), "p99_s": float(np.percentile(st, 99)),
                                          "max_abs_dE_vs_batched": float(max(s[1] for s in single))}}}))

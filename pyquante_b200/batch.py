@@ -16,14 +16,16 @@ torch) runs on the blocks padded per size bucket:
 
 The molecules are grouped into at most 8 buckets of similar basis size
 for the dense work, so small molecules are not padded to the largest one.
-The Fock-build part of an iteration (densities, block gather/scatter, the
-multi-stream J/K launches, F and E of every bucket) is captured once in a
-CUDA graph and replayed; DIIS and the density update run eagerly per
-bucket, as batched GEMMs.  A molecule is converged when its energy changes
-by less than ``conv`` and its commutator FDS - SDF is below ``err_tol`` (its
+With the purification solver the whole iteration is captured once in a CUDA
+graph and replayed: the Fock build (densities, block gather/scatter, the
+multi-stream J/K launches, F and E of every bucket), DIIS (histories in
+fixed rings on the device, the DIIS equations by a batched Gauss-Jordan
+elimination), the purification (a fixed number of steps; converged states
+are frozen) and the convergence flags.  The host reads one flag per
+molecule per iteration.  A molecule is converged when its energy changes by
+less than ``conv`` and its commutator FDS - SDF is below ``err_tol`` (its
 SCF time is the time of that iteration); converged molecules keep their
-last solution, and from the next iteration on their DIIS step and density
-update are skipped.
+last density.
 """
 import ctypes
 import time
@@ -148,12 +150,15 @@ class _Bucket:
         e, V = torch.linalg.eigh(X.transpose(1, 2) @ Fm @ X + shift)
         return X @ V
 
-    def density(self, Fm, ia=None, tol=1e-13, maxit=200):
+    def density(self, Fm, ia=None, tol=1e-13, maxit=200, fixed=False):
         """Densities D = X P X^T of the Fock matrices Fm without an
         eigensolver: P, the projector on the nocc lowest states of
         F' = X^T F X, by the canonical purification of Palser and
         Manolopoulos (Phys. Rev. B 58, 12704 (1998)) -- batched GEMMs only.
-        Padded dimensions sit above the real spectrum and stay empty."""
+        Padded dimensions sit above the real spectrum and stay empty.
+        fixed: run exactly maxit steps with no host check (states that are
+        idempotent to rounding are kept), so that the loop can be captured
+        in a CUDA graph."""
         X = self.X if ia is None else self.X.index_select(0, ia)
         pad = self.pad if ia is None else self.pad.index_select(0, ia)
         nocc = self.occ.sum(1) if ia is None else self.occ.index_select(0, ia).sum(1)
@@ -178,7 +183,7 @@ class _Bucket:
             num = (P2 - P3).diagonal(dim1=1, dim2=2).sum(1)
             den = (P - P2).diagonal(dim1=1, dim2=2).sum(1)
             done = den.abs() < tol * nb          # idempotent to rounding: keep
-            if bool(done.all()):
+            if not fixed and bool(done.all()):
                 break
             c = torch.where(done, torch.full_like(num, 0.5), num / torch.where(done, torch.ones_like(den), den))
             c = c.clamp(0.0, 1.0)
@@ -190,15 +195,82 @@ class _Bucket:
         return X @ P @ X.transpose(1, 2)
 
 
+def _solve_small(A, b):
+    """x with A x = b for a batch of small systems (A: (B, n, n), b: (B, n)) by
+    Gauss-Jordan elimination with partial pivoting, in plain tensor
+    operations (no library solver, no host synchronisation), so that it can
+    be captured in a CUDA graph.  A singular system gives non-finite x."""
+    Bn, n = A.shape[0], A.shape[-1]
+    M = torch.cat([A, b[..., None]], dim=-1)
+    ar = torch.arange(n, device=A.device)[None, :]
+    for j in range(n):
+        col = M[:, :, j].abs()
+        col = torch.where(ar >= j, col, torch.full_like(col, -1.0))
+        p = col.argmax(1)[:, None]
+        perm = torch.where(ar == j, p, torch.where(ar == p, torch.full_like(p, j), ar))
+        M = M.gather(1, perm[:, :, None].expand(-1, -1, n + 1))
+        piv = M[:, j, :] / M[:, j, j:j + 1]
+        M = M - M[:, :, j:j + 1] * piv[:, None, :]
+        M[:, j, :] = piv
+    return M[:, :, n]
+
+
+class _Diis:
+    """Pulay DIIS of one bucket (Convergence.py:73-136, the same guarded
+    form as Convergence.DIIS: at most S vectors) on fixed device buffers: the
+    last S Fock matrices and commutators in rings, the slot and fill count
+    as device scalars, so that a step has static shapes and no host
+    synchronisation."""
+
+    def __init__(self, bk, S):
+        B, nb = len(bk.idx), bk.nb
+        dev = bk.S.device
+        self.S = S
+        self.F = torch.zeros((B, S, nb, nb), dtype=torch.float64, device=dev)
+        self.E = torch.zeros((B, S, nb * nb), dtype=torch.float64, device=dev)
+        self.slot = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.nfill = torch.zeros((), dtype=torch.int64, device=dev)
+        self.ar = torch.arange(S, device=dev)
+        self.eye = torch.eye(S, dtype=torch.float64, device=dev)
+
+    def step(self, F, err):
+        """Store (F, err) and return the extrapolated Fock matrices."""
+        B, S = F.shape[0], self.S
+        self.F.index_copy_(1, self.slot, F[:, None])
+        self.E.index_copy_(1, self.slot, err.reshape(B, 1, -1))
+        newest = (self.ar == self.slot).to(torch.float64)[None, :].expand(B, S)
+        self.nfill.copy_(torch.clamp(self.nfill + 1, max=S))
+        self.slot.copy_((self.slot + 1) % S)
+        filled = self.ar < self.nfill
+        G = self.E @ self.E.transpose(1, 2)
+        scale = torch.where(filled[None, :], G.diagonal(dim1=1, dim2=2), torch.zeros_like(newest))
+        scale = scale.abs().amax(1).clamp(min=1e-300)
+        fm = filled[:, None] & filled[None, :]
+        G = torch.where(fm[None], G / scale[:, None, None], self.eye[None])
+        fcol = -filled.to(torch.float64)
+        A = torch.zeros((B, S + 1, S + 1), dtype=torch.float64, device=F.device)
+        A[:, :S, :S] = G
+        A[:, :S, S] = fcol
+        A[:, S, :S] = fcol
+        rhs = torch.zeros((B, S + 1), dtype=torch.float64, device=F.device)
+        rhs[:, S] = -1.0
+        c = _solve_small(A, rhs)[:, :S]
+        ok = torch.isfinite(c).all(1, keepdim=True)
+        c = torch.where(ok, c, newest)
+        return torch.einsum("bs,bsij->bij", c, self.F)
+
+
 def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, graph=True, schwarz=1e-12,
-                fp32_threshold=1e-5, device=None, max_buckets=8, solver="purify", err_tol=1e-6):
+                fp32_threshold=1e-5, device=None, max_buckets=8, solver="purify", err_tol=1e-6, purify_steps=48):
     """Solve RHF for every (molecule, basis) in ``systems`` together.
 
     The Fock build of every iteration is one engine call for all molecules;
     the dense FP64 algebra runs per size bucket (molecules padded to the
     bucket's largest basis).  ``solver='purify'`` (default) gets each new
     density from the DIIS Fock matrix by batched canonical purification
-    (GEMMs only, no per-molecule eigensolver); ``'eigh'`` diagonalises.
+    (GEMMs only, ``purify_steps`` steps, no per-molecule eigensolver), and
+    with ``graph=True`` the whole iteration is one CUDA graph replay;
+    ``'eigh'`` diagonalises (then only the Fock build is captured).
     A molecule is converged when its energy changes by less than ``conv``
     and its commutator max|FDS - SDF| is below ``err_tol``.  Returns a
     dict: energies, iterations, per-molecule SCF times (s), total time (s),
@@ -218,19 +290,28 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
         S_list.append(Sb)
         h_list.append(Tb + Vb)
     buckets = [_Bucket(idx, eng, S_list, h_list, dev) for idx in _bucket_edges(np.array(eng.n), max_buckets)]
-    def new_density(bk, Fm, ia=None):
+
+    def new_density(bk, Fm):
         if solver == "purify":
-            return bk.density(Fm, ia)
-        C = bk.solve(Fm, ia)
-        occ = bk.occ if ia is None else bk.occ.index_select(0, ia)
-        Co = C * occ[:, None, :]
+            return bk.density(Fm, maxit=purify_steps, fixed=True)
+        C = bk.solve(Fm)
+        Co = C * bk.occ[:, None, :]
         return Co @ Co.transpose(1, 2)
 
     for bk in buckets:
-        bk.D.copy_(new_density(bk, bk.h))
+        # core guess (outside the loop: purification to idempotency)
+        bk.D.copy_(bk.density(bk.h) if solver == "purify" else new_density(bk, bk.h))
+        bk.diis = _Diis(bk, diis_size)
+        bk.eold = torch.zeros(len(bk.idx), **f64)
+        bk.bdone = torch.zeros(len(bk.idx), dtype=torch.bool, device=dev)
+        bk.conv_it = torch.full((len(bk.idx),), -1, dtype=torch.int64, device=dev)
     Dflat = torch.zeros(eng.dense_len, **f64)
     Jf = torch.zeros_like(Dflat)
     Kf = torch.zeros_like(Dflat)
+    it_dev = torch.zeros((), dtype=torch.int64, device=dev)
+    # per molecule (in input order): converged flag and energy, gathered on the device
+    all_idx = torch.cat([torch.as_tensor(bk.idx, device=dev) for bk in buckets])
+    flags = torch.zeros(B, dtype=torch.bool, device=dev)
 
     def fock_build():
         for bk in buckets:
@@ -242,82 +323,82 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
             bk.F.copy_(bk.h + 2.0 * bk.J - bk.K)
             bk.E.copy_((bk.D * bk.h).sum(dim=(1, 2)) + (bk.D * bk.F).sum(dim=(1, 2)) + bk.enuc)
 
-    fock_build()                       # warm-up (kernel attributes, allocator)
+    def update():
+        """DIIS, new densities and convergence flags of every bucket (static
+        shapes; converged molecules keep their density)."""
+        for bk in buckets:
+            err = bk.F @ bk.D @ bk.S - bk.S @ bk.D @ bk.F
+            err = torch.where(bk.padmask, torch.zeros_like(err), err)
+            Fd = bk.diis.step(bk.F, err)
+            emax = err.abs().amax(dim=(1, 2))
+            Dn = new_density(bk, Fd)
+            bk.D.copy_(torch.where(bk.bdone[:, None, None], bk.D, Dn))
+            newly = (~bk.bdone) & ((bk.E - bk.eold).abs() < conv) & (emax < err_tol)
+            bk.eold.copy_(torch.where(bk.bdone, bk.eold, bk.E))
+            bk.conv_it.copy_(torch.where(newly, it_dev, bk.conv_it))
+            bk.bdone.copy_(bk.bdone | newly)
+        flags.index_copy_(0, all_idx, torch.cat([bk.bdone for bk in buckets]))
+        it_dev.add_(1)
+
+    def iteration():
+        fock_build()
+        update()
+
+    # warm-up of the kernels' attributes and the allocator, then the state is reset
+    snapshot = [bk.D.clone() for bk in buckets]
+    iteration()
     torch.cuda.synchronize()
+    whole = graph and solver == "purify"
     g = None
     if graph:
+        body = iteration if whole else fock_build
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
-            fock_build()
+            body()
         torch.cuda.current_stream().wait_stream(s)
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
-            fock_build()
-    energies = np.zeros(B)
-    iters = np.zeros(B, dtype=np.int64)
-    done = np.zeros(B, dtype=bool)
-    times = np.zeros(B)
-    eold = [torch.zeros(len(bk.idx), **f64) for bk in buckets]
-    bdone = [torch.zeros(len(bk.idx), dtype=torch.bool, device=dev) for bk in buckets]
+            body()
+    for bk, D0 in zip(buckets, snapshot):
+        bk.D.copy_(D0)
+        bk.diis.F.zero_()
+        bk.diis.E.zero_()
+        bk.diis.slot.zero_()
+        bk.diis.nfill.zero_()
+        bk.eold.zero_()
+        bk.bdone.zero_()
+        bk.conv_it.fill_(-1)
+    it_dev.zero_()
+    flags.zero_()
+    torch.cuda.synchronize()
+    iter_time = []
     t0 = time.perf_counter()
     for it in range(maxiter):
         if g is not None:
             g.replay()
+            if not whole:
+                update()
         else:
-            fock_build()
-        for q, bk in enumerate(buckets):
-            nb, Bb = bk.nb, len(bk.idx)
-            # molecules converged in earlier iterations keep their orbitals: the
-            # eigensolves (one per molecule) run for the others only
-            act = ~done[bk.idx]
-            if not act.any():
-                continue
-            err = bk.F @ bk.D @ bk.S - bk.S @ bk.D @ bk.F
-            err = torch.where(bk.padmask, torch.zeros_like(err), err)
-            bk.Fs.append(bk.F.clone())
-            bk.Es.append(err.reshape(Bb, -1))
-            if len(bk.Fs) > diis_size:
-                bk.Fs.pop(0)
-                bk.Es.pop(0)
-            k = len(bk.Fs)
-            Em = torch.stack(bk.Es, dim=1)
-            A = torch.zeros((Bb, k + 1, k + 1), **f64)
-            A[:, :k, :k] = Em @ Em.transpose(1, 2)
-            scale = A[:, :k, :k].diagonal(dim1=1, dim2=2).abs().amax(dim=1).clamp(min=1e-300)
-            A[:, :k, :k] /= scale[:, None, None]
-            A[:, :k, k] = -1.0
-            A[:, k, :k] = -1.0
-            rhs = torch.zeros((Bb, k + 1), **f64)
-            rhs[:, k] = -1.0
-            c, info = torch.linalg.solve_ex(A, rhs)
-            c = torch.where((info == 0)[:, None], c, torch.nn.functional.one_hot(
-                torch.full((Bb,), k - 1, device=dev), k + 1).to(torch.float64))
-            Fd = (c[:, :k, None, None] * torch.stack(bk.Fs, dim=1)).sum(dim=1)
-            emax = err.abs().amax(dim=(1, 2))
-            energy = bk.E.clone()
-            if act.all():
-                bk.D.copy_(new_density(bk, Fd))
-            else:
-                ia = torch.from_numpy(np.nonzero(act)[0]).to(dev)
-                bk.D.index_copy_(0, ia, new_density(bk, Fd.index_select(0, ia), ia))
-            newly = (~bdone[q]) & ((energy - eold[q]).abs() < conv) & (emax < err_tol)
-            eold[q] = torch.where(bdone[q], eold[q], energy)
-            bdone[q] = bdone[q] | newly
-        flags = [(bd.cpu().numpy(), e.cpu().numpy()) for bd, e in zip(bdone, eold)]
-        now = time.perf_counter() - t0
-        for bk, (bd, e) in zip(buckets, flags):
-            fresh = bd & ~done[bk.idx]
-            times[bk.idx[fresh]] = now
-            iters[bk.idx[~done[bk.idx]]] = it + 1
-            done[bk.idx] = bd
-            energies[bk.idx] = e
+            iteration()
+        done = flags.cpu().numpy()
+        iter_time.append(time.perf_counter() - t0)
         if done.all():
             break
     torch.cuda.synchronize()
     t_end = time.perf_counter()
-    times[times == 0] = t_end - t0
+    energies = np.zeros(B)
+    iters = np.zeros(B, dtype=np.int64)
+    times = np.zeros(B)
+    done = np.zeros(B, dtype=bool)
+    for bk in buckets:
+        ci = bk.conv_it.cpu().numpy()
+        ok = ci >= 0
+        energies[bk.idx] = bk.eold.cpu().numpy()
+        done[bk.idx] = ok
+        iters[bk.idx] = np.where(ok, ci + 1, len(iter_time))
+        times[bk.idx] = np.where(ok, [iter_time[c] if c >= 0 else 0.0 for c in ci], t_end - t0)
     return dict(energies=energies, iterations=iters, converged=done, scf_times=times, scf_seconds=t_end - t0,
                 total_seconds=t_end - t_start, plan=counts, nbf=np.array(eng.n), graph=g is not None,
-                buckets=[bk.nb for bk in buckets])
+                whole_iteration_graph=whole and g is not None, buckets=[bk.nb for bk in buckets])
