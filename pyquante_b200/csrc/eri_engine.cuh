@@ -691,7 +691,7 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
                 const double T = zeta * eta * izpe * (PQx * PQx + PQy * PQy + PQz * PQz);
                 const double pre = P.K * Q.K * rs;
                 double F[LT + 1];
-                boys_os_bf<LT>(T, F);
+                boys_os<LT>(T, F);
                 R Fs[LT + 1];
 #pragma unroll
                 for (int m = 0; m <= LT; ++m) Fs[m] = (R)(F[m] * pre);

@@ -1031,18 +1031,18 @@ __global__ void boys_eval_kernel(int m, int count, const double *T, double *F)
 }
 
 // F_0 .. F_lt by the branch-free compact-row form of the thread-mode kernels
-// (boys_os_bf)
+// (boys_os)
 __global__ void boys_rows_eval_kernel(int lt, int count, const double *T, double *F)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     double f[5];
     switch (lt) {
-    case 0: boys_os_bf<0>(T[t], f); break;
-    case 1: boys_os_bf<1>(T[t], f); break;
-    case 2: boys_os_bf<2>(T[t], f); break;
-    case 3: boys_os_bf<3>(T[t], f); break;
-    default: boys_os_bf<4>(T[t], f); break;
+    case 0: boys_os<0>(T[t], f); break;
+    case 1: boys_os<1>(T[t], f); break;
+    case 2: boys_os<2>(T[t], f); break;
+    case 3: boys_os<3>(T[t], f); break;
+    default: boys_os<4>(T[t], f); break;
     }
     for (int k = 0; k <= lt; ++k) F[(int64_t)t * (lt + 1) + k] = f[k];
 }

@@ -18,6 +18,7 @@
 #endif
 #include "rys_tables.inc"
 #include "boys_rows.inc"
+#include "boys_top.inc"
 
 namespace pqb {
 
@@ -137,88 +138,29 @@ __device__ __forceinline__ void ld4(const double *p, double &a, double &b, doubl
         : "l"(__cvta_generic_to_global(p)));
 }
 
-// F_0 (NF = 1) or F_0, F_1 (NF = 2) from one 64-byte row of pqb_boys_row1
-// (boys_rows.inc: c_j = F_j(T_k)/j!, j = 0..7, T_k = k/32): with
-// d = T_k - T (|d| <= 1/64), F_0(T) = P(d) = sum_j c_j d^j and
-// F_1(T) = -dF_0/dT = P'(d), both by one Horner pass (truncation below
-// 5e-17 relative); no exp(-T).  For T >= PQB_BOYSROW_TMAX:
-// F_0 = sqrt(pi/T)/2 and F_1 = F_0/(2T), the exp(-T) term of F_1 being below
-// 3e-17 of it there.
-template <int NF>
-__device__ __forceinline__ void boys_row1(double T, double *F)
-{
-    static_assert(NF == 1 || NF == 2, "F_0 or F_0, F_1");
-    if (T < PQB_BOYSROW_TMAX) {
-        const int k = __double2int_rn(T * PQB_BOYSROW_STEP_INV);
-        const double d = k * (1.0 / PQB_BOYSROW_STEP_INV) - T;
-        const double *row = pqb_boys_row1 + 8 * k;
-        double c[8];
-        ld4(row, c[0], c[1], c[2], c[3]);
-        ld4(row + 4, c[4], c[5], c[6], c[7]);
-        double p = c[7], q = 0.0;
-#pragma unroll
-        for (int j = 6; j >= 0; --j) {
-            if (NF > 1) q = j == 6 ? p : fma(q, d, p);
-            p = fma(p, d, c[j]);
-        }
-        F[0] = p;
-        if (NF > 1) F[1] = q;
-    } else {
-        F[0] = 0.88622692545275801365 * rsqrt_nr(T);   // sqrt(pi)/2 / sqrt(T)
-        if (NF > 1) F[1] = F[0] * (0.5 * rcp_nr(T));
-    }
-}
-
-// F_m(T), m = 0..M for M = 3 or 4, from one 64-byte row of pqb_boys_rowM
-// (c_j = F_(M+j)(T_k)/j!, j = 0..6, and exp(-T_k)): F_M by Horner in
-// d = T_k - T, exp(-T) = exp(-T_k) exp(d) with a 7-term series (both below
-// 5e-17 relative for |d| <= 1/64), then the downward recursion
-// F_m = (2T F_(m+1) + exp(-T))/(2m+1).  T >= PQB_BOYSROW_TMAX: the large-T
-// forms F_0 = sqrt(pi/T)/2, F_(m+1) = ((2m+1) F_m - exp(-T))/(2T).
-template <int M>
-__device__ __forceinline__ void boys_rowm(double T, double *F)
-{
-    static_assert(M == 3 || M == 4, "rows exist for M = 3 and 4");
-    if (T < PQB_BOYSROW_TMAX) {
-        const int k = __double2int_rn(T * PQB_BOYSROW_STEP_INV);
-        const double d = k * (1.0 / PQB_BOYSROW_STEP_INV) - T;
-        const double *row = (M == 3 ? pqb_boys_row3 : pqb_boys_row4) + 8 * k;
-        double c[8];
-        ld4(row, c[0], c[1], c[2], c[3]);
-        ld4(row + 4, c[4], c[5], c[6], c[7]);
-        double f = c[6];
-#pragma unroll
-        for (int j = 5; j >= 0; --j) f = fma(f, d, c[j]);
-        F[M] = f;
-        double ed = 1.0 / 720.0;
-        ed = fma(ed, d, 1.0 / 120.0);
-        ed = fma(ed, d, 1.0 / 24.0);
-        ed = fma(ed, d, 1.0 / 6.0);
-        ed = fma(ed, d, 0.5);
-        ed = fma(ed, d, 1.0);
-        ed = fma(ed, d, 1.0);
-        const double e = c[7] * ed, t2 = 2.0 * T;
-#pragma unroll
-        for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * (1.0 / (2 * m + 1));
-    } else {
-        const double it = rcp_nr(T);
-        F[0] = 0.88622692545275801365 * rsqrt_nr(T);
-        const double e = exp(-T), h = 0.5 * it;
-#pragma unroll
-        for (int m = 0; m < M; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
-    }
-}
-
-// Branch-free forms for the thread-mode kernels, whose lanes mix small and
-// large T: every lane evaluates the table polynomial (at a clamped row) and
-// the large-T form, then keeps one.  In the large-T form (T >= 40)
-//   F_0 = sqrt(pi/T)/2 = (sqrt(pi)/2) y, y = 1/sqrt(T), 1/(2T) = y^2/2,
-//   F_(m+1) = ((2m+1) F_m - exp(-T)) / (2T),
-// exp(-T) enters F_m at below 2e-12 of its value, so the hardware
-// single-precision 2^x estimate (ex2.approx, relative error < 2^-22; it is
-// 0 beyond T = 87, where the term is below 1e-30 of F_m) is exact enough.
-// T must be positive and below 1e36 (exponent sums times squared distances
-// of a molecule).
+// ------------------------------------------ Boys for the Fock-build kernels --
+// F_m(T), m <= 4, from the 16-byte rows {F_top(T_k), exp(-T_k)} of
+// boys_top.inc (T_k = k/32, 40-digit values; top = 7 and 10), branch-free
+// because the lanes of a warp mix small and large T.
+//   T < PQB_BOYSROW_TMAX (40): k = round(32 T), d = T_k - T (|d| <= 1/64);
+//     F_j(T_k) for j < top by the downward recursion at T_k,
+//     F_j = (2 T_k F_(j+1) + exp(-T_k)) / (2j+1), which keeps or shrinks the
+//     relative error of every step; then the Taylor series in d
+//     (dF_m/dT = -F_(m+1)), written as nested products
+//     sum_j f_j d^j / j! = f_0 + d (f_1 + d/2 (f_2 + ...)):
+//       M <= 1: F_0 = P(d) = sum_(j<=7) F_j(T_k) d^j/j! and F_1 = P'(d);
+//       M = 3, 4: F_M from F_M .. F_(M+6) at T_k, exp(-T) = exp(-T_k) e^d (7
+//       terms), then F_m = (2T F_(m+1) + exp(-T))/(2m+1) downward;
+//     truncation below 5e-17 relative.
+//   T >= 40: F_0 = sqrt(pi/T)/2 = (sqrt(pi)/2) y with y = 1/sqrt(T) and
+//     F_(m+1) = ((2m+1) F_m - exp(-T)) y^2/2.  exp(-T) enters F_m at below
+//     2e-12 of its value there, so the hardware single-precision 2^x
+//     estimate (ex2.approx, relative error < 2^-22; 0 beyond T = 87, where
+//     the term is below 1e-30 of F_m) is exact enough.
+// Every lane evaluates both forms (the table row index is clamped) and keeps
+// one.  T must be non-negative and below 1e36 (exponent sums times squared
+// distances of a molecule).  Against the 40-digit values: below 2e-15
+// relative.
 __device__ __forceinline__ double rsqrt_nr_unchecked(double x)
 {
     float yf;
@@ -235,23 +177,33 @@ __device__ __forceinline__ double exp_neg_estimate(double T)
     return (double)r;
 }
 
+// Two doubles from 16-byte aligned global memory with one 128-bit load.
+__device__ __forceinline__ void ld2(const double *p, double &a, double &b)
+{
+    asm("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(a), "=d"(b) : "l"(__cvta_generic_to_global(p)));
+}
+
 template <int NF>
-__device__ __forceinline__ void boys_row1_bf(double T, double *F)
+__device__ __forceinline__ void boys_row1(double T, double *F)
 {
     static_assert(NF == 1 || NF == 2, "F_0 or F_0, F_1");
     const bool big = T >= PQB_BOYSROW_TMAX;
     int k = __double2int_rn(T * PQB_BOYSROW_STEP_INV);
     k = k < PQB_BOYSROW_NGRID - 1 ? k : PQB_BOYSROW_NGRID - 1;
-    const double d = k * (1.0 / PQB_BOYSROW_STEP_INV) - T;
-    const double *row = pqb_boys_row1 + 8 * k;
-    double c[8];
-    ld4(row, c[0], c[1], c[2], c[3]);
-    ld4(row + 4, c[4], c[5], c[6], c[7]);
-    double p = c[7], q = 0.0;
+    const double Tk = k * (1.0 / PQB_BOYSROW_STEP_INV), d = Tk - T, t2 = 2.0 * Tk;
+    double f[8], ek;
+    ld2(pqb_boys_top7 + 2 * k, f[7], ek);
 #pragma unroll
-    for (int j = 6; j >= 0; --j) {
-        if (NF > 1) q = j == 6 ? p : fma(q, d, p);
-        p = fma(p, d, c[j]);
+    for (int j = 6; j >= 0; --j) f[j] = fma(t2, f[j + 1], ek) * (1.0 / (2 * j + 1));
+    double dj[7];
+#pragma unroll
+    for (int j = 0; j < 7; ++j) dj[j] = d * (1.0 / (j + 1));
+    double p = f[7], q = f[7];
+#pragma unroll
+    for (int j = 6; j >= 0; --j) p = fma(p, dj[j], f[j]);
+    if (NF > 1) {
+#pragma unroll
+        for (int j = 5; j >= 0; --j) q = fma(q, dj[j], f[j + 1]);
     }
     const double y = rsqrt_nr_unchecked(T);
     const double a0 = 0.88622692545275801365 * y;
@@ -260,20 +212,20 @@ __device__ __forceinline__ void boys_row1_bf(double T, double *F)
 }
 
 template <int M>
-__device__ __forceinline__ void boys_rowm_bf(double T, double *F)
+__device__ __forceinline__ void boys_rowm(double T, double *F)
 {
-    static_assert(M == 3 || M == 4, "rows exist for M = 3 and 4");
+    static_assert(M == 3 || M == 4, "F_M .. F_(M+6) from F_10");
     const bool big = T >= PQB_BOYSROW_TMAX;
     int k = __double2int_rn(T * PQB_BOYSROW_STEP_INV);
     k = k < PQB_BOYSROW_NGRID - 1 ? k : PQB_BOYSROW_NGRID - 1;
-    const double d = k * (1.0 / PQB_BOYSROW_STEP_INV) - T;
-    const double *row = (M == 3 ? pqb_boys_row3 : pqb_boys_row4) + 8 * k;
-    double c[8];
-    ld4(row, c[0], c[1], c[2], c[3]);
-    ld4(row + 4, c[4], c[5], c[6], c[7]);
-    double f = c[6];
+    const double Tk = k * (1.0 / PQB_BOYSROW_STEP_INV), d = Tk - T, tk2 = 2.0 * Tk;
+    double f[11], ek;
+    ld2(pqb_boys_top10 + 2 * k, f[10], ek);
 #pragma unroll
-    for (int j = 5; j >= 0; --j) f = fma(f, d, c[j]);
+    for (int j = 9; j >= M; --j) f[j] = fma(tk2, f[j + 1], ek) * (1.0 / (2 * j + 1));
+    double p = f[M + 6];
+#pragma unroll
+    for (int j = 5; j >= 0; --j) p = fma(p, d * (1.0 / (j + 1)), f[M + j]);
     double ed = 1.0 / 720.0;
     ed = fma(ed, d, 1.0 / 120.0);
     ed = fma(ed, d, 1.0 / 24.0);
@@ -282,10 +234,9 @@ __device__ __forceinline__ void boys_rowm_bf(double T, double *F)
     ed = fma(ed, d, 1.0);
     ed = fma(ed, d, 1.0);
     const double y = rsqrt_nr_unchecked(T), h = 0.5 * y * y;
-    // small T: F_M from the row, downward recursion; large T: upward
-    const double e = big ? exp_neg_estimate(T) : c[7] * ed, t2 = 2.0 * T;
+    const double e = big ? exp_neg_estimate(T) : ek * ed, t2 = 2.0 * T;
     double Ft[M + 1], Fa[M + 1];
-    Ft[M] = f;
+    Ft[M] = p;
 #pragma unroll
     for (int m = M - 1; m >= 0; --m) Ft[m] = fma(t2, Ft[m + 1], e) * (1.0 / (2 * m + 1));
     Fa[0] = 0.88622692545275801365 * y;
@@ -295,7 +246,7 @@ __device__ __forceinline__ void boys_rowm_bf(double T, double *F)
     for (int m = 0; m <= M; ++m) F[m] = big ? Fa[m] : Ft[m];
 }
 
-// F_m(T), m = 0..M for M = 1, 3 or 4 from the compact rows.
+// F_m(T), m = 0..M for M = 1, 3 or 4.
 template <int M>
 __device__ __forceinline__ void boys_row(double T, double *F)
 {
@@ -309,7 +260,7 @@ __device__ __forceinline__ void boys_row(double T, double *F)
 template <int LT>
 __device__ __forceinline__ void boys_os(double T, double *F)
 {
-    static_assert(LT <= 4, "compact rows up to F_4");
+    static_assert(LT <= 4, "up to F_4");
     if constexpr (LT <= 1) {
         boys_row1<LT + 1>(T, F);
     } else if constexpr (LT <= 3) {
@@ -319,23 +270,6 @@ __device__ __forceinline__ void boys_os(double T, double *F)
         for (int m = 0; m <= LT; ++m) F[m] = G[m];
     } else {
         boys_rowm<4>(T, F);
-    }
-}
-
-// The same, branch-free (boys_row1_bf, boys_rowm_bf).
-template <int LT>
-__device__ __forceinline__ void boys_os_bf(double T, double *F)
-{
-    static_assert(LT <= 4, "compact rows up to F_4");
-    if constexpr (LT <= 1) {
-        boys_row1_bf<LT + 1>(T, F);
-    } else if constexpr (LT <= 3) {
-        double G[4];
-        boys_rowm_bf<3>(T, G);
-#pragma unroll
-        for (int m = 0; m <= LT; ++m) F[m] = G[m];
-    } else {
-        boys_rowm_bf<4>(T, F);
     }
 }
 

@@ -5,9 +5,15 @@ kernels; cross-checked against ncu's executed dfma/dadd/dmul counts.
 
 Obara--Saika classes (LA+LB+LC+LD = LT <= 4, csrc/os_classes.inc):
   setup     PQ, zeta+eta, 1/sqrt (Newton step), 1/(zeta+eta), T, prefactor: 24
-  Boys      LT <= 1: grid index and offset 3, Horner 14 (+12 for F_1);
-            LT 2, 3: 3 + F_3 Horner 12 + exp series 12 + 2 + recursion 3 x 3 = 38;
-            LT 4:    the same with four recursion steps = 41
+  Boys      counted at the cost of a Taylor evaluation from stored
+            coefficients: LT <= 1: grid index and offset 3, Horner 14 (+12 for
+            F_1); LT 2, 3: 3 + F_3 Horner 12 + exp series 12 + 2 + recursion
+            3 x 3 = 38; LT 4: the same with four recursion steps = 41.  The
+            kernels store only {F_top(T_k), exp(-T_k)} per grid point and
+            rebuild the coefficients by a downward recursion (about 40 more
+            FP64 operations per primitive quartet, in exchange for 48 fewer
+            table bytes per lane); that recursion is not counted as
+            algorithmic work, so ncu's executed count exceeds this model
   prefactor (LT+1) products
   VRR       the emitted vertical recurrence and the coefficients it reads
             (PA, QC, WP, WQ components, rho/zeta, rho/eta, the 1/(2x) factors;
