@@ -3,8 +3,7 @@
 Writes ``rys_tables.inc`` next to this file.  Run once (takes ~1 min):
 
     python -m pyquante_b200.csrc.gen_tables              # rys_tables.inc
-    python -m pyquante_b200.csrc.gen_tables --boys-rows  # boys_rows.inc (FP32 rows)
-    python -m pyquante_b200.csrc.gen_tables --boys-top   # boys_top.inc (FP64 16-byte rows)
+    python -m pyquante_b200.csrc.gen_tables --boys-top   # boys_top.inc
 
 Two tables are produced, both from 40-digit mpmath arithmetic:
 
@@ -217,47 +216,14 @@ def main():
     print("worst relative error:", worst)
 
 
-# Compact single-precision Boys rows for the FP32 lists of the mixed mode,
-# one 32-byte row per grid point T_k = k/32 (k = 0..BOYSROW_NGRID-1), Taylor
-# coefficients already divided by j! so the device evaluates plain Horner
-# polynomials in d = T_k - T (|d| <= 1/64; F_m(T_k - d) =
-# sum_j F_(m+j)(T_k) d^j / j! since dF_m/dT = -F_(m+1)):
-#   pqb_boys_row1_f32:  c_j = F_j(T_k)/j!, j = 0..4 (F_0 = P(d), F_1 = P'(d));
-#   pqb_boys_rowM_f32, M = 3, 4:  c_j = F_(M+j)(T_k)/j!, j = 0..3, then
-#                       exp(-T_k) (4-term series: 3e-9 relative at |d| <= 1/64).
-# The FP64 kernels use the 16-byte rows of boys_top.inc (below) on the same
-# grid.
+# Grid of the compact Boys rows of the Fock-build kernels: T_k = k/32,
+# k = 0..BOYSROW_NGRID-1, up to BOYS_TMAX (large-T forms beyond).
 BOYSROW_STEP_INV = 32
-BOYSROW_ORDERS = (1, 3, 4)
 BOYSROW_NGRID = int(BOYS_TMAX * BOYSROW_STEP_INV) + 2
 
 
-def main_boys_rows():
-    here = os.path.dirname(os.path.abspath(__file__))
-    lines = ["// Generated by gen_tables.py --boys-rows -- do not edit.",
-             "// Row k at T_k = k/%d (40-digit mpmath), single precision: pqb_boys_row1_f32 holds"
-             % BOYSROW_STEP_INV,
-             "// F_j(T_k)/j!, j = 0..4; pqb_boys_rowM_f32 (M = 3, 4) F_(M+j)(T_k)/j!, j = 0..3, then exp(-T_k).",
-             "#pragma once",
-             "#define PQB_BOYSROW_STEP_INV %d" % BOYSROW_STEP_INV,
-             "#define PQB_BOYSROW_NGRID %d" % BOYSROW_NGRID,
-             "#define PQB_BOYSROW_TMAX %.1f" % BOYS_TMAX]
-    for M in BOYSROW_ORDERS:
-        lines.append("PQB_TABQ __align__(64) float pqb_boys_row%d_f32[PQB_BOYSROW_NGRID * 8] = {" % M)
-        for k in range(BOYSROW_NGRID):
-            T = mp.mpf(k) / BOYSROW_STEP_INV
-            if M == 1:
-                vals = [boys(j, T) / mp.factorial(j) for j in range(5)] + [0, 0, 0]
-            else:
-                vals = [boys(M + j, T) / mp.factorial(j) for j in range(4)] + [mp.exp(-T), 0, 0, 0]
-            lines.append("  " + ", ".join("%.9ef" % float(v) for v in vals) + ",")
-        lines.append("};")
-    with open(os.path.join(here, "boys_rows.inc"), "w") as f:
-        f.write("\n".join(lines) + "\n")
-
-
 # 16-byte Boys rows: {F_top(T_k), exp(-T_k)} at T_k = k/32 for top = 7 and
-# 10.  The device rebuilds F_j(T_k), j < top, by the downward recursion
+# 10 (and an 8-byte single-precision copy for top = 7).  The device rebuilds F_j(T_k), j < top, by the downward recursion
 # F_j = (2 T_k F_(j+1) + exp(-T_k)) / (2j+1) (stable: each step keeps or
 # shrinks the relative error) and then sums the same Taylor series in
 # d = T_k - T as with the 64-byte rows, from a table a quarter of the size.
@@ -267,24 +233,31 @@ BOYSTOP_ORDERS = (7, 10)
 def main_boys_top():
     here = os.path.dirname(os.path.abspath(__file__))
     lines = ["// Generated by gen_tables.py --boys-top -- do not edit.",
-             "// Row k at T_k = k/%d (40-digit mpmath): {F_top(T_k), exp(-T_k)}, top = 7 and 10."
+             "// Row k at T_k = k/%d (40-digit mpmath): {F_top(T_k), exp(-T_k)}, top = 7 and 10; FP32 copy for top = 7."
              % BOYSROW_STEP_INV,
-             "#pragma once"]
+             "#pragma once",
+             "#define PQB_BOYSROW_STEP_INV %d" % BOYSROW_STEP_INV,
+             "#define PQB_BOYSROW_NGRID %d" % BOYSROW_NGRID,
+             "#define PQB_BOYSROW_TMAX %.1f" % BOYS_TMAX]
     for top in BOYSTOP_ORDERS:
         lines.append("PQB_TABQ __align__(16) double pqb_boys_top%d[PQB_BOYSROW_NGRID * 2] = {" % top)
         for k in range(BOYSROW_NGRID):
             T = mp.mpf(k) / BOYSROW_STEP_INV
             lines.append("  %.17e, %.17e," % (float(boys(top, T)), float(mp.exp(-T))))
         lines.append("};")
+    # single precision, top = 7, for the FP32 lists of the mixed mode
+    lines.append("PQB_TABQ __align__(8) float pqb_boys_top7_f32[PQB_BOYSROW_NGRID * 2] = {")
+    for k in range(BOYSROW_NGRID):
+        T = mp.mpf(k) / BOYSROW_STEP_INV
+        lines.append("  %.9ef, %.9ef," % (float(boys(7, T)), float(mp.exp(-T))))
+    lines.append("};")
     with open(os.path.join(here, "boys_top.inc"), "w") as f:
         f.write("\n".join(lines) + "\n")
 
 
 if __name__ == "__main__":
     import sys
-    if "--boys-rows" in sys.argv:
-        main_boys_rows()
-    elif "--boys-top" in sys.argv:
+    if "--boys-top" in sys.argv:
         main_boys_top()
     else:
         main()

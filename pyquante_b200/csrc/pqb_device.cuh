@@ -17,7 +17,6 @@
 #define PQB_CTABQ static __constant__ const
 #endif
 #include "rys_tables.inc"
-#include "boys_rows.inc"
 #include "boys_top.inc"
 
 namespace pqb {
@@ -275,8 +274,7 @@ __device__ __forceinline__ void boys_os(double T, double *F)
 
 // ------------------------------------------------ single precision (mixed) --
 // The FP32 kernels of the mixed mode evaluate the Boys function and the Rys
-// rules in single precision for T < PQB_BOYSROW_TMAX; larger arguments use
-// the FP64 asymptotic forms, rounded to single precision afterwards.
+// rules in single precision.
 
 // Eight floats from 32-byte aligned global memory with one 256-bit load.
 __device__ __forceinline__ void ld8f(const float *p, float *r)
@@ -286,85 +284,64 @@ __device__ __forceinline__ void ld8f(const float *p, float *r)
         : "l"(__cvta_generic_to_global(p)));
 }
 
-// Single-precision rows (T < PQB_BOYSROW_TMAX): row1_f32 holds
-// c_j = F_j(T_k)/j!, j = 0..4 (F_0 = P(d), F_1 = P'(d)); rowM_f32 (M = 3, 4)
-// holds F_(M+j)(T_k)/j!, j = 0..3, and exp(-T_k) (4-term series, 3e-9
-// relative at |d| <= 1/64), then the downward recursion.
-template <int NF>
-__device__ __forceinline__ void boys_row1_f32(float T, float *F)
+// F_0 .. F_LT in single precision for the Obara--Saika classes, from the
+// 8-byte rows {F_7(T_k), exp(-T_k)} (pqb_boys_top7_f32), branch-free like
+// boys_os: F_j(T_k) by the downward recursion, Taylor
+// series of degree 4 (F_0, F_1) or 3 (F_M, M = 3, 4) and a 4-term e^d, then
+// the downward recursion at T; for T >= 40 the large-T forms in single
+// precision (rsqrtf; exp(-T) from ex2.approx).  Truncation below 2e-9
+// relative.
+__device__ __forceinline__ void ld2f(const float *p, float &a, float &b)
 {
-    const int k = __float2int_rn(T * PQB_BOYSROW_STEP_INV);
-    const float d = k * (1.0f / PQB_BOYSROW_STEP_INV) - T;   // -(T - T_k)
-    float c[8];
-    ld8f(pqb_boys_row1_f32 + 8 * k, c);
-    float p = c[4], q = 0.0f;
-#pragma unroll
-    for (int j = 3; j >= 0; --j) {
-        if (NF > 1) q = j == 3 ? p : fmaf(q, d, p);
-        p = fmaf(p, d, c[j]);
-    }
-    F[0] = p;
-    if (NF > 1) F[1] = q;
+    asm("ld.global.nc.v2.f32 {%0, %1}, [%2];" : "=f"(a), "=f"(b) : "l"(__cvta_generic_to_global(p)));
 }
 
-template <int M>
-__device__ __forceinline__ void boys_rowm_f32(float T, float *F)
-{
-    static_assert(M == 3 || M == 4, "rows exist for M = 3 and 4");
-    const int k = __float2int_rn(T * PQB_BOYSROW_STEP_INV);
-    const float d = k * (1.0f / PQB_BOYSROW_STEP_INV) - T;   // -(T - T_k)
-    float r[8];
-    ld8f((M == 3 ? pqb_boys_row3_f32 : pqb_boys_row4_f32) + 8 * k, r);
-    float f = r[3];
-    f = fmaf(f, d, r[2]);
-    f = fmaf(f, d, r[1]);
-    f = fmaf(f, d, r[0]);
-    F[M] = f;
-    float ed = fmaf(d, 1.0f / 6.0f, 0.5f);
-    ed = fmaf(ed, d, 1.0f);
-    ed = fmaf(ed, d, 1.0f);
-    const float e = r[4] * ed, t2 = 2.0f * T;
-#pragma unroll
-    for (int m = M - 1; m >= 0; --m) F[m] = fmaf(t2, F[m + 1], e) * (1.0f / (2 * m + 1));
-}
-
-template <int M>
-__device__ __forceinline__ void boys_row_f32(float T, float *F)
-{
-    if constexpr (M == 1)
-        boys_row1_f32<2>(T, F);
-    else
-        boys_rowm_f32<M>(T, F);
-}
-
-// F_0 .. F_LT in single precision for the Obara--Saika classes; above the
-// rows the large-T forms (in FP64, rounded afterwards).
 template <int LT>
 __device__ __forceinline__ void boys_os_f32(float T, float *F)
 {
-    static_assert(LT <= 4, "compact rows up to F_4");
-    if (T >= (float)PQB_BOYSROW_TMAX) {
-        const double Td = (double)T, it = rcp_nr(Td);
-        double G[LT + 1];
-        G[0] = 0.88622692545275801365 * rsqrt_nr(Td);
-        if (LT > 0) {
-            const double e = LT > 1 ? exp(-Td) : 0.0, h = 0.5 * it;
-#pragma unroll
-            for (int m = 0; m < LT; ++m) G[m + 1] = ((2 * m + 1) * G[m] - e) * h;
-        }
-#pragma unroll
-        for (int m = 0; m <= LT; ++m) F[m] = (float)G[m];
-        return;
-    }
+    static_assert(LT <= 4, "up to F_4");
+    const bool big = T >= (float)PQB_BOYSROW_TMAX;
+    int k = __float2int_rn(T * PQB_BOYSROW_STEP_INV);
+    k = k < PQB_BOYSROW_NGRID - 1 ? k : PQB_BOYSROW_NGRID - 1;
+    const float Tk = k * (1.0f / PQB_BOYSROW_STEP_INV), d = Tk - T, tk2 = 2.0f * Tk;
+    float f[8], ek;
+    ld2f(pqb_boys_top7_f32 + 2 * k, f[7], ek);
+    const float y = rsqrtf(T), h = 0.5f * y * y, a0 = 0.886226925f * y;
     if constexpr (LT <= 1) {
-        boys_row1_f32<LT + 1>(T, F);
-    } else if constexpr (LT <= 3) {
-        float G[4];
-        boys_rowm_f32<3>(T, G);
 #pragma unroll
-        for (int m = 0; m <= LT; ++m) F[m] = G[m];
+        for (int j = 6; j >= 0; --j) f[j] = fmaf(tk2, f[j + 1], ek) * (1.0f / (2 * j + 1));
+        float dj[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dj[j] = d * (1.0f / (j + 1));
+        float p = f[4], q = f[4];
+#pragma unroll
+        for (int j = 3; j >= 0; --j) p = fmaf(p, dj[j], f[j]);
+#pragma unroll
+        for (int j = 2; j >= 0; --j) q = fmaf(q, dj[j], f[j + 1]);
+        F[0] = big ? a0 : p;
+        if (LT == 1) F[1] = big ? a0 * h : q;
     } else {
-        boys_rowm_f32<4>(T, F);
+        constexpr int M = LT <= 3 ? 3 : 4;
+#pragma unroll
+        for (int j = 6; j >= M; --j) f[j] = fmaf(tk2, f[j + 1], ek) * (1.0f / (2 * j + 1));
+        float p = f[M + 3];
+#pragma unroll
+        for (int j = 2; j >= 0; --j) p = fmaf(p, d * (1.0f / (j + 1)), f[M + j]);
+        float ed = fmaf(d, 1.0f / 6.0f, 0.5f);
+        ed = fmaf(ed, d, 1.0f);
+        ed = fmaf(ed, d, 1.0f);
+        float ebig;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(ebig) : "f"(T * -1.44269504f));
+        const float e = big ? ebig : ek * ed, t2 = 2.0f * T;
+        float Ft[M + 1], Fa[M + 1];
+        Ft[M] = p;
+#pragma unroll
+        for (int m = M - 1; m >= 0; --m) Ft[m] = fmaf(t2, Ft[m + 1], e) * (1.0f / (2 * m + 1));
+        Fa[0] = a0;
+#pragma unroll
+        for (int m = 0; m < M; ++m) Fa[m + 1] = ((2 * m + 1) * Fa[m] - e) * h;
+#pragma unroll
+        for (int m = 0; m <= LT; ++m) F[m] = big ? Fa[m] : Ft[m];
     }
 }
 
@@ -433,12 +410,12 @@ __device__ __forceinline__ void rys_roots_f32(float T, float *u, float *w)
     }
     if constexpr (NR == 1) {
         float F[2];
-        boys_row_f32<1>(T, F);
+        boys_os_f32<1>(T, F);
         w[0] = F[0];
         u[0] = __fdividef(F[1], F[0]);
     } else if constexpr (NR == 2) {
         float F[4];
-        boys_row_f32<3>(T, F);
+        boys_os_f32<3>(T, F);
         const float id = __fdividef(1.0f, fmaf(F[0], F[2], -F[1] * F[1]));
         const float a1 = fmaf(F[1], F[2], -F[0] * F[3]) * id, a0 = fmaf(F[1], F[3], -F[2] * F[2]) * id;
         const float disc = fmaf(a1, a1, -4.0f * a0), rs = rsqrtf(disc);
