@@ -79,6 +79,15 @@ int pqb_shells_upload_batch(pqb_ctx *ctx, int nmol, const int *mol_shell_off, in
                             const int *shell_nprim, const int *prim_off, const int *shell_f0, const double *shell_xyz,
                             const double *prim_exp, const double *prim_coef, int nbf, const double *fscale);
 int pqb_dense_len(const pqb_ctx *ctx, int64_t *len);
+/* Batched basis: a device array of nmol ints; the direct builds
+ * (pqb_jk_direct, pqb_jk_direct2) skip the work items of molecules m with
+ * mask[m] == 0, whose J and K blocks then come out zero (a batched SCF stops
+ * building molecules that have converged).  NULL (the default) builds every
+ * molecule.  The array stays owned by the caller and must outlive every
+ * build, including builds the caller captured in a CUDA graph; its contents
+ * may change between builds.  No counterpart in the reference (one molecule
+ * per SCF). */
+int pqb_set_molecule_mask(pqb_ctx *ctx, const int *mask);
 
 /* Schwarz factors Q_ab = sqrt(max |(ab|ab)|) for every shell pair, computed
  * on the device; copied to Q_host (length npairs) when it is not NULL. */

@@ -25,7 +25,8 @@ are frozen) and the convergence flags.  The host reads one flag per
 molecule per iteration.  A molecule is converged when its energy changes by
 less than ``conv`` and its commutator FDS - SDF is below ``err_tol`` (its
 SCF time is the time of that iteration); converged molecules keep their
-last density.
+last density, and from the next iteration on the Fock build skips their
+quartets (a per-molecule mask read by the kernels).
 """
 import ctypes
 import time
@@ -83,6 +84,13 @@ class BatchEngine:
         self.ctx.check(self.ctx.lib.pqb_plan(self.ctx.h, schwarz, fp32_threshold, c))
         self.plan_counts = dict(shell_quartets=c[0], fp64=c[1], fp32=c[2], dropped=c[3])
         return self.plan_counts
+
+    def set_mask(self, mask):
+        """Build only the molecules m with mask[m] != 0 (a device int32
+        tensor of one entry per molecule, kept alive by the caller), or every
+        molecule (None)."""
+        self._mask = mask
+        self.ctx.check(self.ctx.lib.pqb_set_molecule_mask(self.ctx.h, None if mask is None else _lib.ptr(mask)))
 
     def jk(self, Dflat, J, K, mode):
         m = _lib.PQB_MIXED if mode == "mixed" else _lib.PQB_FP64
@@ -312,6 +320,9 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
     # per molecule (in input order): converged flag and energy, gathered on the device
     all_idx = torch.cat([torch.as_tensor(bk.idx, device=dev) for bk in buckets])
     flags = torch.zeros(B, dtype=torch.bool, device=dev)
+    # molecules still iterating: the Fock build skips the others' quartets
+    active = torch.ones(B, dtype=torch.int32, device=dev)
+    eng.set_mask(active)
 
     def fock_build():
         for bk in buckets:
@@ -338,6 +349,7 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
             bk.conv_it.copy_(torch.where(newly, it_dev, bk.conv_it))
             bk.bdone.copy_(bk.bdone | newly)
         flags.index_copy_(0, all_idx, torch.cat([bk.bdone for bk in buckets]))
+        active.copy_((~flags).to(torch.int32))
         it_dev.add_(1)
 
     def iteration():
@@ -372,6 +384,7 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
         bk.conv_it.fill_(-1)
     it_dev.zero_()
     flags.zero_()
+    active.fill_(1)
     torch.cuda.synchronize()
     iter_time = []
     t0 = time.perf_counter()

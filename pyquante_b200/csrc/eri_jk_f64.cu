@@ -4,10 +4,11 @@
 
 namespace pqb {
 cudaError_t launch_jk_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
-                          const double *Dscaled, double *Jacc, double *Kacc, int n, cudaStream_t st, int nsm)
+                          const double *Dscaled, double *Jacc, double *Kacc, int n, cudaStream_t st, int nsm,
+                          const int *molmask)
 {
     (void)n;
-    EpiJK epi{{Dscaled}, {Jacc}, {Kacc}, {nullptr}};
+    EpiJK epi{{Dscaled}, {Jacc}, {Kacc}, {nullptr}, molmask};
     return launch_eri<double>(qc, list, nq, pairs, prims, epi, st, nsm);
 }
 }  // namespace pqb

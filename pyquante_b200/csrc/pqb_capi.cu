@@ -98,6 +98,7 @@ struct pqb_ctx {
     bool graph_warm[6] = {false, false, false, false, false, false};   // one eager build first (one-time launch setup stays out of the capture)
     double *d_Jacc = nullptr, *d_Kacc = nullptr;
     double *d_Jacc2 = nullptr, *d_Kacc2 = nullptr;   // second density's graph accumulators
+    const int *d_molmask = nullptr;  // caller-owned per-molecule mask of the direct builds (batched bases)
     // small scratch
     double *d_atoms = nullptr;
     size_t atoms_cap = 0;
@@ -1403,6 +1404,7 @@ static int shells_upload_batch_impl(pqb_ctx *ctx, int nmol, const int *mol_shell
             pi.cls = pair_class(pi.la, pi.lb);
             const int m = shell_mol[a];
             pi.nm = ctx->mol_n[m];
+            pi.mol = m;
             pi.bo = ctx->mol_off[m] - (long long)ctx->mol_f0[m] * (ctx->mol_n[m] + 1);
             pairs.push_back(pi);
         }
@@ -1815,6 +1817,7 @@ static int launch_build(pqb_ctx *ctx, int nden, double *const Jacc[2], double *c
     }
     const double *Ds[2] = {ctx->d_Dscaled, ctx->d_Dscaled2};
     const float *Dsf[2] = {ctx->d_Dscaled_f, ctx->d_Dscaled2_f};
+    const int *mm = ctx->d_molmask;
     // fork: class launches spread over the context's streams, heaviest first
     PQB_CK(ctx, cudaEventRecord(ctx->ev_fork, st));
     for (int k = 0; k < pqb_ctx::kStreams; ++k) PQB_CK(ctx, cudaStreamWaitEvent(ctx->streams[k], ctx->ev_fork, 0));
@@ -1842,20 +1845,22 @@ static int launch_build(pqb_ctx *ctx, int nden, double *const Jacc[2], double *c
         const bool f32 = part == 1 && mode == PQB_MIXED;
         if (jonly) {
             if (f32)
-                PQB_CK(ctx, launch_j_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds[0], Dsf[0], Jacc[0], sk, ctx->nsm));
+                PQB_CK(ctx, launch_j_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds[0], Dsf[0], Jacc[0], sk, ctx->nsm,
+                                         mm));
             else
-                PQB_CK(ctx, launch_j_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds[0], Jacc[0], sk, ctx->nsm));
+                PQB_CK(ctx, launch_j_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds[0], Jacc[0], sk, ctx->nsm, mm));
         } else if (nden == 2) {
             if (f32)
-                PQB_CK(ctx, launch_jk2_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, Dsf, Jacc, Kacc, sk, ctx->nsm));
+                PQB_CK(ctx, launch_jk2_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, Dsf, Jacc, Kacc, sk, ctx->nsm,
+                                           mm));
             else
-                PQB_CK(ctx, launch_jk2_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, Jacc, Kacc, sk, ctx->nsm));
+                PQB_CK(ctx, launch_jk2_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds, Jacc, Kacc, sk, ctx->nsm, mm));
         } else if (f32) {
             PQB_CK(ctx, launch_jk_f32(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds[0], Dsf[0], Jacc[0], Kacc[0], n, sk,
-                                      ctx->nsm));
+                                      ctx->nsm, mm));
         } else {
             PQB_CK(ctx, launch_jk_f64(c, list, nq, ctx->d_pairs, ctx->d_prims, Ds[0], Jacc[0], Kacc[0], n, sk,
-                                      ctx->nsm));
+                                      ctx->nsm, mm));
         }
     }
     // join
@@ -1996,6 +2001,14 @@ int pqb_jk_direct2(pqb_ctx *ctx, const double *Da, const double *Db, double *Ja,
     const double *Dv[2] = {Da, Db};
     double *Jv[2] = {Ja, Jb}, *Kv[2] = {Ka, Kb};
     return jk_direct_impl(ctx, 2, Dv, Jv, Kv, mode, stream);
+}
+
+int pqb_set_molecule_mask(pqb_ctx *ctx, const int *mask)
+{
+    if (!ctx) return PQB_E_ARG;
+    ctx->d_molmask = mask;
+    drop_graphs(ctx);   // a captured build holds the old pointer
+    return PQB_OK;
 }
 
 int pqb_dense_len(const pqb_ctx *ctx, int64_t *len)

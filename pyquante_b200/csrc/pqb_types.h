@@ -23,6 +23,7 @@ struct PairInfo {
     int cls;           // pair class: index of (La, Lb) in ss ps pp ds dp dd
     int la, lb;
     int nm;            // functions of the pair's molecule (batched bases; else nbf)
+    int mol;           // the pair's molecule (batched bases; else 0)
     long long bo;      // D/J/K element (i, j) of the molecule is at bo + i*nm + j
                        // (global function indices; 0 for a single molecule)
 };

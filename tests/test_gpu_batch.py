@@ -42,6 +42,42 @@ def test_batched_jk_blocks_equal_single_molecule_jk():
         assert float((Kb - Ks).abs().max()) < 1e-10
 
 
+def test_molecule_mask_skips_masked_molecules():
+    """pqb_set_molecule_mask: the masked molecules' J and K blocks come out
+    zero and the others' equal the unmasked build (FP64 and mixed, with the
+    mask changed between builds and cleared again)."""
+    systems = _systems()
+    beng = BatchEngine(systems)
+    beng.plan(schwarz=1e-12, fp32_threshold=1e-5)
+    rng = np.random.default_rng(1)
+    Ds = []
+    for n in beng.n:
+        C = rng.standard_normal((n, max(1, n // 3))) * 0.3
+        Ds.append(C @ C.T)
+    Dflat = torch.tensor(np.concatenate([d.reshape(-1) for d in Ds]), dtype=torch.float64, device="cuda")
+    for mode in ("fp64", "mixed"):
+        J0, K0 = torch.zeros_like(Dflat), torch.zeros_like(Dflat)
+        beng.jk(Dflat, J0, K0, mode)
+        for keep in ([1, 0, 1, 0, 1], [0, 1, 0, 1, 1], [0, 0, 0, 0, 0]):
+            mask = torch.tensor(keep, dtype=torch.int32, device="cuda")
+            beng.set_mask(mask)
+            J, K = torch.zeros_like(Dflat), torch.zeros_like(Dflat)
+            beng.jk(Dflat, J, K, mode)
+            for b, (n, off) in enumerate(zip(beng.n, beng.block_off)):
+                sl = slice(int(off), int(off) + n * n)
+                if keep[b]:
+                    assert float((J[sl] - J0[sl]).abs().max()) < 1e-12 * float(J0[sl].abs().max())
+                    assert float((K[sl] - K0[sl]).abs().max()) < 1e-12 * float(K0[sl].abs().max())
+                else:
+                    assert float(J[sl].abs().max()) == 0.0 and float(K[sl].abs().max()) == 0.0
+        beng.set_mask(None)
+        J, K = torch.zeros_like(Dflat), torch.zeros_like(Dflat)
+        beng.jk(Dflat, J, K, mode)
+        # (the same sums; the FP64 atomics add them in another order)
+        assert float((J - J0).abs().max()) < 1e-12 * float(J0.abs().max())
+        assert float((K - K0).abs().max()) < 1e-12 * float(K0.abs().max())
+
+
 @pytest.mark.parametrize("graph,solver", [(True, "purify"), (False, "purify"), (True, "eigh")])
 def test_batched_rhf_matches_single_solves(graph, solver):
     """Densities by batched canonical purification (no eigensolver) or by
