@@ -68,6 +68,67 @@ def geigh(H, A, **opts):
 GHeigenvectors = geigh   # the older name BASELINE/README use
 
 
+def purify(Fp, nocc, pad=None, tol=1e-13, maxit=200, fixed=False, check=1):
+    """P, the projector on the nocc lowest eigenstates of each symmetric
+    Fp (a batch (B, n, n) of CUDA tensors; nocc per matrix), without an
+    eigensolver: the canonical purification of Palser and Manolopoulos
+    (Phys. Rev. B 58, 12704 (1998)), GEMMs only.
+      P_0 = (lambda/n)(mu - Fp) + nocc/n, mu = tr(Fp)/n, lambda from the
+      Gershgorin bounds of Fp;
+      c = tr(P^2 - P^3)/tr(P - P^2);  P <- ((1+c)P^2 - P^3)/c for c >= 1/2,
+      else ((1-2c)P + (1+c)P^2 - P^3)/(1-c).
+    pad (B, n) marks padded dimensions (batched bases), which are held above
+    the real spectrum and stay empty.  The iteration stops when every P is
+    idempotent to rounding (|tr(P - P^2)| < tol n), tested on the host every
+    ``check`` steps (converged matrices are kept meanwhile); fixed=True runs exactly
+    maxit steps with no host check instead (converged matrices are kept),
+    so that the loop can be captured in a CUDA graph."""
+    Fp = 0.5 * (Fp + Fp.transpose(1, 2))
+    nb = Fp.shape[-1]
+    nocc = torch.as_tensor(nocc, dtype=Fp.dtype, device=Fp.device).reshape(-1)
+    radius = Fp.abs().sum(-1) - Fp.diagonal(dim1=1, dim2=2).abs()
+    d = Fp.diagonal(dim1=1, dim2=2)
+    if pad is None:
+        pad = torch.zeros_like(d, dtype=torch.bool)
+    hi = torch.where(pad, torch.full_like(d, -1e300), d + radius).amax(1)
+    lo = torch.where(pad, torch.full_like(d, 1e300), d - radius).amin(1)
+    top = hi + 1.0
+    Fp = Fp + torch.diag_embed(pad.to(Fp.dtype) * (top[:, None] - d))
+    hi = torch.maximum(hi, top)
+    mu = Fp.diagonal(dim1=1, dim2=2).sum(1) / nb
+    lam = torch.minimum(nocc / (hi - mu), (nb - nocc) / (mu - lo))
+    eye = torch.eye(nb, dtype=Fp.dtype, device=Fp.device)
+    P = (lam / nb)[:, None, None] * (mu[:, None, None] * eye - Fp) + (nocc / nb)[:, None, None] * eye
+    for step in range(maxit):
+        P2 = P @ P
+        P3 = P2 @ P
+        num = (P2 - P3).diagonal(dim1=1, dim2=2).sum(1)
+        den = (P - P2).diagonal(dim1=1, dim2=2).sum(1)
+        done = den.abs() < tol * nb          # idempotent to rounding: keep
+        if not fixed and step % check == check - 1 and bool(done.all()):
+            break
+        c = torch.where(done, torch.full_like(num, 0.5), num / torch.where(done, torch.ones_like(den), den))
+        c = c.clamp(0.0, 1.0)
+        hi_branch = ((1 + c)[:, None, None] * P2 - P3) / c.clamp(min=1e-300)[:, None, None]
+        lo_branch = ((1 - 2 * c)[:, None, None] * P + (1 + c)[:, None, None] * P2 - P3) / \
+            (1 - c).clamp(min=1e-300)[:, None, None]
+        Pn = torch.where((c >= 0.5)[:, None, None], hi_branch, lo_branch)
+        P = torch.where(done[:, None, None], P, Pn)
+    return P
+
+
+def purify_density(F, X, nocc, **opts):
+    """The closed-shell density D = C_occ C_occ^T (mkdens) of the Fock
+    matrix F, for the orthogonalising transform X (CholOrth), by purify
+    instead of the eigenvectors: D = X P X^T, P the projector on the nocc
+    lowest states of X^T F X.  Batched or single (n, n) CUDA tensors."""
+    single = F.dim() == 2
+    Fb, Xb = (F[None], X[None]) if single else (F, X)
+    P = purify(Xb.transpose(1, 2) @ Fb @ Xb, nocc, **opts)
+    D = Xb @ P @ Xb.transpose(1, 2)
+    return D[0] if single else D
+
+
 def mkdens(c, nstart, nstop):
     """D = C[:, nstart:nstop] C[:, nstart:nstop]^T (no factor 2, LA2.py:127-131)."""
     d = c[:, nstart:nstop]

@@ -37,6 +37,7 @@ import torch
 from . import _lib, autotune
 from .Basis.basis import BasisSet
 from .engine import FunctionTable, detect_shells, oneint
+from .LA2 import purify
 
 PAD_SHIFT = 1.0e6   # padded orbital energies, sorted above every real one
 
@@ -170,36 +171,7 @@ class _Bucket:
         X = self.X if ia is None else self.X.index_select(0, ia)
         pad = self.pad if ia is None else self.pad.index_select(0, ia)
         nocc = self.occ.sum(1) if ia is None else self.occ.index_select(0, ia).sum(1)
-        Fp = X.transpose(1, 2) @ Fm @ X
-        Fp = 0.5 * (Fp + Fp.transpose(1, 2))
-        nb = Fp.shape[-1]
-        # Gershgorin bounds of the real block; padded states just above them
-        radius = Fp.abs().sum(-1) - Fp.diagonal(dim1=1, dim2=2).abs()
-        d = Fp.diagonal(dim1=1, dim2=2)
-        hi = torch.where(pad, torch.full_like(d, -1e300), d + radius).amax(1)
-        lo = torch.where(pad, torch.full_like(d, 1e300), d - radius).amin(1)
-        top = hi + 1.0
-        Fp = Fp + torch.diag_embed(pad.to(Fp.dtype) * (top[:, None] - d))
-        hi = torch.maximum(hi, top)
-        mu = Fp.diagonal(dim1=1, dim2=2).sum(1) / nb
-        lam = torch.minimum(nocc / (hi - mu), (nb - nocc) / (mu - lo))
-        eye = torch.eye(nb, dtype=Fp.dtype, device=Fp.device)
-        P = (lam / nb)[:, None, None] * (mu[:, None, None] * eye - Fp) + (nocc / nb)[:, None, None] * eye
-        for _ in range(maxit):
-            P2 = P @ P
-            P3 = P2 @ P
-            num = (P2 - P3).diagonal(dim1=1, dim2=2).sum(1)
-            den = (P - P2).diagonal(dim1=1, dim2=2).sum(1)
-            done = den.abs() < tol * nb          # idempotent to rounding: keep
-            if not fixed and bool(done.all()):
-                break
-            c = torch.where(done, torch.full_like(num, 0.5), num / torch.where(done, torch.ones_like(den), den))
-            c = c.clamp(0.0, 1.0)
-            hi_branch = ((1 + c)[:, None, None] * P2 - P3) / c.clamp(min=1e-300)[:, None, None]
-            lo_branch = ((1 - 2 * c)[:, None, None] * P + (1 + c)[:, None, None] * P2 - P3) / \
-                (1 - c).clamp(min=1e-300)[:, None, None]
-            Pn = torch.where((c >= 0.5)[:, None, None], hi_branch, lo_branch)
-            P = torch.where(done[:, None, None], P, Pn)
+        P = purify(X.transpose(1, 2) @ Fm @ X, nocc, pad=pad, tol=tol, maxit=maxit, fixed=fixed)
         return X @ P @ X.transpose(1, 2)
 
 

@@ -4,7 +4,10 @@ MaxIter 20, DoAveraging False), same energy expression
 E = tr(D h) + tr(D F) + E_nuc with D = C_occ C_occ^T, Fock builds through
 ``Ints.get2JmK``.  Extra options: ``integrals`` as in the reference,
 ``direct=True`` / ``precision`` / ``schwarz`` / ``fp32_threshold`` forwarded
-to ``getints``, and ``device=True`` to keep the SCF loop on the GPU."""
+to ``getints``, ``device=True`` to keep the SCF loop on the GPU, and (rhf)
+``solver='purify'``: each iteration's density from the Fock matrix by
+canonical purification on the GPU (GEMMs, no eigensolver; implies
+device=True), one eigensolve at the end for the returned orbitals."""
 import logging
 
 import numpy as np
@@ -12,7 +15,7 @@ import torch
 
 from .Convergence import DIIS
 from .Ints import get2JmK, getbasis, getints, getJ, getJK2, getK  # noqa: F401  (getJ/getK re-exported)
-from .LA2 import geigh, mkdens, trace2
+from .LA2 import CholOrth, geigh, mkdens, purify_density, trace2
 
 logger = logging.getLogger("pyquante")
 
@@ -58,28 +61,42 @@ def rhf(atoms, **opts):
     nclosed, nopen = atoms.get_closedopen()
     if nopen != 0:
         raise ValueError("SCF currently only works for closed-shell systems")
+    solver = opts.get("solver", "eigh")
+    if solver not in ("eigh", "purify"):
+        raise ValueError("solver must be 'eigh' or 'purify'")
+    if solver == "purify":
+        opts = dict(opts, device=True)
     bfs, S, h, Ints = _setup(atoms, opts)
     orbs = opts.get("orbs")
     if orbs is None:
         orbe, orbs = geigh(h, S)
     elif isinstance(S, torch.Tensor):
         orbs = torch.as_tensor(np.asarray(orbs), dtype=torch.float64, device=S.device)
+    X = CholOrth(S) if solver == "purify" else None
     enuke = atoms.get_enuke()
     eold = 0.0
     avg = DIIS(S) if DoAveraging else None
     energy = 0.0
+    D = mkdens(orbs, 0, nclosed)
+    F = None
     for it in range(MaxIter):
-        D = mkdens(orbs, 0, nclosed)
         G = get2JmK(Ints, D)
         F = h + G
         if avg is not None:
             F = avg.getF(F, D)
-        orbe, orbs = geigh(F, S)
+        if solver == "purify":
+            Dn = purify_density(F, X, nclosed, check=4)
+        else:
+            orbe, orbs = geigh(F, S)
+            Dn = mkdens(orbs, 0, nclosed)
         energy = get_energy(h, F, D, enuke)
         logger.debug("%d %f", it, energy)
+        D = Dn
         if abs(energy - eold) < ConvCriteria:
             break
         eold = energy
+    if solver == "purify" and F is not None:
+        orbe, orbs = geigh(F, S)
     if isinstance(orbs, torch.Tensor):
         orbe, orbs = orbe.cpu().numpy(), orbs.cpu().numpy()
     return energy, orbe, orbs

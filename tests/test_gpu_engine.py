@@ -384,6 +384,20 @@ def test_rhf_water_sto3g_energy():
     assert abs(E2 - e["water_sto3g"]) < E_TOL
 
 
+def test_rhf_purification_solver_matches_eigensolver():
+    """rhf(solver='purify'): the SCF loop on the GPU with densities by
+    canonical purification gives the eigensolver loop's energy (1e-9 Eh)
+    and, from its final eigensolve, the same orbital energies (1e-7)."""
+    mol = geometries.water_cluster(2, seed=4)
+    bs = BasisSet(mol, "6-31g**")
+    kw = dict(bfs=bs, ConvCriteria=1e-10, MaxIter=80, DoAveraging=True, direct=True)
+    e0, orbe0, _ = rhf(mol, **kw)
+    e1, orbe1, orbs1 = rhf(mol, solver="purify", **kw)
+    assert abs(e1 - e0) < 1e-9
+    assert np.abs(np.asarray(orbe1) - np.asarray(orbe0)).max() < 1e-7
+    assert isinstance(orbs1, np.ndarray) and orbs1.shape == (len(bs), len(bs))
+
+
 def test_rhf_reference_unit_test_energies():
     """The reference's own SCF unit tests: He and Ne / 6-31G** (Tests/he.py:16
     to 1e-7, Tests/ne.py:13 to 1e-4, rhf defaults) and H2 / STO-3G, 6-31G**
