@@ -89,6 +89,17 @@ int pqb_dense_len(const pqb_ctx *ctx, int64_t *len);
  * per SCF). */
 int pqb_set_molecule_mask(pqb_ctx *ctx, const int *mask);
 
+/* One step of canonical purification (Palser and Manolopoulos) for nmat
+ * row-major n x n device matrices back to back: from P, P2 = P P and
+ * P3 = P2 P, with c = tr(P2 - P3)/tr(P - P2) clamped to [0, 1],
+ *   P_out = ((1+c) P2 - P3)/c  (c >= 1/2),  ((1-2c) P + (1+c) P2 - P3)/(1-c)  (else);
+ * a matrix with |tr(P - P2)| < tol n is copied unchanged and done[m] = 1
+ * (done may be NULL).  P_out may be P; it must not overlap P2 or P3.  The
+ * batched and device SCF loops get their densities from this step (GEMMs
+ * only, no eigensolver); no counterpart in the reference. */
+int pqb_purify_step(int nmat, int n, const double *P, const double *P2, const double *P3, double *P_out, int *done,
+                    double tol, void *stream);
+
 /* Schwarz factors Q_ab = sqrt(max |(ab|ab)|) for every shell pair, computed
  * on the device; copied to Q_host (length npairs) when it is not NULL. */
 int pqb_schwarz(pqb_ctx *ctx, double *Q_host, void *stream);

@@ -82,7 +82,10 @@ def purify(Fp, nocc, pad=None, tol=1e-13, maxit=200, fixed=False, check=1):
     idempotent to rounding (|tr(P - P^2)| < tol n), tested on the host every
     ``check`` steps (converged matrices are kept meanwhile); fixed=True runs exactly
     maxit steps with no host check instead (converged matrices are kept),
-    so that the loop can be captured in a CUDA graph."""
+    so that the loop can be captured in a CUDA graph.  Each step is two
+    batched GEMMs and one fused trace-and-update kernel (pqb_purify_step)."""
+    from . import _lib
+    lib = _lib.load()
     Fp = 0.5 * (Fp + Fp.transpose(1, 2))
     nb = Fp.shape[-1]
     nocc = torch.as_tensor(nocc, dtype=Fp.dtype, device=Fp.device).reshape(-1)
@@ -98,22 +101,19 @@ def purify(Fp, nocc, pad=None, tol=1e-13, maxit=200, fixed=False, check=1):
     mu = Fp.diagonal(dim1=1, dim2=2).sum(1) / nb
     lam = torch.minimum(nocc / (hi - mu), (nb - nocc) / (mu - lo))
     eye = torch.eye(nb, dtype=Fp.dtype, device=Fp.device)
-    P = (lam / nb)[:, None, None] * (mu[:, None, None] * eye - Fp) + (nocc / nb)[:, None, None] * eye
+    P = ((lam / nb)[:, None, None] * (mu[:, None, None] * eye - Fp) + (nocc / nb)[:, None, None] * eye).contiguous()
+    P2 = torch.empty_like(P)
+    P3 = torch.empty_like(P)
+    done = torch.zeros(P.shape[0], dtype=torch.int32, device=P.device)
     for step in range(maxit):
-        P2 = P @ P
-        P3 = P2 @ P
-        num = (P2 - P3).diagonal(dim1=1, dim2=2).sum(1)
-        den = (P - P2).diagonal(dim1=1, dim2=2).sum(1)
-        done = den.abs() < tol * nb          # idempotent to rounding: keep
+        torch.bmm(P, P, out=P2)
+        torch.bmm(P2, P, out=P3)
+        rc = lib.pqb_purify_step(P.shape[0], nb, _lib.ptr(P), _lib.ptr(P2), _lib.ptr(P3), _lib.ptr(P), _lib.ptr(done),
+                                 float(tol), _lib.stream_ptr())
+        if rc != _lib.PQB_OK:
+            raise _lib.EngineError(rc, "pqb_purify_step")
         if not fixed and step % check == check - 1 and bool(done.all()):
             break
-        c = torch.where(done, torch.full_like(num, 0.5), num / torch.where(done, torch.ones_like(den), den))
-        c = c.clamp(0.0, 1.0)
-        hi_branch = ((1 + c)[:, None, None] * P2 - P3) / c.clamp(min=1e-300)[:, None, None]
-        lo_branch = ((1 - 2 * c)[:, None, None] * P + (1 + c)[:, None, None] * P2 - P3) / \
-            (1 - c).clamp(min=1e-300)[:, None, None]
-        Pn = torch.where((c >= 0.5)[:, None, None], hi_branch, lo_branch)
-        P = torch.where(done[:, None, None], P, Pn)
     return P
 
 

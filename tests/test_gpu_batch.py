@@ -42,6 +42,35 @@ def test_batched_jk_blocks_equal_single_molecule_jk():
         assert float((Kb - Ks).abs().max()) < 1e-10
 
 
+def test_purification_equals_eigenprojector():
+    """LA2.purify (two GEMMs and pqb_purify_step per step) gives the
+    projector on the nocc lowest eigenstates, batched, with padded
+    dimensions held empty; the fixed-step form (no host checks) agrees."""
+    from pyquante_b200.LA2 import purify
+    rng = np.random.default_rng(3)
+    B, n = 6, 40
+    nocc = np.array([3, 7, 10, 12, 15, 20])
+    nreal = np.array([40, 40, 33, 25, 40, 31])
+    F = np.zeros((B, n, n))
+    for b in range(B):
+        m = nreal[b]
+        Q, _ = np.linalg.qr(rng.standard_normal((m, m)))
+        e = np.sort(rng.uniform(-5, 5, m))
+        e[nocc[b]:] += 0.5          # a gap at the Fermi level
+        F[b, :m, :m] = (Q * e) @ Q.T
+    pad = torch.tensor(np.arange(n)[None, :] >= nreal[:, None], device="cuda")
+    Ft = torch.tensor(F, device="cuda")
+    for kw in (dict(), dict(fixed=True, maxit=60)):
+        P = purify(Ft, torch.tensor(nocc, dtype=torch.float64), pad=pad, **kw).cpu().numpy()
+        for b in range(B):
+            m = nreal[b]
+            w, V = np.linalg.eigh(F[b, :m, :m])
+            ref = V[:, :nocc[b]] @ V[:, :nocc[b]].T
+            assert np.abs(P[b, :m, :m] - ref).max() < 1e-10, (kw, b)
+            if m < n:
+                assert np.abs(P[b, m:, :]).max() < 1e-12 and np.abs(P[b, :, m:]).max() < 1e-12
+
+
 def test_molecule_mask_skips_masked_molecules():
     """pqb_set_molecule_mask: the masked molecules' J and K blocks come out
     zero and the others' equal the unmasked build (FP64 and mixed, with the
