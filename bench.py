@@ -428,6 +428,7 @@ def run_batch(a):
                    "per_molecule_scf_s_p50": float(np.percentile(res["scf_times"], 50)),
                    "per_molecule_scf_s_p99": float(np.percentile(res["scf_times"], 99)),
                    "cuda_graph": res["graph"], "whole_iteration_graph": res["whole_iteration_graph"],
+                   "incremental_fock_builds": res["incremental"],
                    "plan": res["plan"],
                    "single_solve_loop": {"sample": len(pick), "molecules_per_s": len(pick) / st.sum(),
                                          "p50_s": float(np.percentile(st, 50)), "p99_s": float(np.percentile(st, 99)),

@@ -89,6 +89,19 @@ int pqb_dense_len(const pqb_ctx *ctx, int64_t *len);
  * per SCF). */
 int pqb_set_molecule_mask(pqb_ctx *ctx, const int *mask);
 
+/* Density screening of the direct builds (incremental Fock builds digest a
+ * density difference, most of whose blocks are small): with shell_dmax, a
+ * device array of nshell bounds max_ij |D_ij| over each shell's rows i (in
+ * its molecule's block; pqb_shell_dmax fills it), a work item (ab|cd) is
+ * skipped when Q_ab Q_cd max(dmax[a], dmax[b], dmax[c], dmax[d]) < tau,
+ * Q the Schwarz factors of pqb_schwarz (required first).  NULL disables it.
+ * The array stays owned by the caller, like the molecule mask; its contents
+ * may change between builds.  pqb_shell_dmax writes those bounds for D (the
+ * dense layout of pqb_jk_direct) on the stream.  No counterpart in the
+ * reference (whose SCF rebuilds F from the full density). */
+int pqb_set_density_screen(pqb_ctx *ctx, const double *shell_dmax, double tau);
+int pqb_shell_dmax(pqb_ctx *ctx, const double *D, double *shell_dmax, void *stream);
+
 /* One step of canonical purification (Palser and Manolopoulos) for nmat
  * row-major n x n device matrices back to back: from P, P2 = P P and
  * P3 = P2 P, with c = tr(P2 - P3)/tr(P - P2) clamped to [0, 1],

@@ -35,6 +35,8 @@ SIGNATURES = {
                                                _c_dbl_p]),
     "pqb_dense_len": (ctypes.c_int, [_vp, _c_i64_p]),
     "pqb_set_molecule_mask": (ctypes.c_int, [_vp, _vp]),
+    "pqb_set_density_screen": (ctypes.c_int, [_vp, _vp, ctypes.c_double]),
+    "pqb_shell_dmax": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "pqb_purify_step": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, _vp]),
     "pqb_schwarz": (ctypes.c_int, [_vp, _c_dbl_p, _vp]),
     "pqb_num_pairs": (ctypes.c_int, [_vp]),

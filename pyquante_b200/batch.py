@@ -27,6 +27,13 @@ less than ``conv`` and its commutator FDS - SDF is below ``err_tol`` (its
 SCF time is the time of that iteration); converged molecules keep their
 last density, and from the next iteration on the Fock build skips their
 quartets (a per-molecule mask read by the kernels).
+
+The Fock builds are incremental: each iteration digests the density change
+D - D_prev into accumulated J and K (J and K are linear in D), with work
+items skipped when their Schwarz bound times the largest density change of
+their shells is below ``screen_tau``; as the SCF converges the changes
+shrink and most items drop out.  Every ``rebuild_every`` iterations the
+accumulators restart from a full build.
 """
 import ctypes
 import time
@@ -68,6 +75,7 @@ class BatchEngine:
             FS += sh["fscale"]
             MOLS.append(len(L))
         ns, nbf, nm = len(L), int(sum(self.n)), len(self.mols)
+        self.nshell = ns
         I, Dd = ctypes.c_int, ctypes.c_double
         self.ctx.check(self.ctx.lib.pqb_shells_upload_batch(
             self.ctx.h, nm, (I * (nm + 1))(*MOLS), ns, (I * ns)(*L), (I * ns)(*NP), (I * ns)(*OFF), (I * ns)(*F0),
@@ -241,7 +249,8 @@ class _Diis:
 
 
 def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, graph=True, schwarz=1e-12,
-                fp32_threshold=1e-5, device=None, max_buckets=8, solver="purify", err_tol=1e-6, purify_steps=48):
+                fp32_threshold=1e-5, device=None, max_buckets=8, solver="purify", err_tol=1e-6, purify_steps=48,
+                incremental=True, screen_tau=1e-12, rebuild_every=8):
     """Solve RHF for every (molecule, basis) in ``systems`` together.
 
     The Fock build of every iteration is one engine call for all molecules;
@@ -288,6 +297,13 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
     Dflat = torch.zeros(eng.dense_len, **f64)
     Jf = torch.zeros_like(Dflat)
     Kf = torch.zeros_like(Dflat)
+    lib, h_ctx = eng.ctx.lib, eng.ctx.h
+    if incremental:
+        # J, K accumulated over density changes, screened by shell bounds of the change
+        Dprev, dD = torch.zeros_like(Dflat), torch.zeros_like(Dflat)
+        Jacc, Kacc = torch.zeros_like(Dflat), torch.zeros_like(Dflat)
+        dsh = torch.zeros(eng.nshell, **f64)
+        eng.ctx.check(lib.pqb_set_density_screen(h_ctx, _lib.ptr(dsh), float(screen_tau)))
     it_dev = torch.zeros((), dtype=torch.int64, device=dev)
     # per molecule (in input order): converged flag and energy, gathered on the device
     all_idx = torch.cat([torch.as_tensor(bk.idx, device=dev) for bk in buckets])
@@ -299,10 +315,20 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
     def fock_build():
         for bk in buckets:
             Dflat.index_copy_(0, bk.flat, bk.D.reshape(-1).index_select(0, bk.pos))
-        eng.jk(Dflat, Jf, Kf, precision)
+        if incremental:
+            torch.sub(Dflat, Dprev, out=dD)
+            eng.ctx.check(lib.pqb_shell_dmax(h_ctx, _lib.ptr(dD), _lib.ptr(dsh), _lib.stream_ptr()))
+            eng.jk(dD, Jf, Kf, precision)
+            Jacc.add_(Jf)
+            Kacc.add_(Kf)
+            Dprev.copy_(Dflat)
+            Js, Ks = Jacc, Kacc
+        else:
+            eng.jk(Dflat, Jf, Kf, precision)
+            Js, Ks = Jf, Kf
         for bk in buckets:
-            bk.J.view(-1).index_copy_(0, bk.pos, Jf.index_select(0, bk.flat))
-            bk.K.view(-1).index_copy_(0, bk.pos, Kf.index_select(0, bk.flat))
+            bk.J.view(-1).index_copy_(0, bk.pos, Js.index_select(0, bk.flat))
+            bk.K.view(-1).index_copy_(0, bk.pos, Ks.index_select(0, bk.flat))
             bk.F.copy_(bk.h + 2.0 * bk.J - bk.K)
             bk.E.copy_((bk.D * bk.h).sum(dim=(1, 2)) + (bk.D * bk.F).sum(dim=(1, 2)) + bk.enuc)
 
@@ -358,9 +384,18 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
     flags.zero_()
     active.fill_(1)
     torch.cuda.synchronize()
+
+    def restart():
+        # the next build is a full one: accumulators from zero
+        if incremental:
+            Dprev.zero_()
+            Jacc.zero_()
+            Kacc.zero_()
     iter_time = []
     t0 = time.perf_counter()
     for it in range(maxiter):
+        if it % rebuild_every == 0:
+            restart()
         if g is not None:
             g.replay()
             if not whole:
@@ -373,6 +408,8 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
             break
     torch.cuda.synchronize()
     t_end = time.perf_counter()
+    eng.ctx.check(lib.pqb_set_density_screen(h_ctx, None, 0.0))
+    eng.set_mask(None)
     energies = np.zeros(B)
     iters = np.zeros(B, dtype=np.int64)
     times = np.zeros(B)
@@ -386,4 +423,5 @@ def batched_rhf(systems, precision="mixed", conv=1e-8, maxiter=60, diis_size=8, 
         times[bk.idx] = np.where(ok, [iter_time[c] if c >= 0 else 0.0 for c in ci], t_end - t0)
     return dict(energies=energies, iterations=iters, converged=done, scf_times=times, scf_seconds=t_end - t0,
                 total_seconds=t_end - t_start, plan=counts, nbf=np.array(eng.n), graph=g is not None,
-                whole_iteration_graph=whole and g is not None, buckets=[bk.nb for bk in buckets])
+                whole_iteration_graph=whole and g is not None, incremental=incremental,
+                buckets=[bk.nb for bk in buckets])

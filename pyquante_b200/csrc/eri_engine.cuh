@@ -95,7 +95,7 @@ struct EpiPacked {
     double *out;
     const double *fscale;
     static constexpr bool kTile = false;
-    __device__ __forceinline__ bool masked(int) const { return false; }
+    __device__ __forceinline__ bool screened(const PairInfo &, const PairInfo &, int, int) const { return false; }
     template <int LC, int LD, typename R>
     __device__ __forceinline__ void ab(const QCtx &q, int ia, int ib, const R *acc) const
     {
@@ -194,9 +194,18 @@ struct EpiJKn {
     const double *D[NDEN];        // pre-scaled densities
     double *Jacc[NDEN], *Kacc[NDEN];
     const float *Df[NDEN];        // their single-precision copies (FP32 lists of the mixed mode), or null
-    const int *molmask;           // batched bases: molecule m's items are skipped when molmask[m] == 0 (null: none)
+    ItemScreen scr;               // items skipped by molecule mask or density bound (all fields optional)
     static constexpr bool kTile = true;
-    __device__ __forceinline__ bool masked(int mol) const { return molmask && __ldg(molmask + mol) == 0; }
+    __device__ __forceinline__ bool screened(const PairInfo &pb, const PairInfo &pk, int bra, int ket) const
+    {
+        if (scr.molmask && __ldg(scr.molmask + pb.mol) == 0) return true;
+        if (scr.dmax) {
+            const double d = fmax(fmax(__ldg(scr.dmax + pb.sa), __ldg(scr.dmax + pb.sb)),
+                                  fmax(__ldg(scr.dmax + pk.sa), __ldg(scr.dmax + pk.sb)));
+            if (__ldg(scr.Qpair + bra) * __ldg(scr.Qpair + ket) * d < scr.tau) return true;
+        }
+        return false;
+    }
 
     // (called by every lane of the warp; a lane past the end of the item list
     // passes its neighbour's quartet with zero integrals)
@@ -447,7 +456,7 @@ struct EpiSchwarz {
     unsigned long long *Q2bits;   // bit patterns of non-negative doubles
     const double *fscale;
     static constexpr bool kTile = false;
-    __device__ __forceinline__ bool masked(int) const { return false; }
+    __device__ __forceinline__ bool screened(const PairInfo &, const PairInfo &, int, int) const { return false; }
     template <int LC, int LD, typename R>
     __device__ __forceinline__ void ab(const QCtx &q, int ia, int ib, const R *acc) const
     {
@@ -606,12 +615,12 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
         int4 e = list[live ? qi : nq - 1];   // bra pair, ket pair, first primitive quartet, count
         if (!live) e.w = 0;
         const PairInfo &pb = pairs[e.x];
-        // items of masked molecules (batched bases) carry no primitive quartets;
-        // a warp with none left skips the item altogether
-        const bool skip = epi.masked(pb.mol);
+        const PairInfo &pk = pairs[e.y];
+        // screened items (masked molecules, small density bounds) carry no
+        // primitive quartets; a warp with none left skips the item altogether
+        const bool skip = live && epi.screened(pb, pk, e.x, e.y);
         if (__all_sync(0xffffffffu, skip || !live)) continue;
         if (skip) e.w = 0;
-        const PairInfo &pk = pairs[e.y];
         const double Ax = pb.A[0], Ay = pb.A[1], Az = pb.A[2];
         const double Cx = pk.A[0], Cy = pk.A[1], Cz = pk.A[2];
         const double ABx = pb.AB[0], ABy = pb.AB[1], ABz = pb.AB[2];
@@ -846,7 +855,11 @@ __global__ void __launch_bounds__(kBlockThreads, ncart(LC) * ncart(LD) <= 6 ? 3 
         if (tid < NSQ) {
             SlotData &s = sd[tid];
             const int qi = base + tid;
-            const bool take = qi < nq && !epi.masked(pairs[list[qi].x].mol);
+            bool take = qi < nq;
+            if (take) {
+                const int4 t = list[qi];
+                take = !epi.screened(pairs[t.x], pairs[t.y], t.x, t.y);
+            }
             if (take) {
                 const int4 e = list[qi];
                 const PairInfo &pb = pairs[e.x];

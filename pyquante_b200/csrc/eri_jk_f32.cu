@@ -8,10 +8,10 @@
 namespace pqb {
 cudaError_t launch_jk_f32(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                           const double *Dscaled, const float *Dscaled_f, double *Jacc, double *Kacc, int n,
-                          cudaStream_t st, int nsm, const int *molmask)
+                          cudaStream_t st, int nsm, const ItemScreen &scr)
 {
     (void)n;
-    EpiJK epi{{Dscaled}, {Jacc}, {Kacc}, {Dscaled_f}, molmask};
+    EpiJK epi{{Dscaled}, {Jacc}, {Kacc}, {Dscaled_f}, scr};
     return launch_eri<float>(qc, list, nq, pairs, prims, epi, st, nsm);
 }
 }  // namespace pqb

@@ -5,10 +5,10 @@
 namespace pqb {
 cudaError_t launch_jk_f64(int qc, const int4 *list, int nq, const PairInfo *pairs, const PrimPair *prims,
                           const double *Dscaled, double *Jacc, double *Kacc, int n, cudaStream_t st, int nsm,
-                          const int *molmask)
+                          const ItemScreen &scr)
 {
     (void)n;
-    EpiJK epi{{Dscaled}, {Jacc}, {Kacc}, {nullptr}, molmask};
+    EpiJK epi{{Dscaled}, {Jacc}, {Kacc}, {nullptr}, scr};
     return launch_eri<double>(qc, list, nq, pairs, prims, epi, st, nsm);
 }
 }  // namespace pqb

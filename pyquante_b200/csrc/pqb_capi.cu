@@ -98,7 +98,9 @@ struct pqb_ctx {
     bool graph_warm[6] = {false, false, false, false, false, false};   // one eager build first (one-time launch setup stays out of the capture)
     double *d_Jacc = nullptr, *d_Kacc = nullptr;
     double *d_Jacc2 = nullptr, *d_Kacc2 = nullptr;   // second density's graph accumulators
-    const int *d_molmask = nullptr;  // caller-owned per-molecule mask of the direct builds (batched bases)
+    ItemScreen scr{};                // caller-owned molecule mask / shell density bounds of the direct builds
+    double *d_Qpair = nullptr;       // Schwarz factor per pair (device)
+    int4 *d_shell_info = nullptr;    // per shell: first function within its molecule, functions, molecule
     // small scratch
     double *d_atoms = nullptr;
     size_t atoms_cap = 0;
@@ -145,6 +147,24 @@ __global__ void symmetrize_kernel(double *M, int n, const double *__restrict__ S
     if (S) s *= S[(int64_t)i * n + j];
     M[(int64_t)i * n + j] = s;
     M[(int64_t)j * n + i] = s;
+}
+
+// dmax[s] = max |D_ij| over the rows i of shell s and the columns j of its
+// molecule's block (one warp per shell).
+__global__ void shell_dmax_kernel(int nshell, const int4 *__restrict__ info, const long long *__restrict__ mol_off,
+                                  const int *__restrict__ mol_n, const double *__restrict__ D, double *__restrict__ dmax)
+{
+    const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (s >= nshell) return;
+    const int4 in = info[s];
+    const int nm = mol_n[in.z];
+    const double *row = D + mol_off[in.z] + (long long)in.x * nm;
+    double m = 0.0;
+    for (int r = 0; r < in.y; ++r, row += nm)
+        for (int j = lane; j < nm; j += 32) m = fmax(m, fabs(row[j]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) dmax[s] = m;
 }
 
 // The graph path's epilogue: J and K (K2 == nullptr: J alone) from their
@@ -1202,6 +1222,12 @@ static void release_basis(pqb_ctx *ctx)
     ctx->d_Dscaled = nullptr;
     ctx->d_Dscaled_f = nullptr;
     free_dev(ctx->d_q2);
+    free_dev(ctx->d_Qpair);
+    free_dev(ctx->d_shell_info);
+    ctx->d_Qpair = nullptr;
+    ctx->d_shell_info = nullptr;
+    ctx->scr.dmax = nullptr;   // the bounds are per shell of the old basis
+    ctx->scr.Qpair = nullptr;
     free_dev(ctx->d_full);
     free_dev(ctx->d_diag);
     free_dev(ctx->d_plan);
@@ -1429,6 +1455,15 @@ static int shells_upload_batch_impl(pqb_ctx *ctx, int nmol, const int *mol_shell
     PQB_CK(ctx, cudaMemcpy(ctx->d_prims, prims.data(), sizeof(PrimPair) * prims.size(), cudaMemcpyHostToDevice));
     PQB_CK(ctx, cudaMemcpy(ctx->d_fscale, fscale, sizeof(double) * nbf, cudaMemcpyHostToDevice));
     {
+        std::vector<int4> si(nshell);
+        for (int sh = 0; sh < nshell; ++sh) {
+            const int m = shell_mol[sh];
+            si[sh] = make_int4(shell_f0[sh] - ctx->mol_f0[m], ncart(shell_l[sh]), m, 0);
+        }
+        PQB_CK(ctx, cudaMalloc(&ctx->d_shell_info, sizeof(int4) * nshell));
+        PQB_CK(ctx, cudaMemcpy(ctx->d_shell_info, si.data(), sizeof(int4) * nshell, cudaMemcpyHostToDevice));
+    }
+    {
         std::vector<double> es((size_t)ctx->dense_len);
         for (int m = 0; m < nmol; ++m) {
             const int f0 = ctx->mol_f0[m], n = ctx->mol_n[m];
@@ -1480,13 +1515,13 @@ static int schwarz_impl(pqb_ctx *ctx, double *Q_host, void *stream)
     for (int c = 0; c < kNumQuartetClass; ++c)
         PQB_CK(ctx, launch_schwarz_f64(c, ctx->d_diag + ctx->diag_off[c], (int)ctx->diag_cnt[c], ctx->d_pairs,
                                        ctx->d_prims, ctx->d_q2, ctx->d_fscale, st, ctx->nsm));
-    double *dQ = nullptr;
-    PQB_CK(ctx, cudaMalloc(&dQ, sizeof(double) * np));
+    if (!ctx->d_Qpair) PQB_CK(ctx, cudaMalloc(&ctx->d_Qpair, sizeof(double) * np));
+    double *dQ = ctx->d_Qpair;
     finalize_q_kernel<<<(np + 255) / 256, 256, 0, st>>>(ctx->d_q2, dQ, np);
     ctx->Q.assign(np, 0.0);
     cudaError_t e = cudaMemcpyAsync(ctx->Q.data(), dQ, sizeof(double) * np, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(dQ);
+    if (ctx->scr.dmax) ctx->scr.Qpair = dQ;
     if (e != cudaSuccess) return fail(ctx, PQB_E_CUDA, "pqb_schwarz: %s", cudaGetErrorString(e));
     ctx->have_q = true;
     if (Q_host) memcpy(Q_host, ctx->Q.data(), sizeof(double) * np);
@@ -1817,7 +1852,7 @@ static int launch_build(pqb_ctx *ctx, int nden, double *const Jacc[2], double *c
     }
     const double *Ds[2] = {ctx->d_Dscaled, ctx->d_Dscaled2};
     const float *Dsf[2] = {ctx->d_Dscaled_f, ctx->d_Dscaled2_f};
-    const int *mm = ctx->d_molmask;
+    const ItemScreen &mm = ctx->scr;
     // fork: class launches spread over the context's streams, heaviest first
     PQB_CK(ctx, cudaEventRecord(ctx->ev_fork, st));
     for (int k = 0; k < pqb_ctx::kStreams; ++k) PQB_CK(ctx, cudaStreamWaitEvent(ctx->streams[k], ctx->ev_fork, 0));
@@ -2006,8 +2041,32 @@ int pqb_jk_direct2(pqb_ctx *ctx, const double *Da, const double *Db, double *Ja,
 int pqb_set_molecule_mask(pqb_ctx *ctx, const int *mask)
 {
     if (!ctx) return PQB_E_ARG;
-    ctx->d_molmask = mask;
-    drop_graphs(ctx);   // a captured build holds the old pointer
+    ctx->scr.molmask = mask;
+    drop_graphs(ctx);   // a captured build holds the old screen
+    return PQB_OK;
+}
+
+int pqb_set_density_screen(pqb_ctx *ctx, const double *shell_dmax, double tau)
+{
+    if (!ctx || tau < 0.0) return fail(ctx, PQB_E_ARG, "pqb_set_density_screen: bad arguments");
+    if (shell_dmax && !ctx->d_Qpair)
+        return fail(ctx, PQB_E_STATE, "pqb_set_density_screen: call pqb_schwarz (or pqb_plan) first");
+    ctx->scr.dmax = shell_dmax;
+    ctx->scr.Qpair = shell_dmax ? ctx->d_Qpair : nullptr;
+    ctx->scr.tau = tau;
+    drop_graphs(ctx);
+    return PQB_OK;
+}
+
+int pqb_shell_dmax(pqb_ctx *ctx, const double *D, double *shell_dmax, void *stream)
+{
+    if (!ctx || !D || !shell_dmax) return fail(ctx, PQB_E_ARG, "pqb_shell_dmax: bad arguments");
+    if (!ctx->d_shell_info) return fail(ctx, PQB_E_STATE, "pqb_shell_dmax: no basis uploaded");
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    const int warps = 8;
+    shell_dmax_kernel<<<(ctx->nshell + warps - 1) / warps, warps * 32, 0, (cudaStream_t)stream>>>(
+        ctx->nshell, ctx->d_shell_info, ctx->d_mol_off, ctx->d_mol_n, D, shell_dmax);
+    PQB_CK(ctx, cudaGetLastError());
     return PQB_OK;
 }
 

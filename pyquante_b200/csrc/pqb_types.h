@@ -13,6 +13,20 @@ constexpr int kMaxL = 2;                         // shells up to d (cartesian)
 constexpr int kNumPairClass = 6;                 // ss ps pp ds dp dd
 constexpr int kNumQuartetClass = 21;             // bra class >= ket class
 
+// Per-item screening of the direct builds (all fields optional):
+//   molmask: batched bases, molecule m's items are skipped when molmask[m] == 0;
+//   dmax:    per shell, a bound on |D_ij| over the shell's rows i (within
+//            its molecule's block); an item (ab|cd) is skipped when
+//            Q_ab Q_cd max(dmax[a], dmax[b], dmax[c], dmax[d]) < tau, Q the
+//            Schwarz factors (the incremental builds of a batched SCF digest
+//            density differences, most of which are small).
+struct ItemScreen {
+    const int *molmask;
+    const double *dmax;
+    const double *Qpair;
+    double tau;
+};
+
 struct PairInfo {
     double A[3];       // centre of the first shell
     double AB[3];      // A - B

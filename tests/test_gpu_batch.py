@@ -119,6 +119,19 @@ def test_batched_rhf_matches_single_solves(graph, solver):
         assert abs(es - e) < 1e-8, (basis, es, e)
 
 
+def test_incremental_fock_builds_match_full_builds():
+    """The incremental builds (density changes, screened by shell bounds of
+    the change, full rebuild every 8 iterations) give the energies of full
+    builds every iteration (1e-9 Eh), in FP64 and in mixed precision."""
+    systems = _systems()
+    for prec in ("fp64", "mixed"):
+        inc = batched_rhf(systems, precision=prec, conv=1e-10, maxiter=80, incremental=True)
+        full = batched_rhf(systems, precision=prec, conv=1e-10, maxiter=80, incremental=False)
+        assert inc["incremental"] and not full["incremental"]
+        assert inc["converged"].all() and full["converged"].all()
+        assert np.abs(inc["energies"] - full["energies"]).max() < 1e-9, prec
+
+
 def test_batched_rhf_64_mixed_size_systems():
     """The batched-SCF workload's recipe on 64 systems (water clusters of
     1..12 molecules, STO-3G or 6-31G*, 7..228 functions): every batched
