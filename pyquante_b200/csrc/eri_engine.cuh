@@ -512,8 +512,13 @@ struct OsClass {
 
 // ---------------------------------------------------------- thread mode --
 // Register cap per class (via the minimum resident blocks of 128 threads):
-// small classes are latency bound, so they trade registers for occupancy.
-__host__ __device__ constexpr int thread_min_blocks(int nabcd) { return nabcd == 1 ? 8 : (nabcd <= 9 ? 4 : 2); }
+// small classes are latency bound, so they trade registers for occupancy
+// (six blocks for up to three components, five for up to nine, measured
+// faster than four even with a few spilled registers).
+__host__ __device__ constexpr int thread_min_blocks(int nabcd)
+{
+    return nabcd == 1 ? 8 : (nabcd <= 3 ? 6 : (nabcd <= 9 ? 5 : 2));
+}
 
 // Single-precision counterpart of add_prim_quartet for the FP32 lists of
 // the mixed mode: geometry, roots (rys_roots_f32), 2-D tables and assembly
