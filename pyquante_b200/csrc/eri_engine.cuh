@@ -513,11 +513,12 @@ struct OsClass {
 // ---------------------------------------------------------- thread mode --
 // Register cap per class (via the minimum resident blocks of 128 threads):
 // small classes are latency bound, so they trade registers for occupancy
-// (six blocks for up to three components, five for up to nine, measured
-// faster than four even with a few spilled registers).
+// (six blocks for up to three components, five for up to nine, three for
+// the 27 of (11|10), measured faster than fewer even with a few spilled
+// registers).
 __host__ __device__ constexpr int thread_min_blocks(int nabcd)
 {
-    return nabcd == 1 ? 8 : (nabcd <= 3 ? 6 : (nabcd <= 9 ? 5 : 2));
+    return nabcd == 1 ? 8 : (nabcd <= 3 ? 6 : (nabcd <= 9 ? 5 : (nabcd == 27 ? 3 : 2)));
 }
 
 // Single-precision counterpart of add_prim_quartet for the FP32 lists of
