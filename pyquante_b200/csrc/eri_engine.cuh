@@ -799,10 +799,10 @@ eri_thread_kernel(const int4 *__restrict__ list, int nq,
 // ----------------------------------------------------------- block mode --
 constexpr int kBlockThreads = 256;
 
-// Shared-memory budget of the 2-D integrals of one round of a block: PB
+// Shared-memory budget of the 2-D integrals of one pass of a block: PB
 // primitive quartets per slot go through the roots, 2-D and assembly phases
-// together (two barriers per round), as many as fit in the budget (at most 4).
-constexpr size_t kBlockRoundBytes = 64 * 1024;
+// together (two barriers per pass), as many as fit in the budget (at most 4).
+constexpr size_t kBlockPassBytes = 64 * 1024;
 
 template <int LA, int LB, int LC, int LD, typename R, class Epi>
 struct BlockLayout {
@@ -812,9 +812,9 @@ struct BlockLayout {
     static constexpr int G2D = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
     static constexpr int NSQ = kBlockThreads / NAB;
     static constexpr size_t pq_bytes = (size_t)NSQ * 3 * NR * G2D * sizeof(R);   // one primitive quartet per slot
-    static constexpr int PB = pq_bytes * 4 <= kBlockRoundBytes ? 4
-                              : pq_bytes * 3 <= kBlockRoundBytes ? 3
-                              : pq_bytes * 2 <= kBlockRoundBytes ? 2 : 1;
+    static constexpr int PB = pq_bytes * 4 <= kBlockPassBytes ? 4
+                              : pq_bytes * 3 <= kBlockPassBytes ? 3
+                              : pq_bytes * 2 <= kBlockPassBytes ? 2 : 1;
     static constexpr size_t g_bytes = (PB * pq_bytes + 15) / 16 * 16;
     // the integral tile of a tiled epilogue reuses the 2-D integral buffer
     static constexpr size_t tile_bytes = Epi::kTile ? (size_t)NSQ * NAB * (NCD + 1) * sizeof(double) : 0;
@@ -899,7 +899,7 @@ __global__ void __launch_bounds__(kBlockThreads, ncart(LC) * ncart(LD) <= 6 ? 3 
         for (int c = 0; c < NCD; ++c) acc[c] = (R)0;
 
         for (int pp0 = 0; pp0 < maxpp; pp0 += PB) {
-            // this round: primitive quartets pp0 .. pp0 + nb - 1 of every slot
+            // this pass: primitive quartets pp0 .. pp0 + nb - 1 of every slot
             const int nb = maxpp - pp0 < PB ? maxpp - pp0 : PB;
             // roots and weights (with the primitive-quartet prefactor)
             for (int t = tid; t < nb * NSQ * NR; t += kBlockThreads) {
@@ -948,7 +948,7 @@ __global__ void __launch_bounds__(kBlockThreads, ncart(LC) * ncart(LD) <= 6 ? 3 
                 }
             }
             __syncthreads();
-            // 2-D integrals, one (round quartet, slot, root, axis) per task; weight on x
+            // 2-D integrals, one (pass quartet, slot, root, axis) per task; weight on x
             for (int t = tid; t < nb * NSQ * NR * 3; t += kBlockThreads) {
                 const int b = t / (NSQ * NR * 3), rb = t - b * (NSQ * NR * 3);
                 const int s = rb / (NR * 3), rem = rb - s * NR * 3, r = rem / 3, x = rem - r * 3;
