@@ -107,6 +107,45 @@ def test_molecule_mask_skips_masked_molecules():
         assert float((K - K0).abs().max()) < 1e-12 * float(K0.abs().max())
 
 
+def test_density_screen_skips_small_density_items():
+    """pqb_set_density_screen / pqb_shell_dmax: with the shell bounds of
+    the density itself and a threshold far below every bound the build is
+    the unscreened one (1e-12); with a threshold above every Q_ab Q_cd dmax
+    every item is skipped (J = K = 0); a threshold in between changes J and
+    K by less than the skipped items' bound allows."""
+    from pyquante_b200 import _lib
+    systems = _systems()
+    beng = BatchEngine(systems)
+    beng.plan(schwarz=1e-12, fp32_threshold=0.0)
+    rng = np.random.default_rng(2)
+    Ds = []
+    for n in beng.n:
+        C = rng.standard_normal((n, max(1, n // 3))) * 0.3
+        Ds.append(C @ C.T)
+    Dflat = torch.tensor(np.concatenate([d.reshape(-1) for d in Ds]), dtype=torch.float64, device="cuda")
+    J0, K0 = torch.zeros_like(Dflat), torch.zeros_like(Dflat)
+    beng.jk(Dflat, J0, K0, "fp64")
+    dsh = torch.zeros(beng.nshell, dtype=torch.float64, device="cuda")
+    lib, h = beng.ctx.lib, beng.ctx.h
+    beng.ctx.check(lib.pqb_shell_dmax(h, _lib.ptr(Dflat), _lib.ptr(dsh), _lib.stream_ptr()))
+    assert float(dsh.min()) > 0.0 and abs(float(dsh.max()) - float(Dflat.abs().max())) < 1e-15
+    for tau, kind in ((1e-30, "none"), (1e30, "all"), (1e-6, "some")):
+        beng.ctx.check(lib.pqb_set_density_screen(h, _lib.ptr(dsh), tau))
+        J, K = torch.zeros_like(Dflat), torch.zeros_like(Dflat)
+        beng.jk(Dflat, J, K, "fp64")
+        dj, dk = float((J - J0).abs().max()), float((K - K0).abs().max())
+        if kind == "none":
+            assert dj < 1e-12 * float(J0.abs().max()) and dk < 1e-12 * float(K0.abs().max())
+        elif kind == "all":
+            assert float(J.abs().max()) == 0.0 and float(K.abs().max()) == 0.0
+        else:
+            assert 0.0 < max(dj, dk) < 1e-2
+    beng.ctx.check(lib.pqb_set_density_screen(h, None, 0.0))
+    J, K = torch.zeros_like(Dflat), torch.zeros_like(Dflat)
+    beng.jk(Dflat, J, K, "fp64")
+    assert float((J - J0).abs().max()) < 1e-12 * float(J0.abs().max())
+
+
 @pytest.mark.parametrize("graph,solver", [(True, "purify"), (False, "purify"), (True, "eigh")])
 def test_batched_rhf_matches_single_solves(graph, solver):
     """Densities by batched canonical purification (no eigensolver) or by
