@@ -170,6 +170,37 @@ struct WarpRuns {
     }
 };
 
+// Full-warp sums of K values per lane (K <= 32) by recursive halving: at each
+// of the first log2(KP) butterfly levels (KP = K rounded up to a power of two)
+// every lane keeps half of its remaining values and adds its partner's half
+// of them, then the remaining levels are a plain butterfly.  Lane L ends with
+// the warp's sum of value idx(L) (the kept halves), held by the 32/KP lanes
+// that agree on those bits; 2 (KP - 1) + 2 (5 - log2 KP) 32-bit shuffles in
+// place of the 10 K of K separate sums.  Every lane of the warp must take part.
+template <int K>
+__device__ __forceinline__ double warp_sum_transposed(const double *v, int lane, int &idx)
+{
+    constexpr int KP = K <= 1 ? 1 : K <= 2 ? 2 : K <= 4 ? 4 : K <= 8 ? 8 : K <= 16 ? 16 : 32;
+    double w[KP];
+#pragma unroll
+    for (int j = 0; j < KP; ++j) w[j] = j < K ? v[j] : 0.0;
+    idx = 0;
+    int o = 16;
+#pragma unroll
+    for (int n = KP; n > 1; n >>= 1, o >>= 1) {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int j = 0; j < n / 2; ++j) {
+            const double keep = up ? w[j + n / 2] : w[j], send = up ? w[j] : w[j + n / 2];
+            w[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+        if (up) idx += n / 2;
+    }
+#pragma unroll
+    for (; o > 0; o >>= 1) w[0] += __shfl_xor_sync(0xffffffffu, w[0], o);
+    return w[0];
+}
+
 // Direct J/K digestion of unique quartets with 8-fold degeneracy weights:
 //   Jacc[i,j] += 2 v' D_kl,  Jacc[k,l] += 2 v' D_ij,
 //   Kacc[i,k] += v' D_jl, Kacc[i,l] += v' D_jk, Kacc[j,k] += v' D_il, Kacc[j,l] += v' D_ik,
@@ -222,6 +253,9 @@ struct EpiJKn {
         // Kacc[b,c] by lanes that also share the ket's first shell
         const WarpRuns rb((long long)q.bra, lane);
         const WarpRuns rbc(((long long)q.bra << 32) | (unsigned)q.sc, lane);
+        // (the shuffle is taken by every lane, outside any condition)
+        const int bra0 = __shfl_sync(0xffffffffu, q.bra, 0);
+        const bool one_bra = __all_sync(0xffffffffu, bra0 == q.bra);
         // every density digests the same integrals, one after the other
 #pragma unroll
         for (int s = 0; s < NDEN; ++s) {
@@ -247,6 +281,7 @@ struct EpiJKn {
                     dcd[c][d] = __ldg(Dc + c * nm + q.fd + d);
                     jcd[c][d] = (T)0;
                 }
+            double jabv[NA * NB];
 #pragma unroll
             for (int a = 0; a < NA; ++a)
 #pragma unroll
@@ -261,9 +296,22 @@ struct EpiJKn {
                             jab = fma(v, dcd[c][d], jab);
                             jcd[c][d] = fma(v, dab[a][b], jcd[c][d]);
                         }
-                    const double js = rb.sum((double)jab);
-                    if (rb.last && js != 0.0) atomicAdd(Jb + (q.fa + a) * nm + q.fb + b, 2.0 * js);
+                    jabv[a * NB + b] = (double)jab;
                 }
+            if (NA * NB <= 32 && one_bra) {
+                // the whole warp is one bra pair: all NAB sums in one transposed reduction
+                int idx;
+                const double js = warp_sum_transposed<(NA * NB <= 32 ? NA * NB : 1)>(jabv, lane, idx);
+                constexpr int KP = NA * NB <= 1 ? 1 : NA * NB <= 2 ? 2 : NA * NB <= 4 ? 4 : NA * NB <= 8 ? 8 : NA * NB <= 16 ? 16 : 32;
+                if (idx < NA * NB && (lane & (32 / KP - 1)) == 0 && js != 0.0)
+                    atomicAdd(Jb + (q.fa + idx / NB) * nm + q.fb + idx % NB, 2.0 * js);
+            } else {
+#pragma unroll
+                for (int ab = 0; ab < NA * NB; ++ab) {
+                    const double js = rb.sum(jabv[ab]);
+                    if (rb.last && js != 0.0) atomicAdd(Jb + (q.fa + ab / NB) * nm + q.fb + ab % NB, 2.0 * js);
+                }
+            }
 #pragma unroll
             for (int c = 0; c < NC; ++c)
 #pragma unroll
