@@ -250,8 +250,8 @@ struct EpiJKn {
         constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NCD = NC * ND;
         const bool bd = q.sa == q.sb, kd = q.sc == q.sd, qd = q.bra == q.ket, af = q.fa > q.fb;
         // Jacc[a,b] is shared by lanes with the same bra pair; Kacc[a,c] and
-        // Kacc[b,c] by lanes that also share the ket's first shell
-        const WarpRuns rb((long long)q.bra, lane);
+        // Kacc[b,c] by lanes that also share the ket's first shell (the bra
+        // runs are scanned only for warps of more than one bra pair)
         const WarpRuns rbc(((long long)q.bra << 32) | (unsigned)q.sc, lane);
         // (the shuffle is taken by every lane, outside any condition)
         const int bra0 = __shfl_sync(0xffffffffu, q.bra, 0);
@@ -306,6 +306,7 @@ struct EpiJKn {
                 if (idx < NA * NB && (lane & (32 / KP - 1)) == 0 && js != 0.0)
                     atomicAdd(Jb + (q.fa + idx / NB) * nm + q.fb + idx % NB, 2.0 * js);
             } else {
+                const WarpRuns rb((long long)q.bra, lane);
 #pragma unroll
                 for (int ab = 0; ab < NA * NB; ++ab) {
                     const double js = rb.sum(jabv[ab]);
