@@ -40,7 +40,7 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one stored-integral J/K
 # launch on this workload, and summed over the 21 class launches of one FP64 direct build
 STORED_TRAFFIC_BYTES = 1620658000 + 5230080
-DIRECT_TRAFFIC_BYTES = 35018496 + 512
+DIRECT_TRAFFIC_BYTES = 34722560 + 0
 
 
 def parse():
