@@ -737,9 +737,12 @@ def main():
         direct = Ints.DirectInts(eng, precision, SCHWARZ, FP32_THRESH)
 
         def step():
+            if world == 1:   # get2JmK on host arrays: one C-ABI call (D in, build, G out)
+                direct.get2jmk_host(Dh, Gh)
+                return
             Dd = Dh.to("cuda", non_blocking=True)
             Jd, Kd = direct.jk(Dd)
-            allreduce_jk(Jd, Kd)
+            allreduce_jk(Jd, Kd)   # each rank built its shard of the quartets
             Gh.copy_(2.0 * Jd - Kd, non_blocking=True)
 
         for _ in range(a.warmup):
@@ -769,7 +772,9 @@ def main():
 
     # roofline: per-class FP64 timing of the direct J/K kernels
     per_class = []
-    nlaunch = 3   # density scaling and two symmetrise kernels per build
+    # density scaling, then one take of J and K from the graph's accumulators
+    # (without the graph: one symmetrise kernel each)
+    nlaunch = 2 if use_graph else 3
     for part in (0, 1):
         for qc in range(21):
             if qs[part, qc] == 0:
@@ -823,7 +828,11 @@ def main():
             "s_per_fock_build": ms * 1e-3,
             "e2e": {"value": Q / (e2e_ms * 1e-3), "unit": "quartets/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": int(D.numel() * 8), "d2h_bytes_per_step": int(D.numel() * 8),
-                    "api": "pyquante_b200.Ints.DirectInts.jk (the get2JmK path), FP64, from pinned host D"},
+                    "api": ("pyquante_b200.Ints.DirectInts.get2jmk_host -> pqb_get2jmk_host (get2JmK on host "
+                            "arrays: D in, build, G = 2J - K out in one call), FP64, pinned host D and G"
+                            if world == 1 else
+                            "pyquante_b200.Ints.DirectInts.jk on each rank's shard, NCCL all-reduce of J and K, "
+                            "G = 2J - K to pinned host memory")},
             "mixed": {"precision": "mixed", "fp32_threshold": FP32_THRESH, "dtype": "f64+f32",
                       "ms_per_step": ms_mixed, "value": Q / (ms_mixed * 1e-3), "unit": "quartets/s",
                       "speedup_vs_fp64": ms / ms_mixed,

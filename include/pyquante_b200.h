@@ -172,6 +172,15 @@ int pqb_eri_packed(pqb_ctx *ctx, double *out, int64_t len, void *stream);
  * must not overlap on different streams (see PQB_PARAM_GRAPH). */
 int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode, void *stream);
 
+/* G = 2J - K of a host density in one call: PyQuante's get2JmK(Ints, D)
+ * (PyQuante/Ints.py:225-238) on integral-direct integrals, with host arrays
+ * D_host and G_host (nbf x nbf, row-major; page-locked for asynchronous
+ * copies).  Copies D in, builds as pqb_jk_direct, takes G from the build's
+ * accumulators in one pass, and copies G out, all enqueued on the stream:
+ * G_host is complete once the stream reaches that point.  Single-molecule
+ * contexts; the context owns the device copies of D and G. */
+int pqb_get2jmk_host(pqb_ctx *ctx, const double *D_host, double *G_host, int mode, void *stream);
+
 /* J and K of two densities from one pass over the integrals: every
  * integral is evaluated once and digested against Da and Db.  Replaces the
  * four calls getJ(Ints, Da), getJ(Ints, Db), getK(Ints, Da), getK(Ints, Db)

@@ -130,6 +130,12 @@ class DirectInts:
     def j(self, D):
         return self.engine.j(D, self.precision, self.schwarz, self.fp32_threshold)
 
+    def get2jmk_host(self, D, G, stream=None):
+        """G = 2J - K into the host array G for the host density D, by one
+        C-ABI call (copies in and out on the stream; synchronise before
+        reading G)."""
+        return self.engine.get2jmk_host(D, G, self.precision, self.schwarz, self.fp32_threshold, stream)
+
 
 def _general_packed(bfs, eng):
     """Packed integrals for function lists that do not form s/p/d shells:
@@ -265,6 +271,24 @@ def getK(Ints, D):
 
 
 def get2JmK(Ints, D):
-    """G = 2J - K (PyQuante/Ints.py:225-238)."""
+    """G = 2J - K (PyQuante/Ints.py:225-238).  A host density on
+    integral-direct Ints (the reference's own call: numpy in, numpy out) goes
+    through pqb_get2jmk_host, which copies D in, builds and copies G out in
+    one call; J and K are not kept for a later getJ/getK."""
+    if isinstance(Ints, DirectInts) and _is_host(D):
+        n = Ints.nbf
+        if isinstance(D, torch.Tensor):
+            Dh = D.to(torch.float64).contiguous()
+            G = torch.empty((n, n), dtype=torch.float64)
+        else:
+            Dh = np.ascontiguousarray(D, dtype=np.float64)
+            G = np.empty((n, n))
+        Ints.get2jmk_host(Dh, G)
+        torch.cuda.current_stream(Ints.engine.device).synchronize()
+        return G
     J, K = _jk(Ints, D)
     return _back(2.0 * J - K, D)
+
+
+def _is_host(D):
+    return not (isinstance(D, torch.Tensor) and D.is_cuda)

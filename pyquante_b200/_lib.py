@@ -47,6 +47,7 @@ SIGNATURES = {
     "pqb_fp64_peak": (ctypes.c_int, [_vp, ctypes.c_int, _c_dbl_p]),
     "pqb_eri_packed": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp]),
     "pqb_jk_direct": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
+    "pqb_get2jmk_host": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
     "pqb_jk_direct2": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
     "pqb_jk_direct_class": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
     "pqb_jk_packed": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int, _vp]),

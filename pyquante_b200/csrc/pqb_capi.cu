@@ -98,6 +98,8 @@ struct pqb_ctx {
     bool graph_warm[6] = {false, false, false, false, false, false};   // one eager build first (one-time launch setup stays out of the capture)
     double *d_Jacc = nullptr, *d_Kacc = nullptr;
     double *d_Jacc2 = nullptr, *d_Kacc2 = nullptr;   // second density's graph accumulators
+    // pqb_get2jmk_host: D in, G out, and J, K of its builds outside the graph
+    double *d_hD = nullptr, *d_hG = nullptr, *d_hJ = nullptr, *d_hK = nullptr;
     ItemScreen scr{};                // caller-owned molecule mask / shell density bounds of the direct builds
     double *d_Qpair = nullptr;       // Schwarz factor per pair (device)
     int4 *d_shell_info = nullptr;    // per shell: first function within its molecule, functions, molecule
@@ -194,6 +196,37 @@ __global__ void symmetrize_take_kernel(double *__restrict__ A1, double *__restri
         M2[ij] = s2;
         M2[ji] = s2;
     }
+}
+
+// G = 2J - K straight from the graph's J and K accumulators (scaled and
+// symmetrised like symmetrize_take_kernel, which it replaces when the caller
+// wants G alone), leaving them zeroed.
+__global__ void take_2jmk_kernel(double *__restrict__ A1, double *__restrict__ A2, double *__restrict__ G, int n,
+                                 const double *__restrict__ S)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t P = (int64_t)n * (n + 1) / 2;
+    if (t >= P) return;
+    int i = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((int64_t)i * (i + 1) / 2 > t) --i;
+    while ((int64_t)(i + 1) * (i + 2) / 2 <= t) ++i;
+    int j = (int)(t - (int64_t)i * (i + 1) / 2);
+    const int64_t ij = (int64_t)i * n + j, ji = (int64_t)j * n + i;
+    const double sc = S ? S[ij] : 1.0;
+    const double g = fma(2.0, A1[ij] + A1[ji], -(A2[ij] + A2[ji])) * sc;
+    A1[ij] = 0.0;
+    A1[ji] = 0.0;
+    A2[ij] = 0.0;
+    A2[ji] = 0.0;
+    G[ij] = g;
+    G[ji] = g;
+}
+
+__global__ void combine_2jmk_kernel(const double *__restrict__ J, const double *__restrict__ K, double *__restrict__ G,
+                                    int64_t len)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < len; t += (int64_t)gridDim.x * blockDim.x)
+        G[t] = fma(2.0, J[t], -K[t]);
 }
 
 // Batched form: one CUDA block per molecule block of a block-diagonal layout.
@@ -1208,6 +1241,11 @@ static void release_basis(pqb_ctx *ctx)
     free_dev(ctx->d_Jacc2);
     free_dev(ctx->d_Kacc2);
     ctx->d_Jacc = ctx->d_Kacc = ctx->d_Jacc2 = ctx->d_Kacc2 = nullptr;
+    free_dev(ctx->d_hD);
+    free_dev(ctx->d_hG);
+    free_dev(ctx->d_hJ);
+    free_dev(ctx->d_hK);
+    ctx->d_hD = ctx->d_hG = ctx->d_hJ = ctx->d_hK = nullptr;
     free_dev(ctx->d_Dscaled2);
     free_dev(ctx->d_Dscaled2_f);
     ctx->d_Dscaled2 = nullptr;
@@ -1959,8 +1997,11 @@ static int ensure_build_graph(pqb_ctx *ctx, int nden, bool jonly, int mode, int 
 
 // J and K of nden densities D[s] into J[s], K[s] (K[0] == nullptr with one
 // density: J alone).
+// J and K of nden densities.  With G (one density, J and K wanted): G = 2J - K
+// as well; on the graph path G alone is written (J, K untouched), else J and
+// K are written and then combined.
 static int jk_direct_impl(pqb_ctx *ctx, int nden, const double *const D[2], double *const J[2], double *const K[2],
-                          int mode, void *stream)
+                          int mode, void *stream, double *G = nullptr)
 {
     const bool jonly = nden == 1 && !K[0];
     const int n = ctx->nbf;
@@ -1992,6 +2033,11 @@ static int jk_direct_impl(pqb_ctx *ctx, int nden, const double *const D[2], doub
         if (rc != PQB_OK) return rc;
         PQB_CK(ctx, cudaGraphLaunch(ctx->graph_exec[gi], st));
         double *Ja[2] = {ctx->d_Jacc, ctx->d_Jacc2}, *Ka[2] = {ctx->d_Kacc, ctx->d_Kacc2};
+        if (G) {
+            take_2jmk_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(Ja[0], Ka[0], G, n, ctx->d_escale);
+            PQB_CK(ctx, cudaGetLastError());
+            return PQB_OK;
+        }
         for (int s = 0; s < nden; ++s)
             symmetrize_take_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(
                 Ja[s], J[s], jonly ? nullptr : Ka[s], jonly ? nullptr : K[s], n, ctx->d_escale);
@@ -2011,6 +2057,7 @@ static int jk_direct_impl(pqb_ctx *ctx, int nden, const double *const D[2], doub
                 symmetrize_blocks_kernel<<<ctx->nmol, 256, 0, st>>>(K[s], ctx->d_mol_off, ctx->d_mol_n, ctx->d_escale);
         }
     }
+    if (G) combine_2jmk_kernel<<<ctx->nsm * 4, 256, 0, st>>>(J[0], K[0], G, (int64_t)n * n);
     PQB_CK(ctx, cudaGetLastError());
     return PQB_OK;
 }
@@ -2024,6 +2071,39 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
     const double *Dv[2] = {D, nullptr};
     double *Jv[2] = {J, nullptr}, *Kv[2] = {K, nullptr};
     return jk_direct_impl(ctx, 1, Dv, Jv, Kv, mode, stream);
+}
+
+static int get2jmk_host_impl(pqb_ctx *ctx, const double *D_host, double *G_host, int mode, void *stream)
+{
+    if (!ctx || !D_host || !G_host) return fail(ctx, PQB_E_ARG, "pqb_get2jmk_host: bad arguments");
+    if (!ctx->have_plan) return fail(ctx, PQB_E_STATE, "pqb_get2jmk_host: call pqb_plan first");
+    if (ctx->nmol != 1) return fail(ctx, PQB_E_STATE, "pqb_get2jmk_host: one molecule per context");
+    if (mode != PQB_FP64 && mode != PQB_MIXED) return fail(ctx, PQB_E_ARG, "pqb_get2jmk_host: mode %d", mode);
+    PQB_CK(ctx, cudaSetDevice(ctx->device));
+    const int n = ctx->nbf;
+    const size_t bytes = sizeof(double) * (size_t)n * n;
+    double **bufs[4] = {&ctx->d_hD, &ctx->d_hG, &ctx->d_hJ, &ctx->d_hK};
+    for (double **b : bufs)
+        if (!*b) PQB_CK(ctx, cudaMalloc(b, bytes));
+    cudaStream_t st = (cudaStream_t)stream;
+    PQB_CK(ctx, cudaMemcpyAsync(ctx->d_hD, D_host, bytes, cudaMemcpyHostToDevice, st));
+    const double *Dv[2] = {ctx->d_hD, nullptr};
+    double *Jv[2] = {ctx->d_hJ, nullptr}, *Kv[2] = {ctx->d_hK, nullptr};
+    const int rc = jk_direct_impl(ctx, 1, Dv, Jv, Kv, mode, stream, ctx->d_hG);
+    if (rc != PQB_OK) return rc;
+    PQB_CK(ctx, cudaMemcpyAsync(G_host, ctx->d_hG, bytes, cudaMemcpyDeviceToHost, st));
+    return PQB_OK;
+}
+
+int pqb_get2jmk_host(pqb_ctx *ctx, const double *D_host, double *G_host, int mode, void *stream)
+{
+    try {
+        return get2jmk_host_impl(ctx, D_host, G_host, mode, stream);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, PQB_E_NOMEM, "pqb_get2jmk_host: host allocation failed");
+    } catch (...) {
+        return fail(ctx, PQB_E_STATE, "pqb_get2jmk_host: unexpected host exception");
+    }
 }
 
 int pqb_jk_direct2(pqb_ctx *ctx, const double *Da, const double *Db, double *Ja, double *Ka, double *Jb, double *Kb,

@@ -21,6 +21,13 @@ from ._lib import ptr, stream_ptr
 _CART = {L: [(x, y, L - x - y) for x in range(L, -1, -1) for y in range(L - x, -1, -1)] for L in range(5)}
 
 
+def _host_ptr(x):
+    """Address of a host array (CPU torch tensor or numpy array)."""
+    if isinstance(x, torch.Tensor):
+        return ctypes.c_void_p(x.data_ptr())
+    return ctypes.c_void_p(x.ctypes.data)
+
+
 def cart_components(L):
     return _CART[L]
 
@@ -228,6 +235,26 @@ class BasisEngine:
         m = _lib.PQB_MIXED if mode == "mixed" else _lib.PQB_FP64
         self.ctx.check(self.ctx.lib.pqb_jk_direct(self.ctx.h, ptr(D), ptr(J), None, m, stream_ptr(stream)))
         return J
+
+    def get2jmk_host(self, D, G, mode="fp64", schwarz=1e-12, fp32_threshold=1e-5, stream=None):
+        """G = 2J - K into the host array G for the host density D (CPU
+        tensors or numpy arrays, float64, C-contiguous, nbf x nbf): one
+        pqb_get2jmk_host call that copies D in, builds and copies G out on the
+        stream; G is complete after a stream synchronisation."""
+        self._need_shells()
+        self.plan(schwarz, fp32_threshold)
+        n = self.nbf
+        for x in (D, G):
+            if isinstance(x, torch.Tensor):
+                ok = (not x.is_cuda) and x.dtype == torch.float64 and x.is_contiguous()
+            else:
+                ok = x.dtype == np.float64 and x.flags.c_contiguous
+            if not ok or tuple(x.shape) != (n, n):
+                raise ValueError("get2jmk_host: D and G must be C-contiguous float64 host arrays of shape (%d, %d)"
+                                 % (n, n))
+        m = _lib.PQB_MIXED if mode == "mixed" else _lib.PQB_FP64
+        self.ctx.check(self.ctx.lib.pqb_get2jmk_host(self.ctx.h, _host_ptr(D), _host_ptr(G), m, stream_ptr(stream)))
+        return G
 
     def jk2(self, Da, Db, mode="fp64", schwarz=1e-12, fp32_threshold=1e-5, stream=None):
         """J and K of two densities (UHF alpha and beta) from one pass over the

@@ -233,6 +233,18 @@ def test_jk_stored_and_direct_vs_oracle():
     d = Ints.get2ints(bs, direct=True, schwarz=0.0)
     Jd, Kd = Ints.getJ(d, D), Ints.getK(d, D)
     assert np.abs(Jd - Jo).max() < ERI_TOL and np.abs(Kd - Ko).max() < ERI_TOL
+    # host arrays through pqb_get2jmk_host on a fresh handle: the first call
+    # builds without the graph (J, K, then G), the next ones replay it and
+    # take G from the accumulators
+    d2 = Ints.get2ints(bs, direct=True, schwarz=0.0)
+    for _ in range(3):
+        Gh = Ints.get2JmK(d2, D)
+        assert isinstance(Gh, np.ndarray) and np.abs(Gh - (2 * Jo - Ko)).max() < 2 * ERI_TOL
+    Dp = torch.as_tensor(D).pin_memory()
+    Gp = torch.empty_like(Dp).pin_memory()
+    d2.get2jmk_host(Dp, Gp)
+    torch.cuda.synchronize()
+    assert np.abs(Gp.numpy() - (2 * Jo - Ko)).max() < 2 * ERI_TOL
     # torch in -> torch out, same values
     Dt = torch.as_tensor(D, device="cuda")
     Gt = Ints.get2JmK(d, Dt)
