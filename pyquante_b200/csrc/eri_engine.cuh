@@ -159,11 +159,11 @@ struct WarpRuns {
         const long long kn = __shfl_down_sync(0xffffffffu, key, 1);
         last = lane == 31 || kn != key;
     }
-    __device__ __forceinline__ double sum(double x) const
+    template <typename V> __device__ __forceinline__ V sum(V x) const
     {
 #pragma unroll
         for (int s = 0; s < 5; ++s) {
-            const double y = __shfl_up_sync(0xffffffffu, x, 1 << s);
+            const V y = __shfl_up_sync(0xffffffffu, x, 1 << s);
             if ((f >> s) & 1u) x += y;
         }
         return x;
@@ -175,15 +175,15 @@ struct WarpRuns {
 // every lane keeps half of its remaining values and adds its partner's half
 // of them, then the remaining levels are a plain butterfly.  Lane L ends with
 // the warp's sum of value idx(L) (the kept halves), held by the 32/KP lanes
-// that agree on those bits; 2 (KP - 1) + 2 (5 - log2 KP) 32-bit shuffles in
-// place of the 10 K of K separate sums.  Every lane of the warp must take part.
-template <int K>
-__device__ __forceinline__ double warp_sum_transposed(const double *v, int lane, int &idx)
+// that agree on those bits; (KP - 1) + (5 - log2 KP) shuffles in place of the
+// 5 K of K separate sums.  Every lane of the warp must take part.
+template <int K, typename V>
+__device__ __forceinline__ V warp_sum_transposed(const V *v, int lane, int &idx)
 {
     constexpr int KP = K <= 1 ? 1 : K <= 2 ? 2 : K <= 4 ? 4 : K <= 8 ? 8 : K <= 16 ? 16 : 32;
-    double w[KP];
+    V w[KP];
 #pragma unroll
-    for (int j = 0; j < KP; ++j) w[j] = j < K ? v[j] : 0.0;
+    for (int j = 0; j < KP; ++j) w[j] = j < K ? v[j] : (V)0;
     idx = 0;
     int o = 16;
 #pragma unroll
@@ -191,7 +191,7 @@ __device__ __forceinline__ double warp_sum_transposed(const double *v, int lane,
         const bool up = (lane & o) != 0;
 #pragma unroll
         for (int j = 0; j < n / 2; ++j) {
-            const double keep = up ? w[j + n / 2] : w[j], send = up ? w[j] : w[j + n / 2];
+            const V keep = up ? w[j + n / 2] : w[j], send = up ? w[j] : w[j + n / 2];
             w[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
         }
         if (up) idx += n / 2;
@@ -240,9 +240,9 @@ struct EpiJKn {
 
     // (called by every lane of the warp; a lane past the end of the item list
     // passes its neighbour's quartet with zero integrals)
-    // The per-quartet products and block sums run in the list's precision R
-    // (FP32 lists read the single-precision density); the sums over lanes and
-    // the accumulation into Jacc/Kacc are FP64.
+    // The per-quartet products, block sums and sums over lanes run in the
+    // list's precision R (FP32 lists read the single-precision density); the
+    // accumulation into Jacc/Kacc is FP64.
     template <int LA, int LB, int LC, int LD, typename R>
     __device__ __forceinline__ void thread_quartet(const QCtx &q, const R *acc, int lane, bool) const
     {
@@ -281,7 +281,7 @@ struct EpiJKn {
                     dcd[c][d] = __ldg(Dc + c * nm + q.fd + d);
                     jcd[c][d] = (T)0;
                 }
-            double jabv[NA * NB];
+            T jabv[NA * NB];
 #pragma unroll
             for (int a = 0; a < NA; ++a)
 #pragma unroll
@@ -296,12 +296,12 @@ struct EpiJKn {
                             jab = fma(v, dcd[c][d], jab);
                             jcd[c][d] = fma(v, dab[a][b], jcd[c][d]);
                         }
-                    jabv[a * NB + b] = (double)jab;
+                    jabv[a * NB + b] = jab;
                 }
             if (NA * NB <= 32 && one_bra) {
                 // the whole warp is one bra pair: all NAB sums in one transposed reduction
                 int idx;
-                const double js = warp_sum_transposed<(NA * NB <= 32 ? NA * NB : 1)>(jabv, lane, idx);
+                const double js = (double)warp_sum_transposed<(NA * NB <= 32 ? NA * NB : 1)>(jabv, lane, idx);
                 constexpr int KP = NA * NB <= 1 ? 1 : NA * NB <= 2 ? 2 : NA * NB <= 4 ? 4 : NA * NB <= 8 ? 8 : NA * NB <= 16 ? 16 : 32;
                 if (idx < NA * NB && (lane & (32 / KP - 1)) == 0 && js != 0.0)
                     atomicAdd(Jb + (q.fa + idx / NB) * nm + q.fb + idx % NB, 2.0 * js);
@@ -309,7 +309,7 @@ struct EpiJKn {
                 const WarpRuns rb((long long)q.bra, lane);
 #pragma unroll
                 for (int ab = 0; ab < NA * NB; ++ab) {
-                    const double js = rb.sum(jabv[ab]);
+                    const double js = (double)rb.sum(jabv[ab]);
                     if (rb.last && js != 0.0) atomicAdd(Jb + (q.fa + ab / NB) * nm + q.fb + ab % NB, 2.0 * js);
                 }
             }
@@ -350,7 +350,7 @@ struct EpiJKn {
                         }
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
-                    const double ks = rbc.sum((double)kac[c]);
+                    const double ks = (double)rbc.sum(kac[c]);
                     if (rbc.last && ks != 0.0) atomicAdd(Kb + (q.fa + a) * nm + q.fc + c, ks);
                 }
 #pragma unroll
@@ -388,7 +388,7 @@ struct EpiJKn {
                         }
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
-                    const double ks = rbc.sum((double)kbc[c]);
+                    const double ks = (double)rbc.sum(kbc[c]);
                     if (rbc.last && ks != 0.0) atomicAdd(Kb + (q.fb + b) * nm + q.fc + c, ks);
                 }
 #pragma unroll
