@@ -130,6 +130,10 @@ class DirectInts:
     def j(self, D):
         return self.engine.j(D, self.precision, self.schwarz, self.fp32_threshold)
 
+    def synchronize(self):
+        """Wait for the engine device's current stream (host results complete)."""
+        torch.cuda.current_stream(self.engine.device).synchronize()
+
     def get2jmk_host(self, D, G, stream=None):
         """G = 2J - K into the host array G for the host density D, by one
         C-ABI call (copies in and out on the stream; synchronise before
@@ -284,7 +288,7 @@ def get2JmK(Ints, D):
             Dh = np.ascontiguousarray(D, dtype=np.float64)
             G = np.empty((n, n))
         Ints.get2jmk_host(Dh, G)
-        torch.cuda.current_stream(Ints.engine.device).synchronize()
+        Ints.synchronize()
         return G
     J, K = _jk(Ints, D)
     return _back(2.0 * J - K, D)

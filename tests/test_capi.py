@@ -95,3 +95,31 @@ def test_repeated_density_reuses_the_last_build(monkeypatch):
     # a new integral array assigned to the same object: nothing remembered for the old one is served
     ints.tensor = torch.full((21,), 3.0, dtype=torch.float64)
     assert np.allclose(I.getK(ints, Db2), 3 * Db2 + 63) and len(calls) == 8
+
+
+def test_get2jmk_of_a_host_density_on_direct_ints_is_one_host_call(monkeypatch):
+    """get2JmK(DirectInts, D) with a host D (numpy in, numpy out; CPU tensor
+    in, CPU tensor out) goes through the one host-array call, which fills G
+    in place, and builds no J/K."""
+    import numpy as np
+    import torch
+
+    import pyquante_b200.Ints as I
+    calls = []
+    d = object.__new__(I.DirectInts)
+    d.nbf = 4
+
+    def fake_host(D, G, stream=None):
+        calls.append(type(D))
+        G[...] = 2.0 * D + 1.0
+        return G
+
+    monkeypatch.setattr(d, "get2jmk_host", fake_host, raising=False)
+    monkeypatch.setattr(d, "synchronize", lambda: None, raising=False)
+    monkeypatch.setattr(I, "_jk", lambda *a, **k: (_ for _ in ()).throw(AssertionError("J/K path taken")))
+    D = np.arange(16, dtype=np.float64).reshape(4, 4)
+    G = I.get2JmK(d, D)
+    assert isinstance(G, np.ndarray) and np.array_equal(G, 2.0 * D + 1.0)
+    Gt = I.get2JmK(d, torch.as_tensor(D))
+    assert isinstance(Gt, torch.Tensor) and not Gt.is_cuda and torch.equal(Gt, torch.as_tensor(2.0 * D + 1.0))
+    assert calls == [np.ndarray, torch.Tensor]
