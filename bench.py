@@ -772,14 +772,15 @@ def main():
 
     # roofline: per-class FP64 timing of the direct J/K kernels
     per_class = []
-    # density scaling, then one take of J and K from the graph's accumulators
-    # (without the graph: one symmetrise kernel each)
-    nlaunch = 2 if use_graph else 3
+    # launches of one timed FP64 build: density scaling, one kernel per class
+    # (an FP64 build runs both lists of a class in one launch), then one take
+    # of J and K from the graph's accumulators (without the graph: one
+    # symmetrise kernel each)
+    nlaunch = (2 if use_graph else 3) + sum(1 for qc in range(21) if qs[0, qc] + qs[1, qc] > 0)
     for part in (0, 1):
         for qc in range(21):
             if qs[part, qc] == 0:
                 continue
-            nlaunch += 1
             tms = []
             for _ in range(3):
                 flush.zero_()
