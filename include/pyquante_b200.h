@@ -177,8 +177,10 @@ int pqb_jk_direct(pqb_ctx *ctx, const double *D, double *J, double *K, int mode,
  * D_host and G_host (nbf x nbf, row-major; page-locked for asynchronous
  * copies).  Copies D in, builds as pqb_jk_direct, takes G from the build's
  * accumulators in one pass, and copies G out, all enqueued on the stream:
- * G_host is complete once the stream reaches that point.  Single-molecule
- * contexts; the context owns the device copies of D and G. */
+ * G_host is complete once the stream reaches that point (with a pageable
+ * G_host, such as a numpy array, when the call returns: CUDA finishes a
+ * device-to-pageable copy before its cudaMemcpyAsync returns).
+ * Single-molecule contexts; the context owns the device copies of D and G. */
 int pqb_get2jmk_host(pqb_ctx *ctx, const double *D_host, double *G_host, int mode, void *stream);
 
 /* J and K of two densities from one pass over the integrals: every
