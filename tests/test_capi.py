@@ -123,3 +123,29 @@ def test_get2jmk_of_a_host_density_on_direct_ints_is_one_host_call(monkeypatch):
     Gt = I.get2JmK(d, torch.as_tensor(D))
     assert isinstance(Gt, torch.Tensor) and not Gt.is_cuda and torch.equal(Gt, torch.as_tensor(2.0 * D + 1.0))
     assert calls == [np.ndarray, torch.Tensor]
+
+
+def test_get2jmk_host_rejects_bad_arrays_before_the_call(monkeypatch):
+    """BasisEngine.get2jmk_host checks shape, dtype and layout of both host
+    arrays and raises before reaching the C entry point."""
+    import numpy as np
+    import pytest
+    import torch
+
+    from pyquante_b200.engine import BasisEngine
+    eng = object.__new__(BasisEngine)
+    eng.nbf = 3
+    monkeypatch.setattr(eng, "_need_shells", lambda: None, raising=False)
+    monkeypatch.setattr(eng, "plan", lambda *a, **k: None, raising=False)
+
+    class NoCall:
+        def __getattr__(self, name):
+            raise AssertionError("C entry point reached")
+
+    eng.ctx = NoCall()
+    good = np.zeros((3, 3))
+    for D, G in ((np.zeros((3, 4)), good), (good, np.zeros((3, 3), dtype=np.float32)),
+                 (np.zeros((3, 6))[:, ::2], good), (torch.zeros(3, 3, dtype=torch.float32), good),
+                 (good, torch.zeros(4, 3, dtype=torch.float64))):
+        with pytest.raises(ValueError):
+            eng.get2jmk_host(D, G)
